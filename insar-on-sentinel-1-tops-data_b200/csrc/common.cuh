@@ -1,0 +1,114 @@
+// common.cuh -- shared device helpers and internal job layouts for the
+// B200 TOPS burst-pair kernels (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "tops_b200.h"
+
+namespace tops {
+
+// ------------------------------------------------------------ status
+// Thread-local record of the last CUDA error (tops_last_cuda_error()).
+void set_cuda_error(cudaError_t e);
+
+#define TOPS_CUDA_TRY(expr)                      \
+  do {                                           \
+    cudaError_t _e = (expr);                     \
+    if (_e != cudaSuccess) {                     \
+      ::tops::set_cuda_error(_e);                \
+      return (_e == cudaErrorMemoryAllocation) ? TOPS_E_NOMEM : TOPS_E_CUDA; \
+    }                                            \
+  } while (0)
+
+// --------------------------------------------------------- constants
+constexpr double kPi = 3.1415926535897931e+0;       // reference Constants.h:7
+constexpr double kSol = 299792458.0;                // reference Constants.h:6
+constexpr int kInterval = 2047;                     // reference Constants.h:8
+constexpr int kLutBins = 2048;
+constexpr int kTaps = 12;
+constexpr double kTwoPiHi = 6.283185307179586232e+00;
+constexpr double kTwoPiLo = 2.449293598294706414e-16;
+constexpr double kInvTwoPi = 0.15915494309189533577;
+
+// Cody-Waite reduction of a double phase to [-pi, pi] with a two-term 2*pi,
+// returned as float.  Exact to ~1e-15 rad for |phi| < 1e9.
+__device__ __forceinline__ float reduce_2pi(double phi) {
+  double n = rint(phi * kInvTwoPi);
+  double r = fma(-n, kTwoPiHi, phi);
+  r = fma(-n, kTwoPiLo, r);
+  return (float)r;
+}
+
+// Float reduction for small arguments (|x| < ~1e3) before __sincosf.
+__device__ __forceinline__ float reduce_2pi_f(float x) {
+  float n = rintf(x * 0.15915494309189535f);
+  x = fmaf(-n, 6.28318548202514648f, x);
+  x = fmaf(-n, -1.7484556e-07f, x);
+  return x;
+}
+
+// ------------------------------------------------- internal job layouts
+// Device-side view of one resample job (built from tops_resample_job).
+struct ResampleJob {
+  const short2 *slave;
+  long slave_pitch;       // short2 elements per row
+  float2 *out;
+  long out_pitch;         // float2 elements per row
+  const double *kt, *tref, *fdc;
+  int mx0, mx1, my0, my1;
+  int sx0, sx1, sy0, sy1;
+  double caz[6], crg[6];
+  double az_shift;
+  const double *az_shift_dev;
+  int s_first_line;
+  double dt;
+  int row0, nrows;        // master rows [row0, row0+nrows) (0-based in box)
+  // normalizeWarp constants: (v - mid) * inv
+  double midP, invP, midL, invL;
+  // work decomposition
+  int strips, segs, seg_rows;
+  int item_begin;         // first global work item of this job
+};
+
+struct CohJob {
+  const short2 *master;
+  long master_pitch;      // elements
+  const float2 *slave;
+  long slave_pitch;
+  float *coh;
+  long coh_pitch;
+  int lines, pixels;
+  int strips, segs, seg_rows;
+  int item_begin;
+};
+
+struct EsdOverlap {
+  const short2 *mF, *mB;
+  long m_pitch;
+  const float2 *sF, *sB;
+  long s_pitch;
+  int lines, pixels;
+  double spec_sep, dt;
+  int strips, segs, seg_rows;
+  int item_begin;
+};
+
+struct GeoJob {
+  const float *dem;
+  long dem_pitch;         // floats per row
+  int lines, pixels;
+  double lat0, lon0, dlat, dlon, nodata;
+  int xmin, xmax, ymin, ymax;
+  double dt[2], first_line_time[2], slr_time[2], range_spacing[2];
+  double mid_time[2], azi_init[2];
+  int line_offset[2];
+  double coef[2][3][8];
+  int ncoef[2];
+  double *cpm;
+  int *status;
+  int blocks;             // blocks assigned to this job
+  int block_begin;
+};
+
+}  // namespace tops

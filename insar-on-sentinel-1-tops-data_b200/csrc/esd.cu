@@ -1,0 +1,297 @@
+// esd.cu -- Enhanced Spectral Diversity azimuth-shift estimation (sm_100a).
+//
+// Reference chain per overlap (EstESDShifts_NonOverlap, EstESD.cu:914-1252):
+//   CohMatrixSet (:94-128) + CohFirstLineSet_ESD/CohDiffer_vertical_ESD/
+//   shfl_vertical_ESD/CpCoh2_ESD (:297-546)   -> gamma of the forward and of
+//                                                the backward band (zero-
+//                                                padded winAz x winRg box)
+//   Divide2 (:243-259)                        -> gamma = (gF + gB) / 2
+//   DoubleDifference4OneD (:62-91)            -> dd = (mF sF*) conj(mB sB*)
+//   MaskOut (:130-161)                        -> 0 if gamma < thr or >= 1,
+//                                                else exp(i arg dd)
+//   reduce0 x3 (:262-295)                     -> S = sum over the band
+//   host (:1213-1217)                         -> shift = atan2(S)/(2 pi df dt)
+//
+// B200 design: ONE kernel for all overlaps and both bands.  A CTA owns a
+// (strip, row segment) of one overlap; each thread owns a loaded column,
+// reads the four bands once per row (coalesced), keeps the vertical box sums
+// of both bands in registers and the centre-pixel interferograms in shared
+// memory; the horizontal box, the mask and the unit phasor are evaluated per
+// output pixel and accumulated in registers.  Per-CTA partial sums go to a
+// scratch array; a second tiny kernel reduces them per overlap in a fixed
+// order (deterministic) and evaluates the shift on the device, so the
+// shifts can feed the corrected resample without a host round trip.
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace tops {
+
+constexpr int ES_NT = 256;
+constexpr int ES_TW = 224;
+constexpr int ES_GR = 4;
+constexpr int ES_SEG = 32;
+constexpr int ES_MAXOV = 32;
+
+struct EsBatch {
+  int n_ov, total_items, win_rg, win_az;
+  float thr;
+  EsdOverlap ov[ES_MAXOV];
+};
+
+struct EsShared {
+  float4 VF[ES_GR][ES_NT];
+  float4 VB[ES_GR][ES_NT];
+  float2 IF[ES_GR][ES_NT];   // centre mF * conj(sF)
+  float2 IB[ES_GR][ES_NT];   // centre mB * conj(sB)
+  float2 red[ES_NT / 32];
+};
+
+__device__ __forceinline__ float4 prod4(short2 m, float2 s) {
+  const float mr = m.x, mi = m.y;
+  return make_float4(mr * s.x + mi * s.y, mi * s.x - mr * s.y, s.x * s.x + s.y * s.y,
+                     mr * mr + mi * mi);
+}
+
+__device__ __forceinline__ float gamma_of(float4 w) {
+  const float p = w.z * w.w;
+  return (p > 0.f) ? sqrtf(w.x * w.x + w.y * w.y) / sqrtf(p) : 0.f;
+}
+
+__global__ void __launch_bounds__(ES_NT) esd_kernel(const __grid_constant__ EsBatch B,
+                                                     double2 *partials) {
+  extern __shared__ __align__(16) unsigned char es_smem[];
+  EsShared &S = *reinterpret_cast<EsShared *>(es_smem);
+  const int tid = threadIdx.x;
+  const int item = blockIdx.x;
+  if (item >= B.total_items) return;
+  int ob = 0;
+  while (ob + 1 < B.n_ov && B.ov[ob + 1].item_begin <= item) ob++;
+  const EsdOverlap &O = B.ov[ob];
+  const int local = item - O.item_begin;
+  const int strip = local % O.strips, seg = local / O.strips;
+  const int win_rg = B.win_rg, win_az = B.win_az;
+  const int dw = (win_rg - 1) / 2, dh = (win_az - 1) / 2;
+  const int c0 = strip * ES_TW;
+  const int cN = min(ES_TW, O.pixels - c0);
+  const int nload = cN + win_rg - 1;
+  const int r_begin = seg * O.seg_rows;
+  const int r_end = min(r_begin + O.seg_rows, O.lines);
+  const int x = c0 - dw + tid;
+  const bool xin = tid < nload && x >= 0 && x < O.pixels;
+  float accr = 0.f, acci = 0.f;
+
+  for (int rg = r_begin; rg < r_end; rg += ES_GR) {
+    const int gr = min(ES_GR, r_end - rg);
+    float4 aF[ES_GR], aB[ES_GR];
+    float2 cF[ES_GR], cB[ES_GR];
+#pragma unroll
+    for (int k = 0; k < ES_GR; k++) {
+      aF[k] = aB[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+      cF[k] = cB[k] = make_float2(0.f, 0.f);
+    }
+    const int nin = gr + win_az - 1;
+    for (int q = 0; q < nin; q++) {
+      const int y = rg - dh + q;
+      float4 pF = make_float4(0.f, 0.f, 0.f, 0.f), pB = pF;
+      if (xin && y >= 0 && y < O.lines) {
+        const long mo = (long)y * O.m_pitch + x, so = (long)y * O.s_pitch + x;
+        pF = prod4(O.mF[mo], O.sF[so]);
+        pB = prod4(O.mB[mo], O.sB[so]);
+      }
+#pragma unroll
+      for (int k = 0; k < ES_GR; k++) {
+        const int j = q - k;
+        if (j >= 0 && j < win_az) {
+          aF[k].x += pF.x; aF[k].y += pF.y; aF[k].z += pF.z; aF[k].w += pF.w;
+          aB[k].x += pB.x; aB[k].y += pB.y; aB[k].z += pB.z; aB[k].w += pB.w;
+        }
+        if (q == k + dh) {
+          cF[k] = make_float2(pF.x, pF.y);
+          cB[k] = make_float2(pB.x, pB.y);
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < ES_GR; k++) {
+      S.VF[k][tid] = aF[k];
+      S.VB[k][tid] = aB[k];
+      S.IF[k][tid] = cF[k];
+      S.IB[k][tid] = cB[k];
+    }
+    __syncthreads();
+    const int ngrp = (cN + 3) >> 2;
+    for (int it = tid; it < gr * ngrp; it += ES_NT) {
+      const int k = it / ngrp;
+      const int cg = (it - k * ngrp) << 2;
+      float4 wF = make_float4(0.f, 0.f, 0.f, 0.f), wB = wF;
+      for (int i = 0; i < win_rg; i++) {
+        const float4 a = S.VF[k][cg + i], b = S.VB[k][cg + i];
+        wF.x += a.x; wF.y += a.y; wF.z += a.z; wF.w += a.w;
+        wB.x += b.x; wB.y += b.y; wB.z += b.z; wB.w += b.w;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        if (u > 0) {
+          const int ia = cg + u - 1 + win_rg, ib = cg + u - 1;
+          const float4 a = S.VF[k][ia], b = S.VF[k][ib];
+          wF.x += a.x - b.x; wF.y += a.y - b.y; wF.z += a.z - b.z; wF.w += a.w - b.w;
+          const float4 c = S.VB[k][ia], d = S.VB[k][ib];
+          wB.x += c.x - d.x; wB.y += c.y - d.y; wB.z += c.z - d.z; wB.w += c.w - d.w;
+        }
+        if (cg + u >= cN) continue;
+        const float g = (gamma_of(wF) + gamma_of(wB)) * 0.5f;
+        if (g < B.thr || g >= 1.f) continue;
+        const float2 f = S.IF[k][cg + u + dw], b = S.IB[k][cg + u + dw];
+        // (mF sF*) * conj(mB sB*)
+        const float dre = f.x * b.x + f.y * b.y;
+        const float dim = f.y * b.x - f.x * b.y;
+        const float n2 = dre * dre + dim * dim;
+        if (n2 > 0.f) {
+          const float inv = rsqrtf(n2);
+          accr += dre * inv;
+          acci += dim * inv;
+        } else {
+          accr += 1.f;  // atan2(0, 0) = 0 -> (1, 0), as the reference
+        }
+      }
+    }
+    __syncthreads();
+  }
+  // ---- block reduction (fixed order)
+  for (int o = 16; o > 0; o >>= 1) {
+    accr += __shfl_xor_sync(0xffffffffu, accr, o);
+    acci += __shfl_xor_sync(0xffffffffu, acci, o);
+  }
+  if ((tid & 31) == 0) S.red[tid >> 5] = make_float2(accr, acci);
+  __syncthreads();
+  if (tid == 0) {
+    double r = 0.0, i = 0.0;
+    for (int w = 0; w < ES_NT / 32; w++) {
+      r += S.red[w].x;
+      i += S.red[w].y;
+    }
+    partials[item] = make_double2(r, i);
+  }
+}
+
+__global__ void esd_finalize_kernel(const __grid_constant__ EsBatch B, const double2 *partials,
+                                    double *shifts, double *sums, int ov_offset) {
+  __shared__ double sr[256], si[256];
+  const int o = blockIdx.x;
+  const EsdOverlap &O = B.ov[o];
+  const int n = O.strips * O.segs;
+  double r = 0.0, i = 0.0;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    r += partials[O.item_begin + k].x;
+    i += partials[O.item_begin + k].y;
+  }
+  sr[threadIdx.x] = r;
+  si[threadIdx.x] = i;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      sr[threadIdx.x] += sr[threadIdx.x + s];
+      si[threadIdx.x] += si[threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double R = sr[0], I = si[0];
+    shifts[ov_offset + o] = atan2(I, R) / (2 * kPi * O.spec_sep * O.dt);
+    if (sums) {
+      sums[2 * (ov_offset + o)] = R;
+      sums[2 * (ov_offset + o) + 1] = I;
+    }
+  }
+}
+
+static int esd_items(const EsdOverlap &o) { return o.strips * o.segs; }
+
+int fill_esd_overlap(const tops_esd_overlap &u, EsdOverlap &O) {
+  if (!u.mF || !u.mB || !u.sF || !u.sB || u.lines < 0 || u.pixels <= 0) return TOPS_E_INVALID;
+  if ((u.m_pitch % sizeof(short2)) || (u.s_pitch % sizeof(float2))) return TOPS_E_INVALID;
+  O.mF = static_cast<const short2 *>(u.mF);
+  O.mB = static_cast<const short2 *>(u.mB);
+  O.m_pitch = (long)(u.m_pitch / sizeof(short2));
+  O.sF = static_cast<const float2 *>(u.sF);
+  O.sB = static_cast<const float2 *>(u.sB);
+  O.s_pitch = (long)(u.s_pitch / sizeof(float2));
+  if (O.m_pitch < u.pixels || O.s_pitch < u.pixels) return TOPS_E_INVALID;
+  O.lines = u.lines;
+  O.pixels = u.pixels;
+  O.spec_sep = u.spec_sep;
+  O.dt = u.dt;
+  O.strips = (u.pixels + ES_TW - 1) / ES_TW;
+  O.seg_rows = ES_SEG;
+  O.segs = u.lines > 0 ? (u.lines + ES_SEG - 1) / ES_SEG : 1;
+  return TOPS_OK;
+}
+
+size_t esd_scratch_bytes(const EsdOverlap *ov, int n) {
+  size_t items = 0;
+  for (int i = 0; i < n; i++) items += esd_items(ov[i]);
+  return items * sizeof(double2);
+}
+
+int launch_esd(const EsdOverlap *ovs, int n_ov, int win_az, int win_rg, float thr,
+               double *shifts, double *sums, void *scratch, size_t scratch_bytes,
+               cudaStream_t st) {
+  if (win_rg < 1 || win_az < 1 || win_rg > ES_NT - ES_TW + 1) return TOPS_E_INVALID;
+  if (esd_scratch_bytes(ovs, n_ov) > scratch_bytes || (!scratch && n_ov > 0) || !shifts)
+    return TOPS_E_INVALID;
+  static bool attr_done = false;
+  if (!attr_done) {
+    TOPS_CUDA_TRY(cudaFuncSetAttribute(esd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sizeof(EsShared)));
+    attr_done = true;
+  }
+  double2 *part = static_cast<double2 *>(scratch);
+  for (int o0 = 0; o0 < n_ov; o0 += ES_MAXOV) {
+    EsBatch B;
+    B.n_ov = 0;
+    B.win_rg = win_rg;
+    B.win_az = win_az;
+    B.thr = thr;
+    int items = 0;
+    for (int o = o0; o < n_ov && o < o0 + ES_MAXOV; o++) {
+      B.ov[B.n_ov] = ovs[o];
+      B.ov[B.n_ov].item_begin = items;
+      items += esd_items(ovs[o]);
+      B.n_ov++;
+    }
+    B.total_items = items;
+    esd_kernel<<<items, ES_NT, sizeof(EsShared), st>>>(B, part);
+    TOPS_CUDA_TRY(cudaGetLastError());
+    esd_finalize_kernel<<<B.n_ov, 256, 0, st>>>(B, part, shifts, sums, o0);
+    TOPS_CUDA_TRY(cudaGetLastError());
+    part += items;
+  }
+  return TOPS_OK;
+}
+
+}  // namespace tops
+
+using namespace tops;
+
+extern "C" size_t tops_esd_scratch_bytes(const tops_esd_overlap *ovs, int n_ov) {
+  std::vector<EsdOverlap> O(n_ov > 0 ? n_ov : 0);
+  for (int i = 0; i < n_ov; i++)
+    if (fill_esd_overlap(ovs[i], O[i]) != TOPS_OK) return 0;
+  return esd_scratch_bytes(O.data(), n_ov);
+}
+
+extern "C" int tops_esd(const tops_esd_overlap *ovs, int n_ov, int win_az, int win_rg,
+                        float coh_thr, double *shifts_dev, double *sums_dev, void *scratch_dev,
+                        size_t scratch_bytes, void *stream) {
+  if ((!ovs && n_ov > 0) || n_ov < 0) return TOPS_E_INVALID;
+  std::vector<EsdOverlap> O(n_ov);
+  for (int i = 0; i < n_ov; i++) {
+    int s = fill_esd_overlap(ovs[i], O[i]);
+    if (s != TOPS_OK) return s;
+  }
+  return launch_esd(O.data(), n_ov, win_az, win_rg, coh_thr, shifts_dev, sums_dev, scratch_dev,
+                    scratch_bytes, static_cast<cudaStream_t>(stream));
+}

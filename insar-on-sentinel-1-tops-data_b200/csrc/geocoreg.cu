@@ -1,0 +1,312 @@
+// geocoreg.cu -- DEM-assisted geometric coregistration (sm_100a, FP64).
+//
+// Reference (GeoCoreg_warp_cuda, Geocoreg_cuda.cu:610-913): per DEM pixel
+//   llh2xyz (:87-99) -> ECEF target; for master and slave a zero-Doppler
+//   Newton solve (ell2lpGeo :211-323 with getPos/getVelo/getAcc :123-205
+//   and SolveNewtonEq :101-112, <= 11 iterations, |step| < 1e-10 s) giving
+//   (line, pixel); weight 1 if the DEM is valid and the master position is
+//   inside the burst box (WeighthSet :548-574); A row [1, L, P, L^2, LP, P^2]
+//   of the normalised master position (AMatrixSet :576-605); then
+//   N = (WA)^T A, rhs = (WA)^T {slave line, slave pixel} by cuBLAS and a
+//   Cholesky solve by cuSOLVER (:822-851).
+//
+// B200 design: one fused kernel.  Each thread geocodes DEM pixels (master
+// and slave share the target position) and accumulates the 21 distinct
+// entries of N and the two right-hand sides (33 FP64 sums) in registers;
+// the block reduces them with warp shuffles in a fixed order and writes one
+// partial per block.  A one-block kernel per burst sums the partials in a
+// fixed order and solves the 6x6 system with the reference's own Cholesky
+// scheme (Func.cpp:959-1013).  No per-pixel buffers touch HBM; results are
+// bit-for-bit reproducible run to run.  Orbit polynomials and their first
+// two derivatives are evaluated with Horner's rule instead of pow().
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace tops {
+
+constexpr int GC_NT = 256;
+constexpr int GC_MAXJOBS = 16;
+constexpr int GC_NSUM = 33;
+constexpr double kEllA = 6378137.0;                              // cuConstants.cuh:5
+constexpr double kEllB = 6356752.3142451794975639665996337;      // cuConstants.cuh:6
+
+struct GcBatch {
+  int njobs, total_blocks;
+  int dem_is_int;
+  GeoJob jobs[GC_MAXJOBS];
+};
+
+// Position, velocity/10 and acceleration/100 of an orbit polynomial at the
+// normalised time t (getPos/getVelo/getAcc semantics).
+__device__ __forceinline__ void orbit_eval(const double (*c)[8], int n, double t, double p[3],
+                                           double v[3], double a[3]) {
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    double pp = c[k][n - 1], vv = 0.0, aa = 0.0;
+    for (int i = n - 2; i >= 0; --i) {
+      aa = fma(aa, t, 2.0 * vv);
+      vv = fma(vv, t, pp);
+      pp = fma(pp, t, c[k][i]);
+    }
+    p[k] = pp;
+    v[k] = vv / 10.0;
+    a[k] = aa / 100.0;
+  }
+}
+
+__device__ __forceinline__ void orbit_pos(const double (*c)[8], int n, double t, double p[3]) {
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    double pp = c[k][n - 1];
+    for (int i = n - 2; i >= 0; --i) pp = fma(pp, t, c[k][i]);
+    p[k] = pp;
+  }
+}
+
+// Zero-Doppler (line, pixel) of target T for image k of job J.
+__device__ void ell2lp(const GeoJob &J, int k, const double T[3], double &line, double &pixel) {
+  double az = J.azi_init[k];
+  const double (*c)[8] = J.coef[k];
+  const int n = J.ncoef[k];
+  double P[3], V[3], A[3];
+  for (int it = 0; it <= 10; it++) {
+    const double t = (az - J.mid_time[k]) / 10.0;
+    orbit_eval(c, n, t, P, V, A);
+    const double dx = T[0] - P[0], dy = T[1] - P[1], dz = T[2] - P[2];
+    const double sol = -(V[0] * dx + V[1] * dy + V[2] * dz) /
+                       ((A[0] * dx + A[1] * dy + A[2] * dz) - V[0] * V[0] - V[1] * V[1] -
+                        V[2] * V[2]);
+    az += sol;
+    if (fabs(sol) < 1e-010) break;
+  }
+  orbit_pos(c, n, (az - J.mid_time[k]) / 10.0, P);
+  line = J.line_offset[k] + (az - J.first_line_time[k]) / J.dt[k];
+  const double r = sqrt((T[0] - P[0]) * (T[0] - P[0]) + (T[1] - P[1]) * (T[1] - P[1]) +
+                        (T[2] - P[2]) * (T[2] - P[2]));
+  pixel = (r - J.slr_time[k] * kSol) / J.range_spacing[k];
+}
+
+__global__ void __launch_bounds__(GC_NT) geocoreg_kernel(const __grid_constant__ GcBatch B,
+                                                         double *partials) {
+  __shared__ double red[GC_NT / 32][GC_NSUM];
+  const int blk = blockIdx.x;
+  if (blk >= B.total_blocks) return;
+  int jb = 0;
+  while (jb + 1 < B.njobs && B.jobs[jb + 1].block_begin <= blk) jb++;
+  const GeoJob &J = B.jobs[jb];
+  const int lblk = blk - J.block_begin;
+  const long npx = (long)J.lines * J.pixels;
+  const double e2 = 1.0 - (kEllB * kEllB / kEllA / kEllA);
+  const double d2r = kPi / 180.0;
+  double acc[GC_NSUM];
+#pragma unroll
+  for (int q = 0; q < GC_NSUM; q++) acc[q] = 0.0;
+
+  for (long id = (long)lblk * GC_NT + threadIdx.x; id < npx; id += (long)J.blocks * GC_NT) {
+    const int row = (int)(id / J.pixels), col = (int)(id - (long)row * J.pixels);
+    float h;
+    if (B.dem_is_int)
+      h = (float)reinterpret_cast<const int *>(J.dem)[(long)row * J.dem_pitch + col];
+    else
+      h = J.dem[(long)row * J.dem_pitch + col];
+    if (h == (float)J.nodata) continue;
+    // llh2xyz (Geocoreg_cuda.cu:87-99)
+    double sphi, cphi, slam, clam;
+    sincos((J.lat0 - J.dlat * row) * d2r, &sphi, &cphi);
+    sincos((J.lon0 + J.dlon * col) * d2r, &slam, &clam);
+    const double nph = kEllA / sqrt(1.0 - e2 * sphi * sphi) + h;
+    const double T[3] = {nph * cphi * clam, nph * cphi * slam, (nph - e2 * (nph - h)) * sphi};
+    double ml, mp, sl, sp;
+    ell2lp(J, 0, T, ml, mp);
+    if (!(ml >= J.ymin && ml <= J.ymax && mp >= J.xmin && mp <= J.xmax)) continue;
+    ell2lp(J, 1, T, sl, sp);
+    const double L = (ml - 0.5 * ((double)J.ymin + (double)J.ymax)) /
+                     (0.25 * ((double)J.ymax - (double)J.ymin));
+    const double P = (mp - 0.5 * ((double)J.xmin + (double)J.xmax)) /
+                     (0.25 * ((double)J.xmax - (double)J.xmin));
+    const double a[6] = {1.0, L, P, L * L, L * P, P * P};
+    int q = 0;
+#pragma unroll
+    for (int i = 0; i < 6; i++)
+#pragma unroll
+      for (int j = i; j < 6; j++) acc[q++] += a[i] * a[j];
+#pragma unroll
+    for (int i = 0; i < 6; i++) {
+      acc[21 + i] += a[i] * sl;
+      acc[27 + i] += a[i] * sp;
+    }
+  }
+  // fixed-order block reduction
+#pragma unroll
+  for (int q = 0; q < GC_NSUM; q++) {
+    double v = acc[q];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5][q] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < GC_NSUM) {
+    double v = 0.0;
+    for (int w = 0; w < GC_NT / 32; w++) v += red[w][threadIdx.x];
+    partials[(long)blk * GC_NSUM + threadIdx.x] = v;
+  }
+}
+
+// Cholesky solve of the 6x6 normal equations (choles/solvechol semantics,
+// Func.cpp:959-1013); one block per job.
+__global__ void geocoreg_solve_kernel(const __grid_constant__ GcBatch B, const double *partials) {
+  __shared__ double tot[GC_NSUM];
+  const GeoJob &J = B.jobs[blockIdx.x];
+  if (threadIdx.x < GC_NSUM) {
+    double v = 0.0;
+    for (int b = 0; b < J.blocks; b++) v += partials[(long)(J.block_begin + b) * GC_NSUM + threadIdx.x];
+    tot[threadIdx.x] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  double n[36];
+  int q = 0;
+  for (int i = 0; i < 6; i++)
+    for (int j = i; j < 6; j++) {
+      n[i * 6 + j] = tot[q];
+      n[j * 6 + i] = tot[q];
+      q++;
+    }
+  int bad = 0;
+  for (int i = 0; i < 6; ++i)
+    for (int j = i; j < 6; ++j) {
+      double sum = n[i * 6 + j];
+      for (int k = i - 1; k >= 0; --k) sum -= n[i * 6 + k] * n[j * 6 + k];
+      if (i == j) {
+        if (!(sum > 0.0)) bad = 1;
+        n[i * 6 + i] = sqrt(sum);
+      } else {
+        n[j * 6 + i] = sum / n[i * 6 + i];
+      }
+    }
+  if (bad) {
+    *J.status = TOPS_E_NOT_PD;
+    return;
+  }
+  for (int r = 0; r < 2; r++) {
+    double b[6];
+    for (int i = 0; i < 6; i++) b[i] = tot[21 + 6 * r + i];
+    for (int i = 0; i < 6; ++i) {
+      double sum = b[i];
+      for (int j = i - 1; j >= 0; --j) sum -= n[i * 6 + j] * b[j];
+      b[i] = sum / n[i * 6 + i];
+    }
+    for (int i = 5; i >= 0; --i) {
+      double sum = b[i];
+      for (int j = i + 1; j < 6; ++j) sum -= n[j * 6 + i] * b[j];
+      b[i] = sum / n[i * 6 + i];
+    }
+    for (int i = 0; i < 6; i++) J.cpm[6 * r + i] = b[i];
+  }
+  *J.status = TOPS_OK;
+}
+
+static int gc_blocks_for(long npx) {
+  // enough blocks to fill the GPU, each thread handling >= 8 pixels
+  long b = (npx + GC_NT * 8 - 1) / (GC_NT * 8);
+  if (b < 1) b = 1;
+  if (b > 4096) b = 4096;
+  return (int)b;
+}
+
+int fill_geo_job(const tops_geo_job &u, GeoJob &J) {
+  if (!u.dem || !u.cpm_dev || !u.status_dev || u.dem_lines <= 0 || u.dem_pixels <= 0)
+    return TOPS_E_INVALID;
+  if (u.dem_pitch % sizeof(float)) return TOPS_E_INVALID;
+  if (u.xmax <= u.xmin || u.ymax <= u.ymin) return TOPS_E_INVALID;
+  for (int k = 0; k < 2; k++)
+    if (u.ncoef[k] < 2 || u.ncoef[k] > 8 || u.dt[k] == 0.0 || u.range_spacing[k] == 0.0)
+      return TOPS_E_INVALID;
+  J.dem = u.dem;
+  J.dem_pitch = (long)(u.dem_pitch / sizeof(float));
+  if (J.dem_pitch < u.dem_pixels) return TOPS_E_INVALID;
+  J.lines = u.dem_lines;
+  J.pixels = u.dem_pixels;
+  J.lat0 = u.lat0;
+  J.lon0 = u.lon0;
+  J.dlat = u.dlat;
+  J.dlon = u.dlon;
+  J.nodata = u.nodata;
+  J.xmin = u.xmin;
+  J.xmax = u.xmax;
+  J.ymin = u.ymin;
+  J.ymax = u.ymax;
+  for (int k = 0; k < 2; k++) {
+    J.dt[k] = u.dt[k];
+    J.first_line_time[k] = u.first_line_time[k];
+    J.slr_time[k] = u.slr_time[k];
+    J.range_spacing[k] = u.range_spacing[k];
+    J.mid_time[k] = u.mid_time[k];
+    J.azi_init[k] = u.azi_init[k];
+    J.line_offset[k] = u.line_offset[k];
+    J.ncoef[k] = u.ncoef[k];
+    for (int a = 0; a < 3; a++)
+      for (int i = 0; i < 8; i++) J.coef[k][a][i] = u.coef[k][a][i];
+  }
+  J.cpm = u.cpm_dev;
+  J.status = u.status_dev;
+  J.blocks = gc_blocks_for((long)u.dem_lines * u.dem_pixels);
+  return TOPS_OK;
+}
+
+size_t geocoreg_scratch(const GeoJob *J, int n) {
+  size_t blocks = 0;
+  for (int i = 0; i < n; i++) blocks += J[i].blocks;
+  return blocks * GC_NSUM * sizeof(double);
+}
+
+int launch_geocoreg(const GeoJob *jobs, int njobs, bool dem_is_int, void *scratch,
+                    size_t scratch_bytes, cudaStream_t st) {
+  if (geocoreg_scratch(jobs, njobs) > scratch_bytes || (!scratch && njobs > 0))
+    return TOPS_E_INVALID;
+  double *part = static_cast<double *>(scratch);
+  for (int j0 = 0; j0 < njobs; j0 += GC_MAXJOBS) {
+    GcBatch B;
+    B.njobs = 0;
+    B.dem_is_int = dem_is_int ? 1 : 0;
+    int blocks = 0;
+    for (int j = j0; j < njobs && j < j0 + GC_MAXJOBS; j++) {
+      B.jobs[B.njobs] = jobs[j];
+      B.jobs[B.njobs].block_begin = blocks;
+      blocks += jobs[j].blocks;
+      B.njobs++;
+    }
+    B.total_blocks = blocks;
+    geocoreg_kernel<<<blocks, GC_NT, 0, st>>>(B, part);
+    TOPS_CUDA_TRY(cudaGetLastError());
+    geocoreg_solve_kernel<<<B.njobs, 64, 0, st>>>(B, part);
+    TOPS_CUDA_TRY(cudaGetLastError());
+    part += (size_t)blocks * GC_NSUM;
+  }
+  return TOPS_OK;
+}
+
+}  // namespace tops
+
+using namespace tops;
+
+extern "C" size_t tops_geocoreg_scratch_bytes(const tops_geo_job *jobs, int njobs) {
+  std::vector<GeoJob> J(njobs > 0 ? njobs : 0);
+  for (int i = 0; i < njobs; i++)
+    if (fill_geo_job(jobs[i], J[i]) != TOPS_OK) return 0;
+  return geocoreg_scratch(J.data(), njobs);
+}
+
+extern "C" int tops_geocoreg(const tops_geo_job *jobs, int njobs, void *scratch_dev,
+                             size_t scratch_bytes, void *stream) {
+  if ((!jobs && njobs > 0) || njobs < 0) return TOPS_E_INVALID;
+  std::vector<GeoJob> J(njobs);
+  for (int i = 0; i < njobs; i++) {
+    int s = fill_geo_job(jobs[i], J[i]);
+    if (s != TOPS_OK) return s;
+  }
+  return launch_geocoreg(J.data(), njobs, false, scratch_dev, scratch_bytes,
+                         static_cast<cudaStream_t>(stream));
+}

@@ -1,0 +1,422 @@
+"""ctypes bindings of libtops_b200.so (the B200 TOPS burst-pair processor).
+
+Mirrors include/tops_b200.h and include/tops_synth.h.  The library must be
+built (``make`` in this directory); importing this module raises if it is
+missing -- there is no Python or CPU fallback for any GPU stage.
+
+Device-side calls take raw device pointers; callers in this repository get
+them from torch tensors (``tensor.data_ptr()``) and pass
+``torch.cuda.current_stream().cuda_stream`` as the stream.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libtops_b200.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(f"libtops_b200.so not built: run `make` in {_HERE}")
+lib = C.CDLL(LIB_PATH)
+
+TOPS_OK = 0
+TOPS_E_INVALID = 1
+TOPS_E_CUDA = 2
+TOPS_E_NOMEM = 3
+TOPS_E_NOT_PD = 4
+TOPS_E_TIMEOUT = 5
+TOPS_E_BUDGET = 6
+TOPS_E_CONFIG = 7
+TOPS_E_NODEVICE = 8
+LUT_BINS = 2048
+NPOINTS = 12
+MAX_BURSTS = 16
+
+_dp = C.POINTER(C.c_double)
+_fp = C.POINTER(C.c_float)
+_ip = C.POINTER(C.c_int)
+
+
+class TopsError(RuntimeError):
+    def __init__(self, status: int, what: str):
+        msg = lib.tops_status_string(status).decode()
+        super().__init__(f"{what}: status {status} ({msg}), cuda error {lib.tops_last_cuda_error()}")
+        self.status = status
+
+
+def check(status: int, what: str) -> None:
+    if status != TOPS_OK:
+        raise TopsError(status, what)
+
+
+# ------------------------------------------------------------------ structs
+class Poly(C.Structure):
+    _fields_ = [("aztime", C.c_double), ("t0", C.c_double), ("c0", C.c_double),
+                ("c1", C.c_double), ("c2", C.c_double)]
+
+
+class SynthCfg(C.Structure):
+    _fields_ = [
+        ("seed", C.c_long),
+        ("n_bursts", C.c_int), ("lines_per_burst", C.c_int), ("samples_per_burst", C.c_int),
+        ("overlap_lines", C.c_int),
+        ("sigma_dn", C.c_double), ("wavelength", C.c_double), ("dt", C.c_double),
+        ("rsr", C.c_double), ("steering_rate_deg", C.c_double), ("az_bandwidth", C.c_double),
+        ("rg_bandwidth", C.c_double), ("altitude", C.c_double), ("inc_mid_deg", C.c_double),
+        ("lat_center_deg", C.c_double),
+        ("dem_lines", C.c_int), ("dem_pixels", C.c_int),
+        ("hurst", C.c_double), ("h_min", C.c_double), ("h_max", C.c_double),
+        ("dem_spacing_arcsec", C.c_double), ("bperp", C.c_double), ("bpar", C.c_double),
+        ("along_track_s", C.c_double), ("az_shift_true", C.c_double),
+        ("topo_phase", C.c_int), ("interp_taps", C.c_int), ("threads", C.c_int),
+    ]
+
+
+class SwathInfo(C.Structure):
+    _fields_ = [
+        ("n_bursts", C.c_int), ("lines_per_burst", C.c_int), ("samples_per_burst", C.c_int),
+        ("first_valid_pixel", C.c_int),
+        ("dt", C.c_double), ("prf", C.c_double), ("slr_time", C.c_double),
+        ("range_spacing", C.c_double), ("wavelength", C.c_double), ("rsr", C.c_double),
+        ("az_bandwidth", C.c_double), ("steering_rate_deg", C.c_double),
+        ("first_line_time", C.c_double), ("last_line_time", C.c_double),
+        ("burst_first_line_time", C.c_double * MAX_BURSTS),
+        ("burst_last_line_time", C.c_double * MAX_BURSTS),
+        ("n_dc", C.c_int), ("n_fm", C.c_int),
+        ("dc_list", Poly * (MAX_BURSTS + 4)), ("fm_list", Poly * (MAX_BURSTS + 4)),
+        ("n_sv", C.c_int),
+        ("sv_t", C.c_double * 32), ("sv_x", C.c_double * 32), ("sv_y", C.c_double * 32),
+        ("sv_z", C.c_double * 32),
+    ]
+
+
+class DemInfo(C.Structure):
+    _fields_ = [("lines", C.c_int), ("pixels", C.c_int), ("lat0", C.c_double),
+                ("lon0", C.c_double), ("dlat", C.c_double), ("dlon", C.c_double)]
+
+
+class DerampDesc(C.Structure):
+    _fields_ = [
+        ("n_bursts", C.c_int), ("samples_per_burst", C.c_int), ("lines_per_burst", C.c_int),
+        ("first_valid_pixel", C.c_int),
+        ("slr_time_first_pixel", C.c_double), ("range_pixel_spacing", C.c_double),
+        ("azimuth_time_interval", C.c_double), ("first_line_time", C.c_double),
+        ("last_line_time", C.c_double), ("steering_rate_deg", C.c_double),
+        ("wavelength", C.c_double),
+        ("burst_first_line_time", _dp), ("burst_last_line_time", _dp),
+        ("dc_list", C.POINTER(Poly)), ("n_dc", C.c_int),
+        ("fm_list", C.POINTER(Poly)), ("n_fm", C.c_int),
+        ("orb_cx", _dp), ("orb_cy", _dp), ("orb_cz", _dp), ("orb_ncoef", C.c_int),
+        ("orb_mid_time", C.c_double),
+    ]
+
+
+class ResampleJob(C.Structure):
+    _fields_ = [
+        ("slave", C.c_void_p), ("slave_pitch", C.c_size_t),
+        ("out", C.c_void_p), ("out_pitch", C.c_size_t),
+        ("kt", C.c_void_p), ("tref", C.c_void_p), ("fdc", C.c_void_p),
+        ("mbox", C.c_int * 4), ("sbox", C.c_int * 4),
+        ("cpm_az", C.c_double * 6), ("cpm_rg", C.c_double * 6),
+        ("az_shift", C.c_double), ("az_shift_dev", C.c_void_p),
+        ("s_first_line", C.c_int), ("dt", C.c_double),
+        ("out_row0", C.c_int), ("out_rows", C.c_int),
+    ]
+
+
+class CohJob(C.Structure):
+    _fields_ = [("master", C.c_void_p), ("master_pitch", C.c_size_t),
+                ("slave", C.c_void_p), ("slave_pitch", C.c_size_t),
+                ("coh", C.c_void_p), ("coh_pitch", C.c_size_t),
+                ("lines", C.c_int), ("pixels", C.c_int)]
+
+
+class EsdOverlap(C.Structure):
+    _fields_ = [("mF", C.c_void_p), ("mB", C.c_void_p), ("m_pitch", C.c_size_t),
+                ("sF", C.c_void_p), ("sB", C.c_void_p), ("s_pitch", C.c_size_t),
+                ("lines", C.c_int), ("pixels", C.c_int),
+                ("spec_sep", C.c_double), ("dt", C.c_double)]
+
+
+class GeoJob(C.Structure):
+    _fields_ = [
+        ("dem", C.c_void_p), ("dem_pitch", C.c_size_t),
+        ("dem_lines", C.c_int), ("dem_pixels", C.c_int),
+        ("lat0", C.c_double), ("lon0", C.c_double), ("dlat", C.c_double), ("dlon", C.c_double),
+        ("nodata", C.c_double),
+        ("xmin", C.c_int), ("xmax", C.c_int), ("ymin", C.c_int), ("ymax", C.c_int),
+        ("dt", C.c_double * 2), ("first_line_time", C.c_double * 2),
+        ("slr_time", C.c_double * 2), ("range_spacing", C.c_double * 2),
+        ("mid_time", C.c_double * 2), ("azi_init", C.c_double * 2),
+        ("line_offset", C.c_int * 2),
+        ("coef", ((C.c_double * 8) * 3) * 2),
+        ("ncoef", C.c_int * 2),
+        ("cpm_dev", C.c_void_p), ("status_dev", C.c_void_p),
+    ]
+
+
+class Config(C.Structure):
+    _fields_ = [
+        ("process_dir", C.c_char * 512), ("masterpath", C.c_char * 512),
+        ("slavepath", C.c_char * 512), ("polarisation", C.c_char * 64),
+        ("preciseOrbitMaster", C.c_char * 512), ("preciseOrbitSlave", C.c_char * 512),
+        ("SpecificDemPath", C.c_char * 512),
+        ("firstsubswath", C.c_int), ("lastsubswath", C.c_int), ("multi_az", C.c_int),
+        ("multi_rg", C.c_int), ("burst0", C.c_int), ("burstN", C.c_int),
+        ("seed", C.c_long),
+        ("n_bursts", C.c_int), ("lines_per_burst", C.c_int), ("samples_per_burst", C.c_int),
+        ("overlap_lines", C.c_int), ("dem_lines", C.c_int), ("dem_pixels", C.c_int),
+        ("sigma_dn", C.c_double), ("az_shift_true", C.c_double),
+        ("coh_win_rg", C.c_int), ("coh_win_az", C.c_int), ("npoints", C.c_int),
+        ("esd_coh_threshold", C.c_double),
+        ("hbm_budget_gb", C.c_double), ("arrival_rate", C.c_double), ("n_jobs", C.c_int),
+    ]
+
+
+# --------------------------------------------------------------- prototypes
+def _proto(name, restype, argtypes):
+    f = getattr(lib, name)
+    f.restype = restype
+    f.argtypes = argtypes
+    return f
+
+
+_vp = C.c_void_p
+_proto("tops_status_string", C.c_char_p, [C.c_int])
+_proto("tops_last_cuda_error", C.c_int, [])
+_proto("tops_version", C.c_char_p, [])
+_proto("tops_lut", C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double, _fp, _fp])
+_proto("tops_polyfit_orbit", C.c_int, [C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _ip])
+_proto("tops_deramp_params", C.c_int, [C.POINTER(DerampDesc), _dp, _dp, _dp, _dp])
+_proto("tops_overlap_size", C.c_int, [C.c_int, _dp, _dp, C.c_double, _ip, _ip, _ip])
+_proto("tops_spectral_sep", C.c_double, [C.c_int, C.c_int, C.c_int, C.c_double, _dp])
+_proto("tops_config_defaults", C.c_int, [C.POINTER(Config)])
+_proto("tops_config_read", C.c_int, [C.c_char_p, C.POINTER(Config), _ip])
+_proto("tops_synth_defaults", C.c_int, [C.POINTER(SynthCfg)])
+_proto("tops_synth_create", C.c_int, [C.POINTER(SynthCfg), C.POINTER(_vp)])
+_proto("tops_synth_destroy", None, [_vp])
+_proto("tops_synth_swath", C.c_int, [_vp, C.c_int, C.POINTER(SwathInfo)])
+_proto("tops_synth_slc", C.POINTER(C.c_int16), [_vp, C.c_int])
+_proto("tops_synth_dem", _fp, [_vp, C.POINTER(DemInfo)])
+_proto("tops_synth_burst_dem_window", C.c_int, [_vp, C.c_int, C.c_int, _ip, _ip, _ip, _ip])
+_proto("tops_synth_truth", C.c_int, [_vp, C.c_int, C.POINTER(C.c_long), C.POINTER(_dp)])
+_proto("tops_synth_timing", C.c_int, [_vp, _dp])
+# reference-compatible ABI (host buffers)
+_proto("GeoCoreg_warp_cuda", C.c_int,
+       [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int,
+        C.c_int, _dp, _dp, C.c_double, C.c_double, C.c_int, C.c_double, C.c_double, C.c_double,
+        C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, _dp, _dp, C.c_int,
+        C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_bool,
+        C.c_bool, _ip, _dp, _dp, _dp, _dp, _dp, _dp, C.c_double, C.c_double])
+_RS_ARGS = [_vp, _dp, _dp, C.c_double, _vp, _fp, _fp, C.c_int, C.c_int, C.c_int, _ip, _ip, C.c_int,
+            C.c_int, C.c_double, _dp, _dp, _dp, C.c_int]
+_proto("DerampDemodResample", C.c_int, _RS_ARGS)
+_proto("DerampDemodResample_ESD", _vp, _RS_ARGS)
+_proto("ResampleFirstBurst", _vp, [_vp, C.c_int, C.c_int])
+_proto("EstESDShifts", C.c_int, [_vp, _vp, _vp, _vp, _ip, _dp, C.c_int, C.c_int, C.c_int, C.c_int,
+                                 C.c_int, C.c_int, C.c_float, C.c_double, C.c_double])
+_COH_ARGS = [C.c_int] * 8 + [_vp, _vp, _fp]
+_proto("CoherenceEst", C.c_int, _COH_ARGS)
+_proto("CoherenceEst_ESD", C.c_int, _COH_ARGS)
+_proto("tops_free_device", C.c_int, [_vp])
+# device API
+_proto("tops_lut_create", C.c_int, [_fp, _fp, C.POINTER(_vp)])
+_proto("tops_lut_destroy", C.c_int, [_vp])
+_proto("tops_resample", C.c_int, [_vp, C.POINTER(ResampleJob), C.c_int, _vp])
+_proto("tops_coherence", C.c_int, [C.POINTER(CohJob), C.c_int, C.c_int, C.c_int, _vp])
+_proto("tops_esd_scratch_bytes", C.c_size_t, [C.POINTER(EsdOverlap), C.c_int])
+_proto("tops_esd", C.c_int, [C.POINTER(EsdOverlap), C.c_int, C.c_int, C.c_int, C.c_float, _vp,
+                             _vp, _vp, C.c_size_t, _vp])
+_proto("tops_geocoreg_scratch_bytes", C.c_size_t, [C.POINTER(GeoJob), C.c_int])
+_proto("tops_geocoreg", C.c_int, [C.POINTER(GeoJob), C.c_int, _vp, C.c_size_t, _vp])
+
+
+def ptr(a: np.ndarray, ctype):
+    """ctypes pointer to a C-contiguous numpy array."""
+    assert a.flags["C_CONTIGUOUS"], "array must be C-contiguous"
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+def vptr(a: np.ndarray):
+    assert a.flags["C_CONTIGUOUS"], "array must be C-contiguous"
+    return C.c_void_p(a.ctypes.data)
+
+
+# ------------------------------------------------------------ host helpers
+def lut(prf: float, abw: float, rsr2x: float, npoints: int = NPOINTS):
+    kaz = np.zeros((LUT_BINS, npoints), np.float32)
+    krg = np.zeros((LUT_BINS, npoints), np.float32)
+    check(lib.tops_lut(npoints, prf, abw, rsr2x, ptr(kaz, C.c_float), ptr(krg, C.c_float)),
+          "tops_lut")
+    return kaz, krg
+
+
+def polyfit_orbit(t, x, y, z):
+    t, x, y, z = (np.ascontiguousarray(v, np.float64) for v in (t, x, y, z))
+    cx, cy, cz = (np.zeros(8) for _ in range(3))
+    n = C.c_int(0)
+    check(lib.tops_polyfit_orbit(len(t), ptr(t, C.c_double), ptr(x, C.c_double),
+                                 ptr(y, C.c_double), ptr(z, C.c_double), ptr(cx, C.c_double),
+                                 ptr(cy, C.c_double), ptr(cz, C.c_double), C.byref(n)),
+          "tops_polyfit_orbit")
+    return cx[:n.value].copy(), cy[:n.value].copy(), cz[:n.value].copy()
+
+
+def overlap_size(first, last, dt):
+    first = np.ascontiguousarray(first, np.float64)
+    last = np.ascontiguousarray(last, np.float64)
+    n = len(first)
+    ov = np.zeros(max(n - 1, 1), np.int32)
+    tot, mx = C.c_int(), C.c_int()
+    check(lib.tops_overlap_size(n, ptr(first, C.c_double), ptr(last, C.c_double), dt,
+                                ptr(ov, C.c_int), C.byref(tot), C.byref(mx)), "tops_overlap_size")
+    return ov[:n - 1], tot.value, mx.value
+
+
+def spectral_sep(kt: np.ndarray, L: int, dt: float) -> float:
+    kt = np.ascontiguousarray(kt, np.float64)
+    return lib.tops_spectral_sep(kt.shape[0], kt.shape[1], L, dt, ptr(kt, C.c_double))
+
+
+def swath_deramp_params(info: SwathInfo, orbit_coefs, ncoef: int):
+    """kt, tref, fdc (and FM rate) [n_bursts][W] for a swath."""
+    nb, W = info.n_bursts, info.samples_per_burst
+    cx, cy, cz = (np.ascontiguousarray(c, np.float64) for c in orbit_coefs)
+    first = np.array(info.burst_first_line_time[:nb])
+    last = np.array(info.burst_last_line_time[:nb])
+    d = DerampDesc()
+    d.n_bursts, d.samples_per_burst, d.lines_per_burst = nb, W, info.lines_per_burst
+    d.first_valid_pixel = info.first_valid_pixel
+    d.slr_time_first_pixel, d.range_pixel_spacing = info.slr_time, info.range_spacing
+    d.azimuth_time_interval = info.dt
+    d.first_line_time, d.last_line_time = info.first_line_time, info.last_line_time
+    d.steering_rate_deg, d.wavelength = info.steering_rate_deg, info.wavelength
+    d.burst_first_line_time, d.burst_last_line_time = ptr(first, C.c_double), ptr(last, C.c_double)
+    d.dc_list = C.cast(info.dc_list, C.POINTER(Poly))
+    d.n_dc = info.n_dc
+    d.fm_list = C.cast(info.fm_list, C.POINTER(Poly))
+    d.n_fm = info.n_fm
+    d.orb_cx, d.orb_cy, d.orb_cz = ptr(cx, C.c_double), ptr(cy, C.c_double), ptr(cz, C.c_double)
+    d.orb_ncoef = ncoef
+    d.orb_mid_time = info.sv_t[info.n_sv // 2]
+    dc, fm, tref, kt = (np.zeros((nb, W)) for _ in range(4))
+    check(lib.tops_deramp_params(C.byref(d), ptr(dc, C.c_double), ptr(fm, C.c_double),
+                                 ptr(tref, C.c_double), ptr(kt, C.c_double)), "tops_deramp_params")
+    return {"dc": dc, "fmrate": fm, "tref": tref, "kt": kt}
+
+
+def read_config(path: str) -> Config:
+    cfg = Config()
+    check(lib.tops_config_defaults(C.byref(cfg)), "tops_config_defaults")
+    line = C.c_int(0)
+    st = lib.tops_config_read(path.encode(), C.byref(cfg), C.byref(line))
+    if st != TOPS_OK:
+        raise TopsError(st, f"tops_config_read({path}) line {line.value}")
+    return cfg
+
+
+# ----------------------------------------------------------- synthetic scene
+class Scene:
+    """A seeded synthetic burst pair (tops_synth_create)."""
+
+    def __init__(self, **overrides):
+        cfg = SynthCfg()
+        check(lib.tops_synth_defaults(C.byref(cfg)), "tops_synth_defaults")
+        for k, v in overrides.items():
+            if not hasattr(cfg, k):
+                raise KeyError(k)
+            setattr(cfg, k, v)
+        self.cfg = cfg
+        h = C.c_void_p()
+        check(lib.tops_synth_create(C.byref(cfg), C.byref(h)), "tops_synth_create")
+        self._h = h
+        nb, L, W = cfg.n_bursts, cfg.lines_per_burst, cfg.samples_per_burst
+        self.shape = (nb * L, W)
+        self.swath = []
+        for w in (0, 1):
+            info = SwathInfo()
+            check(lib.tops_synth_swath(h, w, C.byref(info)), "tops_synth_swath")
+            self.swath.append(info)
+        self.slc = []
+        for w in (0, 1):
+            p = lib.tops_synth_slc(h, w)
+            a = np.ctypeslib.as_array(p, shape=(nb * L, W, 2))
+            self.slc.append(a.copy())
+        di = DemInfo()
+        p = lib.tops_synth_dem(h, C.byref(di))
+        self.dem_info = di
+        self.dem = np.ctypeslib.as_array(p, shape=(di.lines, di.pixels)).copy()
+        t = np.zeros(5)
+        lib.tops_synth_timing(h, ptr(t, C.c_double))
+        self.timing = t
+        # orbit fits and deramp parameters (product host code)
+        self.orbit = []
+        self.deramp = []
+        for w in (0, 1):
+            info = self.swath[w]
+            n = info.n_sv
+            cx, cy, cz = polyfit_orbit(info.sv_t[:n], info.sv_x[:n], info.sv_y[:n], info.sv_z[:n])
+            self.orbit.append((cx, cy, cz))
+            self.deramp.append(swath_deramp_params(info, (cx, cy, cz), len(cx)))
+        m = self.swath[0]
+        self.kaz, self.krg = lut(m.prf, m.az_bandwidth, 2 * m.rsr)
+
+    def dem_window(self, burst: int, margin: int = 24):
+        r0, c0, nr, nc = (C.c_int() for _ in range(4))
+        check(lib.tops_synth_burst_dem_window(self._h, burst, margin, C.byref(r0), C.byref(c0),
+                                              C.byref(nr), C.byref(nc)), "dem window")
+        return r0.value, c0.value, nr.value, nc.value
+
+    def truth(self, burst: int) -> np.ndarray:
+        n = C.c_long()
+        p = _dp()
+        check(lib.tops_synth_truth(self._h, burst, C.byref(n), C.byref(p)), "truth")
+        return np.ctypeslib.as_array(p, shape=(n.value, 4)).copy()
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.tops_synth_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- per-burst views and stage inputs
+    def burst(self, which: int, b: int) -> np.ndarray:
+        L = self.cfg.lines_per_burst
+        return np.ascontiguousarray(self.slc[which][b * L:(b + 1) * L])
+
+    def boxes(self, b: int, burst_gap: int = 0):
+        """MasterBox / SlaveBox of burst b (Func.cpp:2354-2371)."""
+        L, W = self.cfg.lines_per_burst, self.cfg.samples_per_burst
+        mb = np.array([0, W - 1, b * L, (b + 1) * L - 1], np.int32)
+        sb = np.array([0, W - 1, (b + burst_gap) * L, (b + burst_gap + 1) * L - 1], np.int32)
+        return mb, sb
+
+    def geo_args(self, b: int, margin: int = 24):
+        """Arguments of one burst's geometric coregistration (Func.cpp:2225-2278),
+        with the DEM window's own origin (not the burst box corner)."""
+        L, W = self.cfg.lines_per_burst, self.cfg.samples_per_burst
+        m, s = self.swath
+        r0, c0, nr, nc = self.dem_window(b, margin)
+        di = self.dem_info
+        return dict(
+            dem=np.ascontiguousarray(self.dem[r0:r0 + nr, c0:c0 + nc]),
+            lat0=di.lat0 - r0 * di.dlat, lon0=di.lon0 + c0 * di.dlon,
+            dlat=di.dlat, dlon=di.dlon,
+            xmin=0, xmax=W - 1, ymin=b * L, ymax=(b + 1) * L - 1,
+            dt=(m.dt, s.dt),
+            first_line_time=(m.burst_first_line_time[b], s.burst_first_line_time[b]),
+            slr_time=(m.slr_time, s.slr_time), range_spacing=(m.range_spacing, s.range_spacing),
+            mid_time=(m.sv_t[m.n_sv // 2], s.sv_t[s.n_sv // 2]),
+            azi_init=(0.5 * (m.burst_first_line_time[b] + m.burst_last_line_time[b]),
+                      0.5 * (s.burst_first_line_time[b] + s.burst_last_line_time[b])),
+            line_offset=(b * L, b * L),
+            coefs=(self.orbit[0], self.orbit[1]),
+        )
