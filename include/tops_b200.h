@@ -152,10 +152,12 @@ typedef struct {
   int mbox[4], sbox[4];            /* {x0, x1, y0, y1} inclusive */
   double cpm_az[6], cpm_rg[6];
   double az_shift;                 /* lines added to the azimuth polynomial */
-  const double *az_shift_dev;      /* if non-NULL, *az_shift_dev is used */
+  const double *az_shift_dev;      /* if non-NULL, *az_shift_dev is used (|v| > 100 -> 0) */
+  const double *cpm_dev;           /* if non-NULL, 12 device doubles replace cpm_az/cpm_rg */
   int s_first_line;                /* sBurstIdx * linesPerBurst */
   double dt;                       /* azimuth time interval [s] */
-  int out_row0, out_rows;          /* master rows to produce; out_rows<0: all */
+  int out_row0, out_rows;          /* master rows to produce; out_rows<0: all.
+                                      `out` points at the row out_row0 */
 } tops_resample_job;
 
 /* Resamples njobs bursts in one launch on `stream` (cudaStream_t). */
@@ -242,6 +244,27 @@ int tops_deramp_params(const tops_deramp_desc *d, double *dc, double *fmrate, do
 int tops_overlap_size(int n_bursts, const double *first_time, const double *last_time, double dt,
                       int *ov, int *total, int *maximum);
 double tops_spectral_sep(int n_bursts, int W, int L, double dt, const double *kt);
+
+/* ====================================================== swath metadata */
+
+#define TOPS_MAX_BURSTS 16
+
+/* Annotation-level description of one sub-swath of one acquisition: what
+ * the reference reads from the SAFE annotation and the precise orbit
+ * (SubSwathInfo / S1PreciseOrbit, DataTypes.h:41-177).  Times in seconds,
+ * slr_time one-way slant-range time of the first sample. */
+typedef struct {
+  int n_bursts, lines_per_burst, samples_per_burst, first_valid_pixel;
+  double dt, prf, slr_time, range_spacing, wavelength, rsr, az_bandwidth, steering_rate_deg;
+  double first_line_time, last_line_time;
+  double burst_first_line_time[TOPS_MAX_BURSTS];
+  double burst_last_line_time[TOPS_MAX_BURSTS];
+  int n_dc, n_fm;
+  tops_poly dc_list[TOPS_MAX_BURSTS + 4];
+  tops_poly fm_list[TOPS_MAX_BURSTS + 4];
+  int n_sv;
+  double sv_t[32], sv_x[32], sv_y[32], sv_z[32];
+} tops_swath_info;
 
 /* ============================================================ config */
 

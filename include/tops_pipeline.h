@@ -1,0 +1,107 @@
+/*
+ * tops_pipeline.h -- burst-pair processing of one master/slave sub-swath.
+ *
+ * The reference runs its stages per burst from host drivers (Func.cpp:
+ * GeometricCoreg 2215-2297, DerampAndResample 2326-2406, ESDAndCoh
+ * 2496-2763), round-tripping every intermediate through host memory and
+ * GeoTIFF files.  Two forms are provided here:
+ *
+ *  - tops_plain_pair(): the reference's driver sequence, per burst, through
+ *    the reference-compatible entry points with host buffers (the "plain"
+ *    form; same dataflow and ordering as the reference).
+ *
+ *  - tops_pair_*: a device-resident plan.  All inputs, intermediates and
+ *    outputs stay in HBM; each stage is one batched launch over all bursts;
+ *    the offset polynomials and ESD shifts flow from kernel to kernel through
+ *    device memory, so a whole sub-swath pair is a fixed, host-sync-free
+ *    sequence of launches that can be captured in one CUDA graph.
+ *
+ * Dataflow (both forms): geometric coregistration of every burst ->
+ * resample every burst (ReSlave) -> ESD over the burst overlaps -> resample
+ * bursts after the first with the ESD shift of the preceding overlap
+ * (ReSlaveESD; the first burst is not corrected, Func.cpp:2653-2674) ->
+ * coherence of master vs ReSlaveESD.
+ */
+#ifndef TOPS_PIPELINE_H
+#define TOPS_PIPELINE_H
+
+#include "tops_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+  int win_rg, win_az;       /* coherence / ESD window (reference: 24 x 6) */
+  float esd_threshold;      /* ESD coherence threshold (reference: 0.3) */
+  int reslave_full;         /* 1: ReSlave for every line (reference output);
+                               0: only the overlap bands ESD needs */
+  int burst0_deramp_rows;   /* 1: deramp rows of burst 0 for every burst, as
+                               the reference passes them (Func.cpp:2383) */
+} tops_pair_opts;
+
+int tops_pair_opts_default(tops_pair_opts *o);
+
+/* DEM window [row0, row0+rows) x [col0, col0+cols) of one burst. */
+typedef struct { int row0, col0, rows, cols; } tops_dem_window;
+
+typedef struct tops_pair tops_pair;
+
+/* Device bytes a plan allocates (for HBM-budget admission). */
+size_t tops_pair_footprint(const tops_swath_info *master, const tops_pair_opts *o, int dem_lines,
+                           int dem_pixels);
+
+/* Create a plan: host precomputes (orbit fits, deramp parameters, LUT,
+ * overlaps, spectral separation) and every device buffer. */
+int tops_pair_create(const tops_swath_info *master, const tops_swath_info *slave,
+                     const tops_pair_opts *o, int dem_lines, int dem_pixels, tops_pair **out);
+int tops_pair_destroy(tops_pair *p);
+
+/* DEM heights (host float [dem_lines][dem_pixels]), geotransform and one
+ * window per burst.  Asynchronous on `stream`. */
+int tops_pair_set_dem(tops_pair *p, const float *dem, double lat0, double lon0, double dlat,
+                      double dlon, const tops_dem_window *windows, void *stream);
+
+/* Upload the burst-stacked CInt16 SLCs [n_bursts*lines][samples] (host;
+ * pinned memory gives full-bandwidth asynchronous copies). */
+int tops_pair_upload(tops_pair *p, const void *master, const void *slave, void *stream);
+
+/* All stages on the device, enqueued on `stream` without host sync. */
+int tops_pair_run(tops_pair *p, void *stream);
+
+/* Same, as one CUDA graph (captured on first use, then replayed). */
+int tops_pair_run_graph(tops_pair *p, void *stream);
+
+/* Copy results to the host (NULL skips an output): ReSlave (complex64, only
+ * with reslave_full), ReSlaveESD (complex64), coherence (float)
+ * [n_bursts*lines][samples]; cpm [n_bursts][12]; shifts [n_bursts-1]. */
+int tops_pair_download(tops_pair *p, void *reslave, void *reslave_esd, float *coh, double *cpm,
+                       double *shifts, void *stream);
+
+typedef struct {
+  void *master, *slave;            /* CInt16, pitch slc_pitch */
+  void *reslave, *reslave_esd;     /* complex64, pitch cplx_pitch */
+  float *coh;                      /* pitch coh_pitch */
+  double *cpm, *shifts;
+  int *geo_status;
+  size_t slc_pitch, cplx_pitch, coh_pitch;
+  int n_bursts, lines, samples;
+  int n_launches;                  /* kernels one tops_pair_run launches */
+} tops_pair_buffers;
+
+int tops_pair_buffers_get(const tops_pair *p, tops_pair_buffers *b);
+
+/* Reference-shaped per-burst processing through the reference-compatible
+ * entry points (host buffers).  dem_int: int heights of the full DEM;
+ * outputs as tops_pair_download. */
+int tops_plain_pair(const tops_swath_info *master, const tops_swath_info *slave,
+                    const tops_pair_opts *o, const int *dem_int, int dem_lines, int dem_pixels,
+                    double lat0, double lon0, double dlat, double dlon,
+                    const tops_dem_window *windows, const void *master_slc,
+                    const void *slave_slc, void *reslave, void *reslave_esd, float *coh,
+                    double *cpm, double *shifts);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

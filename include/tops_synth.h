@@ -13,7 +13,8 @@
  *            centroid and FM-rate polynomial lists, steering rate
  *   SLCs     master: band-limited circular Gaussian reflectivity with the
  *            TOPS azimuth ramp; slave: the same scene seen from the slave
- *            orbit (geocoded through the DEM), with its own ramp, the
+ *            orbit (geocoded through the DEM): each ground point keeps the
+ *            Doppler history it has in the master burst, plus the
  *            topographic phase and an optional azimuth misregistration of
  *            `az_shift_true` lines (what ESD must measure)
  *
@@ -30,7 +31,7 @@
 extern "C" {
 #endif
 
-#define TOPS_SYNTH_MAX_BURSTS 16
+#define TOPS_SYNTH_MAX_BURSTS TOPS_MAX_BURSTS
 
 typedef struct {
   long seed;
@@ -56,18 +57,6 @@ typedef struct {
   int threads;                /* OpenMP threads (0 = default) */
 } tops_synth_cfg;
 
-typedef struct {
-  int n_bursts, lines_per_burst, samples_per_burst, first_valid_pixel;
-  double dt, prf, slr_time, range_spacing, wavelength, rsr, az_bandwidth, steering_rate_deg;
-  double first_line_time, last_line_time;
-  double burst_first_line_time[TOPS_SYNTH_MAX_BURSTS];
-  double burst_last_line_time[TOPS_SYNTH_MAX_BURSTS];
-  int n_dc, n_fm;
-  tops_poly dc_list[TOPS_SYNTH_MAX_BURSTS + 4];
-  tops_poly fm_list[TOPS_SYNTH_MAX_BURSTS + 4];
-  int n_sv;
-  double sv_t[32], sv_x[32], sv_y[32], sv_z[32];
-} tops_swath_info;
 
 typedef struct {
   int lines, pixels;

@@ -12,11 +12,14 @@ namespace tops {
 // Thread-local record of the last CUDA error (tops_last_cuda_error()).
 void set_cuda_error(cudaError_t e);
 
+// On failure: record the error, clear the thread's last-error state (so a
+// later, unrelated launch check does not report it again) and return.
 #define TOPS_CUDA_TRY(expr)                      \
   do {                                           \
     cudaError_t _e = (expr);                     \
     if (_e != cudaSuccess) {                     \
       ::tops::set_cuda_error(_e);                \
+      (void)cudaGetLastError();                  \
       return (_e == cudaErrorMemoryAllocation) ? TOPS_E_NOMEM : TOPS_E_CUDA; \
     }                                            \
   } while (0)
@@ -61,6 +64,7 @@ struct ResampleJob {
   double caz[6], crg[6];
   double az_shift;
   const double *az_shift_dev;
+  const double *cpm_dev;  // if set: 6 azimuth then 6 range coefficients
   int s_first_line;
   double dt;
   int row0, nrows;        // master rows [row0, row0+nrows) (0-based in box)

@@ -91,6 +91,8 @@ struct RsShared {
   int grp_lmin, grp_lmax, grp_ring_ok;
   int xw;                        // absolute slave column of ring column 0
   double ref_kt, ref_tref, ref_fdc;
+  double caz[6], crg[6];         // offset polynomials of this job
+  double shift;                  // azimuth shift of this job
 };
 
 // Deramp + demodulation phase (DerampAndResample.cu:151-158), FP64.
@@ -195,12 +197,29 @@ __global__ void __launch_bounds__(RS_NT, 2)
   const int cN = min(RS_TW, mpix - c0);
   const int r_begin = J.row0 + seg * J.seg_rows;
   const int r_end = min(r_begin + J.seg_rows, J.row0 + J.nrows);
-  const double shift = J.az_shift_dev ? *J.az_shift_dev : J.az_shift;
-
-  // ---- per-strip setup: normalised columns, ring window
+  // ---- per-strip setup: coefficients, normalised columns, ring window
+  if (tid < 12) {
+    const double v = J.cpm_dev ? J.cpm_dev[tid] : (tid < 6 ? J.caz[tid] : J.crg[tid - 6]);
+    if (tid < 6)
+      S.caz[tid] = v;
+    else
+      S.crg[tid - 6] = v;
+  }
+  if (tid == 12) {
+    double sh = J.az_shift;
+    if (J.az_shift_dev) {
+      // a device-provided ESD shift above 100 px is invalid and reset to 0,
+      // as the reference driver does (Func.cpp:2612-2621)
+      sh = *J.az_shift_dev;
+      if (!(fabs(sh) <= 100.0)) sh = 0.0;
+    }
+    S.shift = sh;
+  }
   for (int c = tid; c < RS_TW; c += RS_NT)
     S.phat[c] = ((double)(c0 + min(c, cN - 1)) - J.midP) * J.invP;
   if (tid < RS_FR) S.ring_row[tid] = INT32_MIN;
+  __syncthreads();
+  const double shift = S.shift;
   if (tid == 0) {
     // range position at the segment corners and edge midpoints
     double pmin = 1e300, pmax = -1e300;
@@ -210,7 +229,7 @@ __global__ void __launch_bounds__(RS_NT, 2)
       for (int b = 0; b < 3; b++) {
         int cc = (b == 0) ? c0 : (b == 1 ? c0 + (cN - 1) / 2 : c0 + cN - 1);
         double P = ((double)cc - J.midP) * J.invP;
-        const double *c = J.crg;
+        const double *c = S.crg;
         double x = c[0] + c[1] * L + c[2] * P + c[3] * L * L + c[4] * L * P + c[5] * P * P;
         pmin = fmin(pmin, x);
         pmax = fmax(pmax, x);
@@ -258,7 +277,7 @@ __global__ void __launch_bounds__(RS_NT, 2)
       if (r >= gr || c >= cN) continue;
       double L = S.row_lhat[r];
       double P = S.phat[c];
-      const double *ca = J.caz, *cr = J.crg;
+      const double *ca = S.caz, *cr = S.crg;
       double y = ca[0] + ca[1] * L + ca[2] * P + ca[3] * L * L + ca[4] * L * P + ca[5] * P * P;
       y += shift;
       double x = cr[0] + cr[1] * L + cr[2] * P + cr[3] * L * L + cr[4] * L * P + cr[5] * P * P;
@@ -563,7 +582,7 @@ __global__ void __launch_bounds__(RS_NT, 2)
         }
       }
       // store: vectorised when the 4 outputs are in the strip and aligned
-      float2 *orow = J.out + (long)mr * J.out_pitch + c0 + cg;
+      float2 *orow = J.out + (long)(mr - J.row0) * J.out_pitch + c0 + cg;
       if (cg + 4 <= cN && ((reinterpret_cast<uintptr_t>(orow) & 15) == 0)) {
         float4 *o4 = reinterpret_cast<float4 *>(orow);
         o4[0] = make_float4(res[0].x, res[0].y, res[1].x, res[1].y);
@@ -659,6 +678,7 @@ int fill_resample_job(const tops_resample_job &u, ResampleJob &J) {
   }
   J.az_shift = u.az_shift;
   J.az_shift_dev = u.az_shift_dev;
+  J.cpm_dev = u.cpm_dev;
   J.s_first_line = u.s_first_line;
   J.dt = u.dt;
   J.row0 = u.out_rows < 0 ? 0 : u.out_row0;

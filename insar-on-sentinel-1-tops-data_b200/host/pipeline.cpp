@@ -1,0 +1,644 @@
+// pipeline.cpp -- burst-pair processing of one sub-swath (tops_pipeline.h).
+//
+// tops_pair_*: device-resident plan.  Stage order and per-burst semantics
+// follow the reference drivers (Func.cpp:2215-2297, 2326-2406, 2496-2763);
+// every stage is one batched launch over the bursts and the offset
+// polynomials / ESD shifts stay on the device between stages.
+//
+// tops_plain_pair: the same drivers, per burst, through the reference-
+// compatible entry points with host buffers.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <string.h>
+
+#include <vector>
+
+#include "tops_pipeline.h"
+
+namespace {
+
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+struct OrbitFit {
+  double cx[8], cy[8], cz[8];
+  int n = 0;
+};
+
+int fit_orbit(const tops_swath_info &s, OrbitFit &f) {
+  return tops_polyfit_orbit(s.n_sv, s.sv_t, s.sv_x, s.sv_y, s.sv_z, f.cx, f.cy, f.cz, &f.n);
+}
+
+struct Deramp {
+  std::vector<double> dc, fm, tref, kt;
+};
+
+int deramp_of(const tops_swath_info &s, const OrbitFit &f, Deramp &d) {
+  const size_t n = (size_t)s.n_bursts * s.samples_per_burst;
+  d.dc.resize(n);
+  d.fm.resize(n);
+  d.tref.resize(n);
+  d.kt.resize(n);
+  tops_deramp_desc x;
+  memset(&x, 0, sizeof(x));
+  x.n_bursts = s.n_bursts;
+  x.samples_per_burst = s.samples_per_burst;
+  x.lines_per_burst = s.lines_per_burst;
+  x.first_valid_pixel = s.first_valid_pixel;
+  x.slr_time_first_pixel = s.slr_time;
+  x.range_pixel_spacing = s.range_spacing;
+  x.azimuth_time_interval = s.dt;
+  x.first_line_time = s.first_line_time;
+  x.last_line_time = s.last_line_time;
+  x.steering_rate_deg = s.steering_rate_deg;
+  x.wavelength = s.wavelength;
+  x.burst_first_line_time = s.burst_first_line_time;
+  x.burst_last_line_time = s.burst_last_line_time;
+  x.dc_list = s.dc_list;
+  x.n_dc = s.n_dc;
+  x.fm_list = s.fm_list;
+  x.n_fm = s.n_fm;
+  x.orb_cx = f.cx;
+  x.orb_cy = f.cy;
+  x.orb_cz = f.cz;
+  x.orb_ncoef = f.n;
+  x.orb_mid_time = s.sv_t[s.n_sv / 2];
+  return tops_deramp_params(&x, d.dc.data(), d.fm.data(), d.tref.data(), d.kt.data());
+}
+
+#define P_TRY(expr)               \
+  do {                            \
+    int _s = (expr);              \
+    if (_s != TOPS_OK) return _s; \
+  } while (0)
+
+#define P_CUDA(expr)                                                              \
+  do {                                                                            \
+    cudaError_t _e = (expr);                                                      \
+    if (_e != cudaSuccess) {                                                      \
+      (void)cudaGetLastError();                                                   \
+      return _e == cudaErrorMemoryAllocation ? TOPS_E_NOMEM : TOPS_E_CUDA;        \
+    }                                                                             \
+  } while (0)
+
+}  // namespace
+
+struct tops_pair {
+  tops_swath_info m, s;
+  tops_pair_opts o;
+  int nb, L, W, dem_lines, dem_pixels;
+  OrbitFit fm, fs;
+  Deramp dm, ds;
+  std::vector<float> kaz, krg;
+  std::vector<int> ov;
+  std::vector<int> ov_off;  // line offset of each overlap in the band buffers
+  int ov_total = 0;
+  double spec_sep = 0;
+  // device memory
+  size_t slc_pitch = 0, cplx_pitch = 0, coh_pitch = 0, dem_pitch = 0;
+  char *d_master = nullptr, *d_slave = nullptr, *d_reslave = nullptr, *d_res_esd = nullptr;
+  char *d_fwd = nullptr, *d_back = nullptr;  // overlap bands when !reslave_full
+  float *d_coh = nullptr, *d_dem = nullptr;
+  double *d_kt = nullptr, *d_tref = nullptr, *d_fdc = nullptr;
+  double *d_cpm = nullptr, *d_shift = nullptr, *d_sums = nullptr;
+  int *d_status = nullptr;
+  void *d_geo_scratch = nullptr, *d_esd_scratch = nullptr;
+  size_t geo_scratch = 0, esd_scratch = 0;
+  tops_lut_dev *lut = nullptr;
+  std::vector<tops_geo_job> geo;
+  bool dem_set = false;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  cudaStream_t capture_stream = nullptr;  // private: the legacy stream cannot be captured
+  std::vector<void *> allocs;
+  int n_launches = 0;
+
+  int alloc(void **p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
+    if (e != cudaSuccess) return e == cudaErrorMemoryAllocation ? TOPS_E_NOMEM : TOPS_E_CUDA;
+    allocs.push_back(*p);
+    return TOPS_OK;
+  }
+  ~tops_pair() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (capture_stream) cudaStreamDestroy(capture_stream);
+    for (void *p : allocs) cudaFree(p);
+    if (lut) tops_lut_destroy(lut);
+  }
+};
+
+extern "C" {
+
+int tops_pair_opts_default(tops_pair_opts *o) {
+  if (!o) return TOPS_E_INVALID;
+  o->win_rg = 10;
+  o->win_az = 3;
+  o->esd_threshold = 0.3f;
+  o->reslave_full = 1;
+  o->burst0_deramp_rows = 1;
+  return TOPS_OK;
+}
+
+static void pitches(int W, int dem_pixels, size_t &slc, size_t &cplx, size_t &coh, size_t &dem) {
+  slc = align_up((size_t)W * 4, 512);
+  cplx = align_up((size_t)W * 8, 512);
+  coh = align_up((size_t)W * 4, 512);
+  dem = align_up((size_t)dem_pixels * 4, 512);
+}
+
+size_t tops_pair_footprint(const tops_swath_info *m, const tops_pair_opts *o, int dem_lines,
+                           int dem_pixels) {
+  if (!m || !o) return 0;
+  const int nb = m->n_bursts, L = m->lines_per_burst, W = m->samples_per_burst;
+  size_t slc, cplx, coh, dem;
+  pitches(W, dem_pixels, slc, cplx, coh, dem);
+  const size_t lines = (size_t)nb * L;
+  size_t b = 2 * lines * slc + lines * cplx + lines * coh + (size_t)dem_lines * dem;
+  if (o->reslave_full) {
+    b += lines * cplx;
+  } else {
+    int ov[TOPS_MAX_BURSTS], tot = 0, mx = 0;
+    tops_overlap_size(nb, m->burst_first_line_time, m->burst_last_line_time, m->dt, ov, &tot,
+                      &mx);
+    b += 2 * (size_t)(tot > 0 ? tot : 0) * cplx;
+  }
+  b += 3 * sizeof(double) * (size_t)nb * W;           // deramp rows
+  b += (size_t)nb * 4096 * 33 * sizeof(double);       // geocoreg partials (upper bound)
+  b += (size_t)nb * (W / 224 + 1) * 8 * 16;           // ESD partials (upper bound)
+  b += 2 * sizeof(float) * 2048 * 12 + 2048 * 4 + 4096;
+  return b;
+}
+
+int tops_pair_create(const tops_swath_info *m, const tops_swath_info *s, const tops_pair_opts *o,
+                     int dem_lines, int dem_pixels, tops_pair **out) {
+  if (!m || !s || !o || !out) return TOPS_E_INVALID;
+  const int nb = m->n_bursts, L = m->lines_per_burst, W = m->samples_per_burst;
+  if (nb < 1 || nb > TOPS_MAX_BURSTS || L < 16 || W < 16 || s->n_bursts != nb ||
+      s->lines_per_burst != L || s->samples_per_burst != W || dem_lines <= 0 || dem_pixels <= 0 ||
+      m->n_sv < 3 || s->n_sv < 3)
+    return TOPS_E_INVALID;
+  tops_pair *P = new tops_pair();
+  P->m = *m;
+  P->s = *s;
+  P->o = *o;
+  P->nb = nb;
+  P->L = L;
+  P->W = W;
+  P->dem_lines = dem_lines;
+  P->dem_pixels = dem_pixels;
+  int st = TOPS_OK;
+  auto fail = [&](int e) {
+    delete P;
+    return e;
+  };
+  // host precomputes (reference Main.cpp:57-76, Func.cpp:2510-2555)
+  if ((st = fit_orbit(*m, P->fm)) || (st = fit_orbit(*s, P->fs))) return fail(st);
+  if ((st = deramp_of(*m, P->fm, P->dm)) || (st = deramp_of(*s, P->fs, P->ds))) return fail(st);
+  P->kaz.resize(2048 * 12);
+  P->krg.resize(2048 * 12);
+  if ((st = tops_lut(12, m->prf, m->az_bandwidth, 2 * m->rsr, P->kaz.data(), P->krg.data())))
+    return fail(st);
+  if (nb > 1) {
+    P->ov.resize(nb - 1);
+    int tot = 0, mx = 0;
+    if ((st = tops_overlap_size(nb, m->burst_first_line_time, m->burst_last_line_time, m->dt,
+                                P->ov.data(), &tot, &mx)))
+      return fail(st);
+    for (int v : P->ov)
+      if (v < 1 || v >= L) return fail(TOPS_E_INVALID);
+    P->ov_off.resize(nb - 1);
+    int off = 0;
+    for (int i = 0; i < nb - 1; i++) {
+      P->ov_off[i] = off;
+      off += P->ov[i];
+    }
+    P->ov_total = off;
+  }
+  P->spec_sep = tops_spectral_sep(nb, W, L, m->dt, P->dm.kt.data());
+  // device buffers
+  pitches(W, dem_pixels, P->slc_pitch, P->cplx_pitch, P->coh_pitch, P->dem_pitch);
+  const size_t lines = (size_t)nb * L;
+  void *v;
+#define P_ALLOC(dst, bytes)                     \
+  do {                                          \
+    if ((st = P->alloc(&v, (bytes)))) return fail(st); \
+    dst = reinterpret_cast<decltype(dst)>(v);   \
+  } while (0)
+  P_ALLOC(P->d_master, lines * P->slc_pitch);
+  P_ALLOC(P->d_slave, lines * P->slc_pitch);
+  if (o->reslave_full) {
+    P_ALLOC(P->d_reslave, lines * P->cplx_pitch);
+  } else if (nb > 1) {
+    P_ALLOC(P->d_fwd, (size_t)P->ov_total * P->cplx_pitch);
+    P_ALLOC(P->d_back, (size_t)P->ov_total * P->cplx_pitch);
+  }
+  P_ALLOC(P->d_res_esd, lines * P->cplx_pitch);
+  P_ALLOC(P->d_coh, lines * P->coh_pitch);
+  P_ALLOC(P->d_dem, (size_t)dem_lines * P->dem_pitch);
+  P_ALLOC(P->d_kt, sizeof(double) * lines / L * W);
+  P_ALLOC(P->d_tref, sizeof(double) * lines / L * W);
+  P_ALLOC(P->d_fdc, sizeof(double) * lines / L * W);
+  P_ALLOC(P->d_cpm, sizeof(double) * 12 * nb);
+  P_ALLOC(P->d_status, sizeof(int) * nb);
+  P_ALLOC(P->d_shift, sizeof(double) * (nb > 1 ? nb - 1 : 1));
+  P_ALLOC(P->d_sums, sizeof(double) * 2 * (nb > 1 ? nb - 1 : 1));
+  P->geo_scratch = (size_t)nb * 4096 * 33 * sizeof(double);
+  P_ALLOC(P->d_geo_scratch, P->geo_scratch);
+#undef P_ALLOC
+  // slave deramp rows (Func.cpp:2383 passes burst 0's rows for every burst)
+  if (cudaMemcpy(P->d_kt, P->ds.kt.data(), sizeof(double) * nb * W, cudaMemcpyHostToDevice) ||
+      cudaMemcpy(P->d_tref, P->ds.tref.data(), sizeof(double) * nb * W, cudaMemcpyHostToDevice) ||
+      cudaMemcpy(P->d_fdc, P->ds.dc.data(), sizeof(double) * nb * W, cudaMemcpyHostToDevice))
+    return fail(TOPS_E_CUDA);
+  if ((st = tops_lut_create(P->kaz.data(), P->krg.data(), &P->lut))) return fail(st);
+  // ESD scratch
+  if (nb > 1) {
+    std::vector<tops_esd_overlap> ovs(nb - 1);
+    for (int i = 0; i < nb - 1; i++) {
+      tops_esd_overlap &e = ovs[i];
+      e.mF = e.mB = P->d_master;
+      e.sF = e.sB = P->d_res_esd;
+      e.m_pitch = P->slc_pitch;
+      e.s_pitch = P->cplx_pitch;
+      e.lines = P->ov[i];
+      e.pixels = W;
+      e.spec_sep = P->spec_sep;
+      e.dt = m->dt;
+    }
+    P->esd_scratch = tops_esd_scratch_bytes(ovs.data(), nb - 1);
+    void *sp;
+    if ((st = P->alloc(&sp, P->esd_scratch))) return fail(st);
+    P->d_esd_scratch = sp;
+  }
+  *out = P;
+  return TOPS_OK;
+}
+
+int tops_pair_destroy(tops_pair *p) {
+  delete p;
+  return TOPS_OK;
+}
+
+int tops_pair_set_dem(tops_pair *P, const float *dem, double lat0, double lon0, double dlat,
+                      double dlon, const tops_dem_window *win, void *stream) {
+  if (!P || !dem || !win) return TOPS_E_INVALID;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  P_CUDA(cudaMemcpy2DAsync(P->d_dem, P->dem_pitch, dem, (size_t)P->dem_pixels * 4,
+                           (size_t)P->dem_pixels * 4, P->dem_lines, cudaMemcpyHostToDevice, st));
+  const int nb = P->nb, L = P->L, W = P->W;
+  P->geo.assign(nb, tops_geo_job());
+  for (int b = 0; b < nb; b++) {
+    const tops_dem_window &w = win[b];
+    if (w.row0 < 0 || w.col0 < 0 || w.rows < 1 || w.cols < 1 || w.row0 + w.rows > P->dem_lines ||
+        w.col0 + w.cols > P->dem_pixels)
+      return TOPS_E_INVALID;
+    tops_geo_job &g = P->geo[b];
+    memset(&g, 0, sizeof(g));
+    g.dem = reinterpret_cast<const float *>(reinterpret_cast<const char *>(P->d_dem) +
+                                            (size_t)w.row0 * P->dem_pitch) + w.col0;
+    g.dem_pitch = P->dem_pitch;
+    g.dem_lines = w.rows;
+    g.dem_pixels = w.cols;
+    g.lat0 = lat0 - w.row0 * dlat;
+    g.lon0 = lon0 + w.col0 * dlon;
+    g.dlat = dlat;
+    g.dlon = dlon;
+    g.nodata = -32768.0;
+    // master burst box (Func.cpp:2228-2231)
+    g.xmin = 0;
+    g.xmax = W - 1;
+    g.ymin = b * L;
+    g.ymax = (b + 1) * L - 1;
+    const tops_swath_info *sw[2] = {&P->m, &P->s};
+    const OrbitFit *of[2] = {&P->fm, &P->fs};
+    for (int k = 0; k < 2; k++) {
+      g.dt[k] = sw[k]->dt;
+      g.first_line_time[k] = sw[k]->burst_first_line_time[b];
+      g.slr_time[k] = sw[k]->slr_time;
+      g.range_spacing[k] = sw[k]->range_spacing;
+      g.mid_time[k] = sw[k]->sv_t[sw[k]->n_sv / 2];
+      // initial azimuth time: burst centre (Func.cpp:2234-2235)
+      g.azi_init[k] = 0.5 * (sw[k]->burst_first_line_time[b] + sw[k]->burst_last_line_time[b]);
+      g.line_offset[k] = b * L;
+      g.ncoef[k] = of[k]->n;
+      for (int i = 0; i < of[k]->n; i++) {
+        g.coef[k][0][i] = of[k]->cx[i];
+        g.coef[k][1][i] = of[k]->cy[i];
+        g.coef[k][2][i] = of[k]->cz[i];
+      }
+    }
+    g.cpm_dev = P->d_cpm + 12 * b;
+    g.status_dev = P->d_status + b;
+  }
+  if (tops_geocoreg_scratch_bytes(P->geo.data(), nb) > P->geo_scratch) return TOPS_E_INVALID;
+  P->dem_set = true;
+  return TOPS_OK;
+}
+
+int tops_pair_upload(tops_pair *P, const void *master, const void *slave, void *stream) {
+  if (!P || !master || !slave) return TOPS_E_INVALID;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const size_t row = (size_t)P->W * 4, lines = (size_t)P->nb * P->L;
+  P_CUDA(cudaMemcpy2DAsync(P->d_master, P->slc_pitch, master, row, row, lines,
+                           cudaMemcpyHostToDevice, st));
+  P_CUDA(cudaMemcpy2DAsync(P->d_slave, P->slc_pitch, slave, row, row, lines,
+                           cudaMemcpyHostToDevice, st));
+  return TOPS_OK;
+}
+
+static tops_resample_job base_job(const tops_pair *P, int b) {
+  tops_resample_job j;
+  memset(&j, 0, sizeof(j));
+  const int L = P->L, W = P->W;
+  j.slave = P->d_slave + (size_t)b * L * P->slc_pitch;
+  j.slave_pitch = P->slc_pitch;
+  const int row = P->o.burst0_deramp_rows ? 0 : b;
+  j.kt = P->d_kt + (size_t)row * W;
+  j.tref = P->d_tref + (size_t)row * W;
+  j.fdc = P->d_fdc + (size_t)row * W;
+  j.mbox[0] = 0;
+  j.mbox[1] = W - 1;
+  j.mbox[2] = b * L;
+  j.mbox[3] = (b + 1) * L - 1;
+  j.sbox[0] = 0;
+  j.sbox[1] = W - 1;
+  j.sbox[2] = b * L;
+  j.sbox[3] = (b + 1) * L - 1;
+  j.cpm_dev = P->d_cpm + 12 * b;
+  j.s_first_line = b * L;
+  j.dt = P->s.dt;
+  j.out_pitch = P->cplx_pitch;
+  return j;
+}
+
+int tops_pair_run(tops_pair *P, void *stream) {
+  if (!P || !P->dem_set) return TOPS_E_INVALID;
+  const int nb = P->nb, L = P->L, W = P->W;
+  int launches = 0;
+  // 1. geometric coregistration of every burst (2 kernels)
+  P_TRY(tops_geocoreg(P->geo.data(), nb, P->d_geo_scratch, P->geo_scratch, stream));
+  launches += 2;
+  // 2. resample without shift: full ReSlave, or only the overlap bands
+  std::vector<tops_resample_job> jobs;
+  if (P->o.reslave_full) {
+    for (int b = 0; b < nb; b++) {
+      tops_resample_job j = base_job(P, b);
+      j.out = P->d_reslave + (size_t)b * L * P->cplx_pitch;
+      j.out_rows = -1;
+      jobs.push_back(j);
+    }
+  } else {
+    for (int i = 0; i < nb - 1; i++) {
+      tops_resample_job f = base_job(P, i);   // forward band: end of burst i
+      f.out = P->d_fwd + (size_t)P->ov_off[i] * P->cplx_pitch;
+      f.out_row0 = L - P->ov[i];
+      f.out_rows = P->ov[i];
+      jobs.push_back(f);
+      tops_resample_job k = base_job(P, i + 1);   // backward band: start of burst i+1
+      k.out = P->d_back + (size_t)P->ov_off[i] * P->cplx_pitch;
+      k.out_row0 = 0;
+      k.out_rows = P->ov[i];
+      jobs.push_back(k);
+    }
+  }
+  if (!jobs.empty()) {
+    P_TRY(tops_resample(P->lut, jobs.data(), (int)jobs.size(), stream));
+    launches += 1;
+  }
+  // 3. ESD over the overlaps (shifts stay on the device)
+  if (nb > 1) {
+    std::vector<tops_esd_overlap> ovs(nb - 1);
+    for (int i = 0; i < nb - 1; i++) {
+      tops_esd_overlap &e = ovs[i];
+      const size_t fl = (size_t)(i + 1) * L - P->ov[i], bl = (size_t)(i + 1) * L;
+      e.mF = P->d_master + fl * P->slc_pitch;
+      e.mB = P->d_master + bl * P->slc_pitch;
+      e.m_pitch = P->slc_pitch;
+      if (P->o.reslave_full) {
+        e.sF = P->d_reslave + fl * P->cplx_pitch;
+        e.sB = P->d_reslave + bl * P->cplx_pitch;
+      } else {
+        e.sF = P->d_fwd + (size_t)P->ov_off[i] * P->cplx_pitch;
+        e.sB = P->d_back + (size_t)P->ov_off[i] * P->cplx_pitch;
+      }
+      e.s_pitch = P->cplx_pitch;
+      e.lines = P->ov[i];
+      e.pixels = W;
+      e.spec_sep = P->spec_sep;
+      e.dt = P->m.dt;
+    }
+    P_TRY(tops_esd(ovs.data(), nb - 1, P->o.win_az, P->o.win_rg, P->o.esd_threshold, P->d_shift,
+                   P->d_sums, P->d_esd_scratch, P->esd_scratch, stream));
+    launches += 2;
+  }
+  // 4. resample with the ESD shift of the preceding overlap (first burst
+  //    uncorrected, Func.cpp:2653-2702)
+  jobs.clear();
+  for (int b = 0; b < nb; b++) {
+    tops_resample_job j = base_job(P, b);
+    j.out = P->d_res_esd + (size_t)b * L * P->cplx_pitch;
+    j.out_rows = -1;
+    if (b > 0) j.az_shift_dev = P->d_shift + (b - 1);
+    j.dt = P->m.dt;   // DerampDemodResample_ESD gets the master's interval (Func.cpp:2704)
+    jobs.push_back(j);
+  }
+  P_TRY(tops_resample(P->lut, jobs.data(), nb, stream));
+  launches += 1;
+  // 5. coherence of master vs ReSlaveESD
+  std::vector<tops_coh_job> cj(nb);
+  for (int b = 0; b < nb; b++) {
+    tops_coh_job &c = cj[b];
+    c.master = P->d_master + (size_t)b * L * P->slc_pitch;
+    c.master_pitch = P->slc_pitch;
+    c.slave = P->d_res_esd + (size_t)b * L * P->cplx_pitch;
+    c.slave_pitch = P->cplx_pitch;
+    c.coh = reinterpret_cast<float *>(reinterpret_cast<char *>(P->d_coh) +
+                                      (size_t)b * L * P->coh_pitch);
+    c.coh_pitch = P->coh_pitch;
+    c.lines = L;
+    c.pixels = W;
+  }
+  P_TRY(tops_coherence(cj.data(), nb, P->o.win_rg, P->o.win_az, stream));
+  launches += 1;
+  P->n_launches = launches;
+  return TOPS_OK;
+}
+
+int tops_pair_run_graph(tops_pair *P, void *stream) {
+  if (!P) return TOPS_E_INVALID;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (!P->graph_exec) {
+    // one eager run first: it sets per-kernel attributes outside the capture
+    P_TRY(tops_pair_run(P, stream));
+    if (!P->capture_stream)
+      P_CUDA(cudaStreamCreateWithFlags(&P->capture_stream, cudaStreamNonBlocking));
+    cudaStream_t cs = P->capture_stream;
+    P_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    int s = tops_pair_run(P, cs);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(cs, &g);
+    if (s != TOPS_OK) {
+      if (g) cudaGraphDestroy(g);
+      return s;
+    }
+    P_CUDA(e);
+    P->graph = g;
+    P_CUDA(cudaGraphInstantiate(&P->graph_exec, g, 0));
+  }
+  P_CUDA(cudaGraphLaunch(P->graph_exec, st));
+  return TOPS_OK;
+}
+
+int tops_pair_download(tops_pair *P, void *reslave, void *reslave_esd, float *coh, double *cpm,
+                       double *shifts, void *stream) {
+  if (!P) return TOPS_E_INVALID;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const size_t lines = (size_t)P->nb * P->L, W = P->W;
+  if (reslave) {
+    if (!P->o.reslave_full) return TOPS_E_INVALID;
+    P_CUDA(cudaMemcpy2DAsync(reslave, W * 8, P->d_reslave, P->cplx_pitch, W * 8, lines,
+                             cudaMemcpyDeviceToHost, st));
+  }
+  if (reslave_esd)
+    P_CUDA(cudaMemcpy2DAsync(reslave_esd, W * 8, P->d_res_esd, P->cplx_pitch, W * 8, lines,
+                             cudaMemcpyDeviceToHost, st));
+  if (coh)
+    P_CUDA(cudaMemcpy2DAsync(coh, W * 4, P->d_coh, P->coh_pitch, W * 4, lines,
+                             cudaMemcpyDeviceToHost, st));
+  if (cpm)
+    P_CUDA(cudaMemcpyAsync(cpm, P->d_cpm, sizeof(double) * 12 * P->nb, cudaMemcpyDeviceToHost, st));
+  if (shifts && P->nb > 1)
+    P_CUDA(cudaMemcpyAsync(shifts, P->d_shift, sizeof(double) * (P->nb - 1),
+                           cudaMemcpyDeviceToHost, st));
+  return TOPS_OK;
+}
+
+int tops_pair_buffers_get(const tops_pair *P, tops_pair_buffers *b) {
+  if (!P || !b) return TOPS_E_INVALID;
+  b->master = P->d_master;
+  b->slave = P->d_slave;
+  b->reslave = P->d_reslave;
+  b->reslave_esd = P->d_res_esd;
+  b->coh = P->d_coh;
+  b->cpm = P->d_cpm;
+  b->shifts = P->d_shift;
+  b->geo_status = P->d_status;
+  b->slc_pitch = P->slc_pitch;
+  b->cplx_pitch = P->cplx_pitch;
+  b->coh_pitch = P->coh_pitch;
+  b->n_bursts = P->nb;
+  b->lines = P->L;
+  b->samples = P->W;
+  b->n_launches = P->n_launches;
+  return TOPS_OK;
+}
+
+// ------------------------------------------------------------ plain form
+int tops_plain_pair(const tops_swath_info *m, const tops_swath_info *s, const tops_pair_opts *o,
+                    const int *dem_int, int dem_lines, int dem_pixels, double lat0, double lon0,
+                    double dlat, double dlon, const tops_dem_window *win, const void *master_slc,
+                    const void *slave_slc, void *reslave, void *reslave_esd, float *coh,
+                    double *cpm, double *shifts) {
+  if (!m || !s || !o || !dem_int || !win || !master_slc || !slave_slc || !reslave ||
+      !reslave_esd || !coh)
+    return TOPS_E_INVALID;
+  const int nb = m->n_bursts, L = m->lines_per_burst, W = m->samples_per_burst;
+  OrbitFit fm, fs;
+  Deramp dm, ds;
+  P_TRY(fit_orbit(*m, fm));
+  P_TRY(fit_orbit(*s, fs));
+  P_TRY(deramp_of(*m, fm, dm));
+  P_TRY(deramp_of(*s, fs, ds));
+  std::vector<float> kaz(2048 * 12), krg(2048 * 12);
+  P_TRY(tops_lut(12, m->prf, m->az_bandwidth, 2 * m->rsr, kaz.data(), krg.data()));
+  std::vector<double> az(6 * nb), rg(6 * nb);
+  std::vector<double> mt(m->sv_t, m->sv_t + m->n_sv), st_(s->sv_t, s->sv_t + s->n_sv);
+  std::vector<int> demw;
+  // GeometricCoreg (Func.cpp:2225-2291)
+  for (int b = 0; b < nb; b++) {
+    const tops_dem_window &w = win[b];
+    demw.resize((size_t)w.rows * w.cols);
+    for (int r = 0; r < w.rows; r++)
+      memcpy(&demw[(size_t)r * w.cols], dem_int + (size_t)(w.row0 + r) * dem_pixels + w.col0,
+             sizeof(int) * w.cols);
+    P_TRY(GeoCoreg_warp_cuda(
+        b, b, 0, W - 1, b * L, (b + 1) * L - 1, dlat, dlon, w.rows, w.cols, &az[6 * b],
+        &rg[6 * b], lat0 - w.row0 * dlat, lon0 + w.col0 * dlon, -32768, m->dt, s->dt,
+        m->wavelength, L, L, m->burst_first_line_time[b], s->burst_first_line_time[b], W, W,
+        mt.data(), st_.data(), m->n_sv, fm.n, s->n_sv, fs.n, m->slr_time, s->slr_time,
+        m->range_spacing, s->range_spacing, false, false, demw.data(), fm.cx, fm.cy, fm.cz, fs.cx,
+        fs.cy, fs.cz, 0.5 * (m->burst_first_line_time[b] + m->burst_last_line_time[b]),
+        0.5 * (s->burst_first_line_time[b] + s->burst_last_line_time[b])));
+  }
+  if (cpm)
+    for (int b = 0; b < nb; b++)
+      for (int i = 0; i < 6; i++) {
+        cpm[12 * b + i] = az[6 * b + i];
+        cpm[12 * b + 6 + i] = rg[6 * b + i];
+      }
+  // DerampAndResample (Func.cpp:2351-2393)
+  const size_t bl = (size_t)L * W;
+  auto slave_b = [&](int b) {
+    return const_cast<int16_t *>(static_cast<const int16_t *>(slave_slc) + 2 * b * bl);
+  };
+  auto master_b = [&](int b) {
+    return const_cast<int16_t *>(static_cast<const int16_t *>(master_slc) + 2 * b * bl);
+  };
+  float *rs = static_cast<float *>(reslave), *re = static_cast<float *>(reslave_esd);
+  for (int b = 0; b < nb; b++) {
+    int MB[4] = {0, W - 1, b * L, (b + 1) * L - 1}, SB[4] = {0, W - 1, b * L, (b + 1) * L - 1};
+    const int row = o->burst0_deramp_rows ? 0 : b;
+    P_TRY(DerampDemodResample(slave_b(b), &az[6 * b], &rg[6 * b], 0.0, rs + 2 * b * bl,
+                              kaz.data(), krg.data(), b, W, L, MB, SB, L, W, s->dt,
+                              ds.kt.data() + (size_t)row * W, ds.tref.data() + (size_t)row * W,
+                              ds.dc.data() + (size_t)row * W, 12));
+  }
+  // ESDAndCoh (Func.cpp:2510-2727)
+  std::vector<double> sh(nb > 1 ? nb - 1 : 1, 0.0);
+  if (nb > 1) {
+    std::vector<int> ov(nb - 1);
+    int tot = 0, mx = 0;
+    P_TRY(tops_overlap_size(nb, m->burst_first_line_time, m->burst_last_line_time, m->dt,
+                            ov.data(), &tot, &mx));
+    const double ss = tops_spectral_sep(nb, W, L, m->dt, dm.kt.data());
+    std::vector<int16_t> mF((size_t)tot * W * 2), mB((size_t)tot * W * 2);
+    std::vector<float> sF((size_t)tot * W * 2), sB((size_t)tot * W * 2);
+    size_t off = 0;
+    for (int i = 0; i < nb - 1; i++) {
+      const size_t f = (size_t)(i + 1) * L - ov[i], k = (size_t)(i + 1) * L, n = (size_t)ov[i] * W;
+      memcpy(&mF[2 * off * W], static_cast<const int16_t *>(master_slc) + 2 * f * W, 4 * n);
+      memcpy(&mB[2 * off * W], static_cast<const int16_t *>(master_slc) + 2 * k * W, 4 * n);
+      memcpy(&sF[2 * off * W], rs + 2 * f * W, 8 * n);
+      memcpy(&sB[2 * off * W], rs + 2 * k * W, 8 * n);
+      off += ov[i];
+    }
+    P_TRY(EstESDShifts(mF.data(), mB.data(), sF.data(), sB.data(), ov.data(), sh.data(), nb - 1,
+                       tot, W, o->win_az, o->win_rg, mx, o->esd_threshold, ss, m->dt));
+    for (auto &v : sh)
+      if (fabs(v) > 100) v = 0;   // Func.cpp:2612-2621
+    if (shifts) memcpy(shifts, sh.data(), sizeof(double) * (nb - 1));
+  }
+  const int dx = (o->win_rg - 1) / 2, dy = (o->win_az - 1) / 2;
+  for (int b = 0; b < nb; b++) {
+    void *d = nullptr;
+    if (b == 0) {
+      memcpy(re, rs, 8 * bl);
+      d = ResampleFirstBurst(re, W, L);
+      if (!d) return TOPS_E_CUDA;
+      P_TRY(CoherenceEst_ESD(0, 0, W, L, dx, dy, o->win_rg, o->win_az, master_b(0), d, coh));
+    } else {
+      int MB[4] = {0, W - 1, b * L, (b + 1) * L - 1}, SB[4] = {0, W - 1, b * L, (b + 1) * L - 1};
+      const int row = o->burst0_deramp_rows ? 0 : b;
+      d = DerampDemodResample_ESD(slave_b(b), &az[6 * b], &rg[6 * b], sh[b - 1], re + 2 * b * bl,
+                                  kaz.data(), krg.data(), b, W, L, MB, SB, L, W, m->dt,
+                                  ds.kt.data() + (size_t)row * W, ds.tref.data() + (size_t)row * W,
+                                  ds.dc.data() + (size_t)row * W, 12);
+      if (!d) return TOPS_E_CUDA;
+      P_TRY(CoherenceEst(0, b * L, W, L, dx, dy, o->win_rg, o->win_az, master_b(b), d,
+                         coh + b * bl));
+    }
+  }
+  return TOPS_OK;
+}
+
+}  // extern "C"

@@ -121,7 +121,7 @@ class ResampleJob(C.Structure):
         ("kt", C.c_void_p), ("tref", C.c_void_p), ("fdc", C.c_void_p),
         ("mbox", C.c_int * 4), ("sbox", C.c_int * 4),
         ("cpm_az", C.c_double * 6), ("cpm_rg", C.c_double * 6),
-        ("az_shift", C.c_double), ("az_shift_dev", C.c_void_p),
+        ("az_shift", C.c_double), ("az_shift_dev", C.c_void_p), ("cpm_dev", C.c_void_p),
         ("s_first_line", C.c_int), ("dt", C.c_double),
         ("out_row0", C.c_int), ("out_rows", C.c_int),
     ]
@@ -420,3 +420,231 @@ class Scene:
             line_offset=(b * L, b * L),
             coefs=(self.orbit[0], self.orbit[1]),
         )
+
+
+# ------------------------------------------- reference-compatible ABI calls
+def deramp_demod_resample(slave, cpm_az, cpm_rg, az_shift, kaz, krg, s_burst_idx, mbox, sbox,
+                          lines_per_burst, dt, kt, tref, fdc, keep_device=False):
+    """DerampDemodResample / DerampDemodResample_ESD on host arrays.
+
+    slave: int16 [sLines][sPixels][2]; kt/tref/fdc: float64 [SamplesPerBurst].
+    Returns complex64 [mLines][mPixels] (and the device pointer if keep_device)."""
+    slave = np.ascontiguousarray(slave, np.int16)
+    mbox = np.ascontiguousarray(mbox, np.int32)
+    sbox = np.ascontiguousarray(sbox, np.int32)
+    mlin, mpix = int(mbox[3] - mbox[2] + 1), int(mbox[1] - mbox[0] + 1)
+    out = np.zeros((mlin, mpix), np.complex64)
+    caz = np.ascontiguousarray(cpm_az, np.float64)
+    crg = np.ascontiguousarray(cpm_rg, np.float64)
+    kaz = np.ascontiguousarray(kaz, np.float32)
+    krg = np.ascontiguousarray(krg, np.float32)
+    kt, tref, fdc = (np.ascontiguousarray(v, np.float64) for v in (kt, tref, fdc))
+    args = (vptr(slave), ptr(caz, C.c_double), ptr(crg, C.c_double), float(az_shift), vptr(out),
+            ptr(kaz, C.c_float), ptr(krg, C.c_float), int(s_burst_idx), slave.shape[1],
+            slave.shape[0], ptr(mbox, C.c_int), ptr(sbox, C.c_int), int(lines_per_burst),
+            len(kt), float(dt), ptr(kt, C.c_double), ptr(tref, C.c_double),
+            ptr(fdc, C.c_double), kaz.shape[1])
+    if keep_device:
+        d = lib.DerampDemodResample_ESD(*args)
+        if not d:
+            raise TopsError(TOPS_E_CUDA if lib.tops_last_cuda_error() else TOPS_E_INVALID,
+                            "DerampDemodResample_ESD")
+        return out, d
+    check(lib.DerampDemodResample(*args), "DerampDemodResample")
+    return out
+
+
+def resample_first_burst(reslave: np.ndarray):
+    a = np.ascontiguousarray(reslave, np.complex64)
+    d = lib.ResampleFirstBurst(vptr(a), a.shape[1], a.shape[0])
+    if not d:
+        raise TopsError(TOPS_E_CUDA, "ResampleFirstBurst")
+    return d
+
+
+def coherence_est(master, d_slave, win_rg, win_az, esd_variant=False):
+    """CoherenceEst(_ESD): master int16 [Dh][Dw][2] on the host, d_slave a device
+    pointer from deramp_demod_resample(keep_device=True) / resample_first_burst
+    (freed by the call, as in the reference).  Returns float32 [Dh][Dw]."""
+    master = np.ascontiguousarray(master, np.int16)
+    Dh, Dw = master.shape[0], master.shape[1]
+    coh = np.zeros((Dh, Dw), np.float32)
+    f = lib.CoherenceEst_ESD if esd_variant else lib.CoherenceEst
+    check(f(0, 0, Dw, Dh, (win_rg - 1) // 2, (win_az - 1) // 2, win_rg, win_az, vptr(master),
+            C.c_void_p(d_slave), ptr(coh, C.c_float)), "CoherenceEst")
+    return coh
+
+
+def est_esd_shifts(mF, mB, sF, sB, ov, win_az, win_rg, thr, spec_sep, dt):
+    """EstESDShifts on the concatenated overlap bands (host arrays)."""
+    mF, mB = (np.ascontiguousarray(a, np.int16) for a in (mF, mB))
+    sF, sB = (np.ascontiguousarray(a, np.complex64) for a in (sF, sB))
+    ov = np.ascontiguousarray(ov, np.int32)
+    shift = np.zeros(len(ov))
+    check(lib.EstESDShifts(vptr(mF), vptr(mB), vptr(sF), vptr(sB), ptr(ov, C.c_int),
+                           ptr(shift, C.c_double), len(ov), mF.shape[0], mF.shape[1], win_az,
+                           win_rg, int(ov.max()) if len(ov) else 0, float(thr), float(spec_sep),
+                           float(dt)), "EstESDShifts")
+    return shift
+
+
+def geocoreg_warp(dem_int, lat0, lon0, dlat, dlon, xmin, xmax, ymin, ymax, m_burst, s_burst,
+                  lines_per_burst, dt, first_line_time, slr_time, range_spacing, orbit_t,
+                  coefs, azi_init, samples, wavelength=0.05547, nodata=-32768):
+    """GeoCoreg_warp_cuda with its reference argument list (int DEM window).
+
+    orbit_t: (master SV times, slave SV times); coefs: ((cx,cy,cz) master, slave)."""
+    dem_int = np.ascontiguousarray(dem_int, np.int32)
+    az, rg = np.zeros(6), np.zeros(6)
+    mt, st_ = (np.ascontiguousarray(t, np.float64) for t in orbit_t)
+    (mx, my, mz), (sx, sy, sz) = [[np.ascontiguousarray(c, np.float64) for c in cc] for cc in coefs]
+    st = lib.GeoCoreg_warp_cuda(
+        m_burst, s_burst, xmin, xmax, ymin, ymax, dlat, dlon, dem_int.shape[0], dem_int.shape[1],
+        ptr(az, C.c_double), ptr(rg, C.c_double), lat0, lon0, nodata, dt[0], dt[1], wavelength,
+        float(lines_per_burst), float(lines_per_burst), first_line_time[0], first_line_time[1],
+        samples, samples, ptr(mt, C.c_double), ptr(st_, C.c_double), len(mt), len(mx), len(st_),
+        len(sx), slr_time[0], slr_time[1], range_spacing[0], range_spacing[1], False, False,
+        ptr(dem_int, C.c_int), ptr(mx, C.c_double), ptr(my, C.c_double), ptr(mz, C.c_double),
+        ptr(sx, C.c_double), ptr(sy, C.c_double), ptr(sz, C.c_double), azi_init[0], azi_init[1])
+    check(st, "GeoCoreg_warp_cuda")
+    return az, rg
+
+
+# ------------------------------------------------------- burst-pair pipeline
+class PairOpts(C.Structure):
+    _fields_ = [("win_rg", C.c_int), ("win_az", C.c_int), ("esd_threshold", C.c_float),
+                ("reslave_full", C.c_int), ("burst0_deramp_rows", C.c_int)]
+
+
+class DemWindow(C.Structure):
+    _fields_ = [("row0", C.c_int), ("col0", C.c_int), ("rows", C.c_int), ("cols", C.c_int)]
+
+
+class PairBuffers(C.Structure):
+    _fields_ = [("master", C.c_void_p), ("slave", C.c_void_p), ("reslave", C.c_void_p),
+                ("reslave_esd", C.c_void_p), ("coh", C.c_void_p), ("cpm", C.c_void_p),
+                ("shifts", C.c_void_p), ("geo_status", C.c_void_p),
+                ("slc_pitch", C.c_size_t), ("cplx_pitch", C.c_size_t), ("coh_pitch", C.c_size_t),
+                ("n_bursts", C.c_int), ("lines", C.c_int), ("samples", C.c_int),
+                ("n_launches", C.c_int)]
+
+
+_proto("tops_pair_opts_default", C.c_int, [C.POINTER(PairOpts)])
+_proto("tops_pair_footprint", C.c_size_t, [C.POINTER(SwathInfo), C.POINTER(PairOpts), C.c_int,
+                                           C.c_int])
+_proto("tops_pair_create", C.c_int, [C.POINTER(SwathInfo), C.POINTER(SwathInfo),
+                                     C.POINTER(PairOpts), C.c_int, C.c_int, C.POINTER(_vp)])
+_proto("tops_pair_destroy", C.c_int, [_vp])
+_proto("tops_pair_set_dem", C.c_int, [_vp, _fp, C.c_double, C.c_double, C.c_double, C.c_double,
+                                      C.POINTER(DemWindow), _vp])
+_proto("tops_pair_upload", C.c_int, [_vp, _vp, _vp, _vp])
+_proto("tops_pair_run", C.c_int, [_vp, _vp])
+_proto("tops_pair_run_graph", C.c_int, [_vp, _vp])
+_proto("tops_pair_download", C.c_int, [_vp, _vp, _vp, _fp, _dp, _dp, _vp])
+_proto("tops_pair_buffers_get", C.c_int, [_vp, C.POINTER(PairBuffers)])
+_proto("tops_plain_pair", C.c_int, [C.POINTER(SwathInfo), C.POINTER(SwathInfo), C.POINTER(PairOpts),
+                                    _ip, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                    C.c_double, C.POINTER(DemWindow), _vp, _vp, _vp, _vp, _fp, _dp,
+                                    _dp])
+
+
+def pair_opts(**kw) -> PairOpts:
+    o = PairOpts()
+    check(lib.tops_pair_opts_default(C.byref(o)), "tops_pair_opts_default")
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def scene_windows(scene: "Scene", margin: int = 24):
+    nb = scene.cfg.n_bursts
+    w = (DemWindow * nb)()
+    for b in range(nb):
+        r0, c0, nr, nc = scene.dem_window(b, margin)
+        w[b] = DemWindow(r0, c0, nr, nc)
+    return w
+
+
+class Pair:
+    """Device-resident burst-pair plan (tops_pair_*).  `stream` arguments are
+    raw cudaStream_t values (0 = legacy default stream)."""
+
+    def __init__(self, master: SwathInfo, slave: SwathInfo, dem_shape, opts: PairOpts = None):
+        self.opts = opts or pair_opts()
+        self.master, self.slave = master, slave
+        self.nb, self.L, self.W = master.n_bursts, master.lines_per_burst, master.samples_per_burst
+        self.dem_shape = dem_shape
+        h = C.c_void_p()
+        check(lib.tops_pair_create(C.byref(master), C.byref(slave), C.byref(self.opts),
+                                   dem_shape[0], dem_shape[1], C.byref(h)), "tops_pair_create")
+        self._h = h
+
+    @staticmethod
+    def footprint(master: SwathInfo, dem_shape, opts: PairOpts = None) -> int:
+        opts = opts or pair_opts()
+        return lib.tops_pair_footprint(C.byref(master), C.byref(opts), dem_shape[0], dem_shape[1])
+
+    def set_dem(self, dem, lat0, lon0, dlat, dlon, windows, stream=0):
+        dem = np.ascontiguousarray(dem, np.float32)
+        assert dem.shape == tuple(self.dem_shape)
+        self._dem_keep = dem
+        check(lib.tops_pair_set_dem(self._h, ptr(dem, C.c_float), lat0, lon0, dlat, dlon, windows,
+                                    C.c_void_p(stream)), "tops_pair_set_dem")
+
+    def upload(self, master_slc, slave_slc, stream=0):
+        check(lib.tops_pair_upload(self._h, C.c_void_p(master_slc.ctypes.data),
+                                   C.c_void_p(slave_slc.ctypes.data), C.c_void_p(stream)),
+              "tops_pair_upload")
+
+    def run(self, stream=0, graph=False):
+        f = lib.tops_pair_run_graph if graph else lib.tops_pair_run
+        check(f(self._h, C.c_void_p(stream)), "tops_pair_run")
+
+    def download(self, reslave=True, stream=0):
+        n = self.nb * self.L
+        rs = np.zeros((n, self.W), np.complex64) if reslave else None
+        re = np.zeros((n, self.W), np.complex64)
+        coh = np.zeros((n, self.W), np.float32)
+        cpm = np.zeros((self.nb, 12))
+        sh = np.zeros(max(self.nb - 1, 1))
+        check(lib.tops_pair_download(self._h, vptr(rs) if reslave else None, vptr(re),
+                                     ptr(coh, C.c_float), ptr(cpm, C.c_double),
+                                     ptr(sh, C.c_double), C.c_void_p(stream)), "tops_pair_download")
+        return dict(reslave=rs, reslave_esd=re, coh=coh, cpm=cpm, shifts=sh[:self.nb - 1])
+
+    def buffers(self) -> PairBuffers:
+        b = PairBuffers()
+        check(lib.tops_pair_buffers_get(self._h, C.byref(b)), "tops_pair_buffers_get")
+        return b
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.tops_pair_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def plain_pair(scene: "Scene", opts: PairOpts = None, dem_int=None, windows=None):
+    """Reference-shaped per-burst processing (tops_plain_pair) on host arrays."""
+    opts = opts or pair_opts()
+    S = scene
+    n, W = S.shape
+    di = S.dem_info
+    dem_int = np.ascontiguousarray(np.rint(S.dem) if dem_int is None else dem_int, np.int32)
+    windows = windows if windows is not None else scene_windows(S)
+    rs = np.zeros((n, W), np.complex64)
+    re = np.zeros((n, W), np.complex64)
+    coh = np.zeros((n, W), np.float32)
+    cpm = np.zeros((S.cfg.n_bursts, 12))
+    sh = np.zeros(max(S.cfg.n_bursts - 1, 1))
+    check(lib.tops_plain_pair(C.byref(S.swath[0]), C.byref(S.swath[1]), C.byref(opts),
+                              ptr(dem_int, C.c_int), di.lines, di.pixels, di.lat0, di.lon0,
+                              di.dlat, di.dlon, windows, vptr(S.slc[0]), vptr(S.slc[1]), vptr(rs),
+                              vptr(re), ptr(coh, C.c_float), ptr(cpm, C.c_double),
+                              ptr(sh, C.c_double)), "tops_plain_pair")
+    return dict(reslave=rs, reslave_esd=re, coh=coh, cpm=cpm, shifts=sh[:S.cfg.n_bursts - 1])

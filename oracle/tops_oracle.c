@@ -656,7 +656,11 @@ void orc_esd(const int16_t *mF, const int16_t *mB, const float *sF, const float 
         double dre = fr * br + fi * bi, dim = fi * br - fr * bi;
         /* MaskOut (:130-161) */
         if (g < thr || g >= 1) continue;
-        double th = atan2(dim, dre);
+        /* An exactly-zero double difference (slave outside its box) has no
+         * phase; the reference's atan2 then depends on the signs of zero of
+         * its FP32 products.  Both the oracle and the kernel use
+         * atan2(+0, +0) = 0, i.e. the phasor (1, 0). */
+        double th = (dre == 0 && dim == 0) ? 0.0 : atan2(dim, dre);
         ar += cos(th);
         ai += sin(th);
         used++;

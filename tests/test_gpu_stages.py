@@ -1,0 +1,222 @@
+"""GPU parity of the four stages through the reference-compatible C ABI.
+
+Each test runs the CUDA path (libtops_b200.so) and the FP64 oracle on the
+same seeded synthetic inputs and compares at the tolerances of the task:
+resampled SLC within 1e-4 relative complex RMS, coherence within 1e-5
+absolute, ESD shift within 1e-5 px, offsets within 1e-4 px.
+"""
+import numpy as np
+import pytest
+
+from conftest import c64, rel_rms
+
+pytestmark = pytest.mark.gpu
+
+RS_TOL = 1e-4      # relative complex RMS of the resampled SLC
+COH_TOL = 1e-5     # absolute coherence
+ESD_TOL = 1e-5     # pixels
+OFF_TOL = 1e-4     # pixels
+
+
+def oracle_cpm(O, S, b):
+    g = S.geo_args(b)
+    az, rg, st, nv = O.geocoreg(g["dem"], g["lat0"], g["lon0"], g["dlat"], g["dlon"], g["xmin"],
+                                g["xmax"], g["ymin"], g["ymax"], g["dt"], g["first_line_time"],
+                                g["slr_time"], g["range_spacing"], g["mid_time"], g["azi_init"],
+                                g["line_offset"], g["coefs"])
+    assert st == 0 and nv > 100
+    return az, rg
+
+
+def rs_inputs(S, b, cpm, shift=0.0):
+    mb, sb = S.boxes(b)
+    d = S.deramp[1]
+    L = S.cfg.lines_per_burst
+    # the reference passes the burst-0 rows for every burst (Func.cpp:2383)
+    return dict(slave=S.burst(1, b), cpm_az=cpm[0], cpm_rg=cpm[1], az_shift=shift, kaz=S.kaz,
+                krg=S.krg, s_burst_idx=b, mbox=mb, sbox=sb, lines_per_burst=L, dt=S.swath[1].dt,
+                kt=d["kt"][0], tref=d["tref"][0], fdc=d["dc"][0])
+
+
+@pytest.mark.parametrize("b,shift", [(0, 0.0), (1, 0.0), (1, 0.0371)])
+def test_resample_parity(T, O, scene_small, b, shift):
+    S = scene_small
+    cpm = oracle_cpm(O, S, b)
+    kw = rs_inputs(S, b, cpm, shift)
+    gpu = T.deramp_demod_resample(**kw)
+    ref, cnt = O.resample(**kw)
+    assert cnt[2] > 0.9 * ref.size
+    err = rel_rms(gpu, ref)
+    assert err < RS_TOL, err
+
+
+def test_resample_regions(T, O, scene_small):
+    """Polynomial pushing the grid off the slave box: outside -> 0, edge ->
+    the nearest sample, interior -> interpolated (DerampAndResample.cu:383-404)."""
+    S = scene_small
+    az, rg = oracle_cpm(O, S, 0)
+    az = az.copy()
+    rg = rg.copy()
+    az[0] += 120.0   # shift down by 120 lines and right by 200 samples
+    rg[0] += 200.0
+    kw = rs_inputs(S, 0, (az, rg))
+    gpu = T.deramp_demod_resample(**kw)
+    ref, cnt = O.resample(**kw)
+    assert cnt[0] > 1000 and cnt[1] > 1000 and cnt[2] > 1000
+    assert rel_rms(gpu, ref) < RS_TOL
+    zero = np.abs(ref) == 0
+    assert np.all(gpu[zero] == 0)
+
+
+def test_resample_nonuniform_bins(T, O, scene_small):
+    """Azimuth offset varying quickly across range: the LUT bin changes
+    inside row segments, exercising the per-pixel paths."""
+    S = scene_small
+    az, rg = oracle_cpm(O, S, 1)
+    az = az.copy()
+    az[2] += 0.9      # ~1.8 lines across the burst width
+    az[5] += 0.35
+    kw = rs_inputs(S, 1, (az, rg))
+    gpu = T.deramp_demod_resample(**kw)
+    ref, _ = O.resample(**kw)
+    assert rel_rms(gpu, ref) < RS_TOL
+
+
+def test_resample_steep_polynomial(T, O, scene_small):
+    """Strongly rotated/scaled mapping: ring window misses, HBM fallback."""
+    S = scene_small
+    az, rg = oracle_cpm(O, S, 0)
+    az = az.copy()
+    rg = rg.copy()
+    az[2] += 25.0     # azimuth position moves 50 lines across the width
+    rg[1] += 12.0     # range position moves 24 samples along azimuth
+    kw = rs_inputs(S, 0, (az, rg))
+    gpu = T.deramp_demod_resample(**kw)
+    ref, cnt = O.resample(**kw)
+    assert rel_rms(gpu, ref) < RS_TOL
+
+
+def test_resample_deterministic(T, O, scene_small):
+    S = scene_small
+    cpm = oracle_cpm(O, S, 1)
+    kw = rs_inputs(S, 1, cpm, 0.01)
+    a = T.deramp_demod_resample(**kw)
+    b = T.deramp_demod_resample(**kw)
+    assert np.array_equal(a, b)
+
+
+def test_coherence_parity(T, O, scene_small):
+    S = scene_small
+    b = 1
+    cpm = oracle_cpm(O, S, b)
+    kw = rs_inputs(S, b, cpm)
+    ref_rs, _ = O.resample(**kw)
+    slave = c64(ref_rs)
+    master = S.burst(0, b)
+    for win_rg, win_az in [(10, 3), (24, 6), (5, 5)]:
+        d = T.resample_first_burst(slave.view(np.complex64).reshape(slave.shape[:2]))
+        gpu = T.coherence_est(master, d, win_rg, win_az)
+        ref = O.coherence(master, slave, win_rg, win_az)
+        err = np.abs(gpu - ref).max()
+        assert err < COH_TOL, (win_rg, win_az, err)
+    assert ref[5:-5, 12:-12].mean() > 0.9
+
+
+def test_coherence_slave_equals_master(T, O, scene_small):
+    S = scene_small
+    m = S.burst(0, 0)
+    s = m.astype(np.float32)
+    d = T.resample_first_burst(s.view(np.complex64).reshape(s.shape[:2]))
+    gpu = T.coherence_est(m, d, 10, 3, esd_variant=True)
+    live = np.hypot(s[..., 0], s[..., 1]) >= 1e-3
+    assert np.abs(gpu[live] - 1.0).max() < 1e-5
+    assert np.all(gpu[~live] == 0)
+
+
+def _esd_bands(O, S, shifts=None):
+    nb, L, W = S.cfg.n_bursts, S.cfg.lines_per_burst, S.cfg.samples_per_burst
+    m = S.swath[0]
+    ov, tot, mx = O.overlap_size(np.array(m.burst_first_line_time[:nb]),
+                                 np.array(m.burst_last_line_time[:nb]), m.dt)
+    res = []
+    for b in range(nb):
+        cpm = oracle_cpm(O, S, b)
+        r, _ = O.resample(**rs_inputs(S, b, cpm))
+        res.append(r)
+    mF = np.concatenate([S.slc[0][(i + 1) * L - ov[i]:(i + 1) * L] for i in range(nb - 1)])
+    mB = np.concatenate([S.slc[0][(i + 1) * L:(i + 1) * L + ov[i]] for i in range(nb - 1)])
+    sF = np.concatenate([res[i][L - ov[i]:] for i in range(nb - 1)])
+    sB = np.concatenate([res[i + 1][:ov[i]] for i in range(nb - 1)])
+    ss = O.spectral_sep(S.deramp[0]["kt"], L, m.dt)
+    return mF, mB, c64(sF), c64(sB), ov, ss, m.dt
+
+
+def test_esd_parity_and_known_answer(T, O, scene_esd):
+    S = scene_esd
+    mF, mB, sF, sB, ov, ss, dt = _esd_bands(O, S)
+    ref, sums, used = O.esd(mF, mB, sF, sB, ov, 3, 10, 0.3, ss, dt)
+    gpu = T.est_esd_shifts(mF, mB, sF.view(np.complex64)[..., 0], sB.view(np.complex64)[..., 0],
+                           ov, 3, 10, 0.3, ss, dt)
+    assert np.abs(gpu - ref).max() < ESD_TOL, (gpu, ref)
+    # injected misregistration of 0.05 lines, seen through the reference's
+    # spectral separation (L*dt instead of the true burst cycle)
+    L, o = S.cfg.lines_per_burst, S.cfg.overlap_lines
+    expect = -0.05 * (L - o - 1) / L
+    assert np.all(np.abs(ref - expect) < 0.01), (ref, expect)
+
+
+def test_esd_reference_window(T, O, scene_esd):
+    """The reference's hard-coded 24 x 6 window (Func.cpp:2583-2585)."""
+    S = scene_esd
+    mF, mB, sF, sB, ov, ss, dt = _esd_bands(O, S)
+    ref, _, _ = O.esd(mF, mB, sF, sB, ov, 6, 24, 0.3, ss, dt)
+    gpu = T.est_esd_shifts(mF, mB, sF.view(np.complex64)[..., 0], sB.view(np.complex64)[..., 0],
+                           ov, 6, 24, 0.3, ss, dt)
+    assert np.abs(gpu - ref).max() < ESD_TOL
+
+
+def _poly_grid(c, ymin, ymax, xmin, xmax):
+    y = np.linspace(ymin, ymax, 31)
+    x = np.linspace(xmin, xmax, 41)
+    Y, X = np.meshgrid(y, x, indexing="ij")
+    Lh = (Y - 0.5 * (ymin + ymax)) / (0.25 * (ymax - ymin))
+    Ph = (X - 0.5 * (xmin + xmax)) / (0.25 * (xmax - xmin))
+    return c[0] + c[1] * Lh + c[2] * Ph + c[3] * Lh * Lh + c[4] * Lh * Ph + c[5] * Ph * Ph
+
+
+@pytest.mark.parametrize("b", [0, 1])
+def test_geocoreg_parity(T, O, scene_small, b):
+    S = scene_small
+    g = S.geo_args(b)
+    dem_int = np.rint(g["dem"]).astype(np.int32)
+    az_o, rg_o, st, nv = O.geocoreg(dem_int.astype(np.float32), g["lat0"], g["lon0"], g["dlat"],
+                                    g["dlon"], g["xmin"], g["xmax"], g["ymin"], g["ymax"], g["dt"],
+                                    g["first_line_time"], g["slr_time"], g["range_spacing"],
+                                    g["mid_time"], g["azi_init"], g["line_offset"], g["coefs"])
+    m, s = S.swath
+    L = S.cfg.lines_per_burst
+    az_g, rg_g = T.geocoreg_warp(
+        dem_int, g["lat0"], g["lon0"], g["dlat"], g["dlon"], g["xmin"], g["xmax"], g["ymin"],
+        g["ymax"], b, b, L, g["dt"], g["first_line_time"], g["slr_time"], g["range_spacing"],
+        (np.array(m.sv_t[:m.n_sv]), np.array(s.sv_t[:s.n_sv])), g["coefs"], g["azi_init"],
+        S.cfg.samples_per_burst)
+    box = (g["ymin"], g["ymax"], g["xmin"], g["xmax"])
+    daz = np.abs(_poly_grid(az_g, *box) - _poly_grid(az_o, *box)).max()
+    drg = np.abs(_poly_grid(rg_g, *box) - _poly_grid(rg_o, *box)).max()
+    assert daz < OFF_TOL and drg < OFF_TOL, (daz, drg)
+
+
+def test_geocoreg_not_positive_definite(T, scene_small):
+    """All-nodata DEM: the normal matrix is singular -> TOPS_E_NOT_PD and the
+    output coefficients are left untouched (as the reference)."""
+    S = scene_small
+    g = S.geo_args(0)
+    dem_int = np.full(g["dem"].shape, -32768, np.int32)
+    m, s = S.swath
+    with pytest.raises(T.TopsError) as ei:
+        T.geocoreg_warp(dem_int, g["lat0"], g["lon0"], g["dlat"], g["dlon"], g["xmin"], g["xmax"],
+                        g["ymin"], g["ymax"], 0, 0, S.cfg.lines_per_burst, g["dt"],
+                        g["first_line_time"], g["slr_time"], g["range_spacing"],
+                        (np.array(m.sv_t[:m.n_sv]), np.array(s.sv_t[:s.n_sv])), g["coefs"],
+                        g["azi_init"], S.cfg.samples_per_burst)
+    assert ei.value.status == T.TOPS_E_NOT_PD
