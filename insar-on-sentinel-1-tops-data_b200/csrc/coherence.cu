@@ -13,8 +13,9 @@
 // rows: it reads master (CInt16) and slave (complex64) once per row with
 // coalesced loads, forms the four products and accumulates the vertical box
 // sums for the group's rows in registers.  The vertical sums go to shared
-// memory; the horizontal box is a sliding sum over 4 consecutive outputs per
-// thread, written with one 16-byte store.  HBM traffic is the algorithmic
+// memory; the horizontal box is a sliding sum over 8 consecutive outputs per
+// thread, written with 16-byte stores.  The azimuth window is a template
+// parameter for the common sizes (3 and the reference's 6).  HBM traffic is the algorithmic
 // 4 + 8 + 4 bytes per pixel plus the column halo.
 #include <cuda_runtime.h>
 
@@ -28,6 +29,7 @@ constexpr int CO_NT = 256;
 constexpr int CO_TW = 224;   // output columns per strip (win_rg <= 33)
 constexpr int CO_GR = 8;     // rows per group
 constexpr int CO_SEG = 64;   // rows per work item
+constexpr int CO_CPI = 8;    // output columns per horizontal item
 constexpr int CO_MAXJOBS = 32;
 constexpr int CO_MAX_WIN_RG = CO_NT - CO_TW + 1;
 
@@ -37,12 +39,15 @@ struct CoBatch {
 };
 
 struct CoShared {
-  float4 V[CO_GR][CO_NT];      // vertical sums: (re, im, |s|^2, |m|^2)
-  float judge[CO_GR][CO_NT];   // |s| of the centre pixel
+  float4 V[CO_GR][pad8(CO_NT)];      // vertical sums (re, im, |s|^2, |m|^2), pad8(x)
+  float judge[CO_GR][pad8(CO_NT)];   // |s|^2 of the centre pixel, pad8(x)
 };
 
-__global__ void __launch_bounds__(CO_NT)
-    coherence_kernel(const __grid_constant__ CoBatch B) {
+// WAZ > 0: azimuth window known at compile time (the vertical box is fully
+// unrolled); WAZ == 0: runtime window.  The amplitude mask |s| < 0.001 of
+// the reference (EstCoh.cu:393, 446) is evaluated as |s|^2 < 1e-6.
+template <int WAZ>
+__global__ void __launch_bounds__(CO_NT) coherence_kernel(const __grid_constant__ CoBatch B) {
   __shared__ CoShared S;
   const int tid = threadIdx.x;
   const int item = blockIdx.x;
@@ -52,7 +57,8 @@ __global__ void __launch_bounds__(CO_NT)
   const CohJob &J = B.jobs[jb];
   const int local = item - J.item_begin;
   const int strip = local % J.strips, seg = local / J.strips;
-  const int win_rg = B.win_rg, win_az = B.win_az;
+  const int win_rg = B.win_rg;
+  const int win_az = WAZ > 0 ? WAZ : B.win_az;
   const int dx = (win_rg - 1) / 2, dy = (win_az - 1) / 2;
   const int c0 = strip * CO_TW;
   const int cN = min(CO_TW, J.pixels - c0);
@@ -73,72 +79,106 @@ __global__ void __launch_bounds__(CO_NT)
       judge[k] = 0.f;
     }
     const int nin = gr + win_az - 1;
-    for (int q = 0; q < nin; q++) {
+    auto product = [&](short2 m, float2 s) {
+      const float mr = m.x, mi = m.y;
+      return make_float4(mr * s.x + mi * s.y,   // m * conj(s)
+                         mi * s.x - mr * s.y, s.x * s.x + s.y * s.y, mr * mr + mi * mi);
+    };
+    auto load = [&](int q, short2 &m, float2 &s) {
       const int y = rg - dy + q;
-      float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
-      float sabs = 0.f;
-      if (xin && y >= 0 && y < J.lines) {
-        const short2 m = J.master[(long)y * J.master_pitch + x];
-        const float2 s = J.slave[(long)y * J.slave_pitch + x];
-        const float mr = m.x, mi = m.y;
-        p.x = mr * s.x + mi * s.y;   // m * conj(s)
-        p.y = mi * s.x - mr * s.y;
-        p.z = s.x * s.x + s.y * s.y;
-        p.w = mr * mr + mi * mi;
-        sabs = hypotf(s.x, s.y);
+      m = make_short2(0, 0);
+      s = make_float2(0.f, 0.f);
+      if (xin && q < nin && y >= 0 && y < J.lines) {
+        m = J.master[(long)y * J.master_pitch + x];
+        s = J.slave[(long)y * J.slave_pitch + x];
       }
+    };
+    if (WAZ > 0) {
+      // all loads of the group first (memory-level parallelism), then math
+      constexpr int NQ = CO_GR + (WAZ > 0 ? WAZ : 1) - 1;
+      short2 mv[NQ];
+      float2 sv[NQ];
 #pragma unroll
-      for (int k = 0; k < CO_GR; k++) {
-        const int j = q - k;
-        if (j >= 0 && j < win_az) {
-          acc[k].x += p.x;
-          acc[k].y += p.y;
-          acc[k].z += p.z;
-          acc[k].w += p.w;
+      for (int q = 0; q < NQ; q++) load(q, mv[q], sv[q]);
+#pragma unroll
+      for (int q = 0; q < NQ; q++) {
+        const float4 p = product(mv[q], sv[q]);
+#pragma unroll
+        for (int k = 0; k < CO_GR; k++) {
+          if (q - k >= 0 && q - k < WAZ) {
+            acc[k].x += p.x;
+            acc[k].y += p.y;
+            acc[k].z += p.z;
+            acc[k].w += p.w;
+          }
+          if (q == k + (WAZ - 1) / 2) judge[k] = p.z;
         }
-        if (q == k + dy) judge[k] = sabs;
+      }
+    } else {
+      for (int q = 0; q < nin; q++) {
+        short2 m;
+        float2 sl;
+        load(q, m, sl);
+        const float4 p = product(m, sl);
+#pragma unroll
+        for (int k = 0; k < CO_GR; k++) {
+          const int j = q - k;
+          if (j >= 0 && j < win_az) {
+            acc[k].x += p.x;
+            acc[k].y += p.y;
+            acc[k].z += p.z;
+            acc[k].w += p.w;
+          }
+          if (q == k + dy) judge[k] = p.z;
+        }
       }
     }
 #pragma unroll
     for (int k = 0; k < CO_GR; k++) {
-      S.V[k][tid] = acc[k];
-      S.judge[k][tid] = judge[k];
+      S.V[k][pad8(tid)] = acc[k];
+      S.judge[k][pad8(tid)] = judge[k];
     }
     __syncthreads();
-    // ---- horizontal pass: 4 consecutive outputs per item
-    const int ngrp = (cN + 3) >> 2;
-    for (int it = tid; it < gr * ngrp; it += CO_NT) {
-      const int k = it / ngrp;
-      const int cg = (it - k * ngrp) << 2;
+    // ---- horizontal pass: CO_CPI consecutive outputs per item
+    constexpr int NG = CO_TW / CO_CPI;
+    for (int it = tid; it < gr * NG; it += CO_NT) {
+      const int k = it / NG;
+      const int cg = (it - k * NG) * CO_CPI;
+      if (cg >= cN) continue;
       float4 w = make_float4(0.f, 0.f, 0.f, 0.f);
       for (int i = 0; i < win_rg; i++) {
-        const float4 v = S.V[k][cg + i];
+        const float4 v = S.V[k][pad8(cg + i)];
         w.x += v.x;
         w.y += v.y;
         w.z += v.z;
         w.w += v.w;
       }
-      float out[4];
+      float out[CO_CPI];
 #pragma unroll
-      for (int u = 0; u < 4; u++) {
+      for (int u = 0; u < CO_CPI; u++) {
         if (u > 0) {
-          const float4 a = S.V[k][cg + u - 1 + win_rg];
-          const float4 b = S.V[k][cg + u - 1];
+          const float4 a = S.V[k][pad8(cg + u - 1 + win_rg)];
+          const float4 b = S.V[k][pad8(cg + u - 1)];
           w.x += a.x - b.x;
           w.y += a.y - b.y;
           w.z += a.z - b.z;
           w.w += a.w - b.w;
         }
         const float p = w.z * w.w;
-        float g = (p > 0.f) ? sqrtf(w.x * w.x + w.y * w.y) / sqrtf(p) : 0.f;
-        if (S.judge[k][cg + u + dx] < 0.001f) g = 0.f;
+        float g = (p > 0.f) ? sqrtf(w.x * w.x + w.y * w.y) * rsqrtf(p) : 0.f;
+        if (S.judge[k][pad8(cg + u + dx)] < 1e-6f) g = 0.f;
         out[u] = g;
       }
       float *orow = J.coh + (long)(rg + k) * J.coh_pitch + c0 + cg;
-      if (cg + 4 <= cN && ((reinterpret_cast<uintptr_t>(orow) & 15) == 0)) {
-        *reinterpret_cast<float4 *>(orow) = make_float4(out[0], out[1], out[2], out[3]);
+      if (cg + CO_CPI <= cN && ((reinterpret_cast<uintptr_t>(orow) & 15) == 0)) {
+#pragma unroll
+        for (int u = 0; u < CO_CPI; u += 4)
+          *reinterpret_cast<float4 *>(orow + u) = make_float4(out[u], out[u + 1], out[u + 2],
+                                                              out[u + 3]);
       } else {
-        for (int u = 0; u < 4 && cg + u < cN; u++) orow[u] = out[u];
+#pragma unroll
+        for (int u = 0; u < CO_CPI; u++)
+          if (cg + u < cN) orow[u] = out[u];
       }
     }
     __syncthreads();
@@ -161,7 +201,12 @@ int launch_coherence(const CohJob *jobs, int njobs, int win_rg, int win_az, cuda
     }
     B.total_items = items;
     if (!items) continue;
-    coherence_kernel<<<items, CO_NT, 0, st>>>(B);
+    if (win_az == 3)
+      coherence_kernel<3><<<items, CO_NT, 0, st>>>(B);
+    else if (win_az == 6)
+      coherence_kernel<6><<<items, CO_NT, 0, st>>>(B);
+    else
+      coherence_kernel<0><<<items, CO_NT, 0, st>>>(B);
     TOPS_CUDA_TRY(cudaGetLastError());
   }
   return TOPS_OK;

@@ -43,6 +43,10 @@ __device__ __forceinline__ float reduce_2pi(double phi) {
   return (float)r;
 }
 
+// Shared-memory index padding: one slot every 8 elements, so threads that
+// each own 8 consecutive elements (lanes 8 apart) hit distinct banks.
+__host__ __device__ constexpr int pad8(int x) { return x + (x >> 3); }
+
 // Float reduction for small arguments (|x| < ~1e3) before __sincosf.
 __device__ __forceinline__ float reduce_2pi_f(float x) {
   float n = rintf(x * 0.15915494309189535f);

@@ -1,7 +1,7 @@
 // resample.cu -- TOPS deramp + demodulation + 12-point LUT sinc resampling
 // + reramp of slave bursts onto the master grid (sm_100a).
 //
-// Computes exactly the reference algorithm of DerampDemod_Shared
+// Computes the reference algorithm of DerampDemod_Shared
 // (DerampAndResample.cu:117-183) followed by Interpolation_12p
 // (DerampAndResample.cu:349-520), GetIndexes (:108-112) and my_polyval /
 // normalizeWarp (cuConstants.cuh:53-65):
@@ -9,7 +9,8 @@
 //   index     L0 = trunc(y), bin = int(frac * 2047 + 0.5)  (same for x)
 //   regions   outside the slave box -> 0; within 5/7 samples of its edge ->
 //             the nearest sample; interior -> separable 12x12 LUT sinc of the
-//             deramped slave, reramped with the interpolated deramp phase.
+//             deramped slave d = s exp(i phi), reramped with the LUT-weighted
+//             sum of the deramp phase phi.
 //
 // B200 design (no textures, no phase array in HBM):
 //   * A CTA owns a strip of RS_TW output columns and sweeps a segment of
@@ -21,14 +22,17 @@
 //     interior pixel of a row segment uses the same (azimuth line, LUT bin),
 //     v(x) = sum_j kAz[j] d(L0-5+j, x) is computed once per slave column and
 //     reused by the 12 range taps of all pixels; the azimuth pass is
-//     register-blocked over 4 consecutive rows (15 ring loads for 4 rows).
-//   * Phase: phi(y,x) = phi_ref(y) + G(y,x), with phi_ref(y) the FP64 phase
-//     of a reference column and G a small FP32 residual (|G| < a few rad).
-//     The interpolated phase is S_P * Psi_row + sum kRg*gamma(x), where
-//     Psi_row = sum_j kAz[j] phi_ref(y_j) is FP64 per row (reduced mod 2*pi)
-//     and S_P = sum kRg = 1 + sp1 per LUT bin.  This equals the reference's
-//     144-tap FP64 phase sum in exact arithmetic with FP32 only on
-//     few-radian quantities.
+//     register-blocked over 4 consecutive rows (15 ring loads serve 4 rows)
+//     and uses the packed FP32x2 FMA of sm_100 for the complex samples.
+//   * Phase: phi(y,x) = phi_ref(y) + G(y,x), phi_ref the FP64 phase of a
+//     reference column, G an FP32 residual of a few radians.  For a column,
+//     G is exactly quadratic in azimuth time, so its azimuth interpolation
+//     is sum_j kAz[j] G(y_j) = M0 G(L0) + dG/dt(L0) dt M1 + d2G dt^2 M2 with
+//     the LUT row moments M0..M2 -- three FMAs instead of twelve taps.  The
+//     interpolated phase is (1 + sp1) Psi_row + sum_i kRg[i] gamma(x_i),
+//     where Psi_row = sum_j kAz[j] phi_ref(y_j) is FP64 (reduced mod 2 pi)
+//     and 1 + sp1 = sum kRg.  This equals the reference's 144-tap FP64 phase
+//     sum in exact arithmetic with FP32 only on few-radian quantities.
 //   * Rows whose bins are not uniform, or pixels whose support leaves the
 //     ring window, take per-pixel paths (from the ring, else from HBM) that
 //     compute the same formula.
@@ -43,16 +47,19 @@ namespace tops {
 
 constexpr int RS_NT = 256;   // threads per CTA
 constexpr int RS_TW = 112;   // output columns per strip
-constexpr int RS_GR = 8;     // output rows per group
+constexpr int RS_GR = 16;    // output rows per group
 constexpr int RS_FR = 32;    // ring rows (power of two)
-constexpr int RS_FW = 128;   // ring columns
+constexpr int RS_FW = 128;   // ring columns (= threads per half CTA)
 constexpr int RS_SEG = 256;  // output rows per work item
+constexpr int RS_CPI = 8;    // output columns per range-pass item
 constexpr int RS_MAXJOBS = 32;
+constexpr int KEY_NONE = 0x7fffffff;
 
 enum : int { REG_OUT = 0, REG_EDGE = 1, REG_IN = 2 };
 
 struct RsLut {
   const float *kaz, *krg;  // [2048][12]
+  const float4 *krg2;      // [2048][6]: range taps duplicated (w0,w0,w1,w1), ...
   const float *sp1;        // [2048]: sum(krg row) - 1
 };
 
@@ -62,45 +69,47 @@ struct RsBatch {
   ResampleJob jobs[RS_MAXJOBS];
 };
 
-struct RsTask {
-  int kind;      // 4: four-row blocked, 1: single row
-  int row;       // first row
-  int xlo, n;    // ring-relative first column, count
-  int begin;     // first item index
-};
-
-struct RsShared {
+struct __align__(16) RsShared {
   float2 ring_d[RS_FR][RS_FW];
   float ring_g[RS_FR][RS_FW];
+  float2 vd[RS_GR][pad8(RS_FW)];   // indexed with pad8(x)
+  float vg[RS_GR][pad8(RS_FW)];
+  float4 wpair[RS_GR][6];        // azimuth taps duplicated: (w0,w0,w1,w1), ...
   double ring_phiref[RS_FR];
-  int ring_row[RS_FR];
-  float2 vd[RS_GR][RS_FW];
-  float vg[RS_GR][RS_FW];
-  int kl0[RS_GR][RS_TW];
-  int kp0[RS_GR][RS_TW];
-  int kb[RS_GR][RS_TW];          // binL | binP << 12 | region << 24
-  double phat[RS_TW];            // normalised master column per strip column
-  int row_uniform[RS_GR];
-  int row_L0[RS_GR], row_bL[RS_GR];
-  int row_xlo[RS_GR], row_xhi[RS_GR];   // ring-relative, inclusive
-  double row_lhat[RS_GR];         // normalised master line of each row
-  double row_psi[RS_GR];
+  double rowA_az[RS_SEG], rowB_az[RS_SEG], rowA_rg[RS_SEG], rowB_rg[RS_SEG];
+  int kl0[RS_GR][pad8(RS_TW)];     // indexed with pad8(column)
+  int kp0[RS_GR][pad8(RS_TW)];
+  int kb[RS_GR][pad8(RS_TW)];      // binL | binP << 12 | region << 24
+  // per-row statistics of the group (interior pixels)
+  int st_kmin[RS_GR], st_kmax[RS_GR], st_pmin[RS_GR], st_pmax[RS_GR];
+  int row_flag[RS_GR];           // 1: shared azimuth pass
+  int row_L0[RS_GR], row_xlo[RS_GR], row_xhi[RS_GR];
+  float row_M0[RS_GR], row_P1[RS_GR], row_P2[RS_GR];
   float row_rho[RS_GR], row_psif[RS_GR];
-  RsTask tasks[RS_GR];
-  int ntasks, nitems;
-  int grp_lmin, grp_lmax, grp_ring_ok;
+  double caz[6], crg[6], shift;
   int xw;                        // absolute slave column of ring column 0
-  double ref_kt, ref_tref, ref_fdc;
-  double caz[6], crg[6];         // offset polynomials of this job
-  double shift;                  // azimuth shift of this job
+  double ref_a0, ref_a1, ref_a2; // deramp quadratic of the reference column
 };
 
-// Deramp + demodulation phase (DerampAndResample.cu:151-158), FP64.
+// Deramp + demodulation phase (DerampAndResample.cu:151-158), FP64, as the
+// quadratic a2 ta^2 + a1 ta + a0 of the burst-local azimuth time ta:
+//   -pi kt (ta - tref)^2 - 2 pi fdc ta.
+struct DerampQuad {
+  double a0, a1, a2;
+};
+__device__ __forceinline__ DerampQuad deramp_quad(double kt, double tref, double fdc) {
+  DerampQuad q;
+  q.a2 = -kPi * kt;
+  q.a1 = 2.0 * kPi * kt * tref - 2.0 * kPi * fdc;
+  q.a0 = -kPi * kt * tref * tref;
+  return q;
+}
+__device__ __forceinline__ double quad_eval(const DerampQuad &q, double ta) {
+  return fma(fma(q.a2, ta, q.a1), ta, q.a0);
+}
 __device__ __forceinline__ double deramp_phase(double ta, double kt, double tref, double fdc) {
-  double e = ta - tref;
-  double deramp = -kPi * kt * (e * e);
-  double demod = -2.0 * kPi * fdc * ta;
-  return deramp + demod;
+  const double e = ta - tref;
+  return -kPi * kt * (e * e) - 2.0 * kPi * fdc * ta;
 }
 
 __device__ __forceinline__ float2 cmul_conj_phase(float2 a, float phi) {
@@ -177,11 +186,16 @@ __device__ float2 interior_from_ring(const RsShared &S, const RsLut &lut, int L0
   return cmul_conj_phase(make_float2(sre, sim), phi);
 }
 
+__device__ __forceinline__ int warp_min(int v) { return __reduce_min_sync(0xffffffffu, v); }
+__device__ __forceinline__ int warp_max(int v) { return __reduce_max_sync(0xffffffffu, v); }
+
 __global__ void __launch_bounds__(RS_NT, 2)
     resample_kernel(const __grid_constant__ RsBatch B, RsLut lut) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   RsShared &S = *reinterpret_cast<RsShared *>(smem_raw);
   const int tid = threadIdx.x;
+  const int ct = tid & (RS_FW - 1);  // column of this thread (key, ring, azimuth passes)
+  const int half = tid >> 7;         // 0 / 1
 
   // ---- locate the work item (job, strip, segment)
   const int item = blockIdx.x;
@@ -197,7 +211,8 @@ __global__ void __launch_bounds__(RS_NT, 2)
   const int cN = min(RS_TW, mpix - c0);
   const int r_begin = J.row0 + seg * J.seg_rows;
   const int r_end = min(r_begin + J.seg_rows, J.row0 + J.nrows);
-  // ---- per-strip setup: coefficients, normalised columns, ring window
+
+  // ---- per work item setup: polynomials, shift, statistics
   if (tid < 12) {
     const double v = J.cpm_dev ? J.cpm_dev[tid] : (tid < 6 ? J.caz[tid] : J.crg[tid - 6]);
     if (tid < 6)
@@ -215,13 +230,27 @@ __global__ void __launch_bounds__(RS_NT, 2)
     }
     S.shift = sh;
   }
-  for (int c = tid; c < RS_TW; c += RS_NT)
-    S.phat[c] = ((double)(c0 + min(c, cN - 1)) - J.midP) * J.invP;
-  if (tid < RS_FR) S.ring_row[tid] = INT32_MIN;
+  if (tid < RS_GR) {
+    S.st_kmin[tid] = KEY_NONE;
+    S.st_kmax[tid] = -1;
+    S.st_pmin[tid] = KEY_NONE;
+    S.st_pmax[tid] = -KEY_NONE;
+  }
   __syncthreads();
-  const double shift = S.shift;
+  // per-row polynomial terms: y = A(row) + B(row) P^ + c5 P^2
+  {
+    const int r = r_begin + tid;
+    if (r < r_end) {
+      const double L = ((double)(r + J.my0) - J.midL) * J.invL;
+      const double *a = S.caz, *g = S.crg;
+      S.rowA_az[tid] = a[0] + a[1] * L + a[3] * L * L + S.shift;
+      S.rowB_az[tid] = a[2] + a[4] * L;
+      S.rowA_rg[tid] = g[0] + g[1] * L + g[3] * L * L;
+      S.rowB_rg[tid] = g[2] + g[4] * L;
+    }
+  }
   if (tid == 0) {
-    // range position at the segment corners and edge midpoints
+    // range position at the segment corners and edge midpoints -> ring window
     double pmin = 1e300, pmax = -1e300;
     for (int a = 0; a < 3; a++) {
       int rr = (a == 0) ? r_begin : (a == 1 ? (r_begin + r_end - 1) / 2 : r_end - 1);
@@ -240,356 +269,335 @@ __global__ void __launch_bounds__(RS_NT, 2)
     int xw = lo - (slack > 0 ? slack / 2 : 0);
     S.xw = xw;
     int xr = min(max(xw + RS_FW / 2, J.sx0), J.sx1);
-    S.ref_kt = J.kt[xr];
-    S.ref_tref = J.tref[xr];
-    S.ref_fdc = J.fdc[xr];
+    const DerampQuad q = deramp_quad(J.kt[xr], J.tref[xr], J.fdc[xr]);
+    S.ref_a0 = q.a0;
+    S.ref_a1 = q.a1;
+    S.ref_a2 = q.a2;
   }
   __syncthreads();
 
-  // per-thread ring column (fixed for the work item) and its deramp params
-  const int rcol = tid & (RS_FW - 1);
-  const int rpar = tid >> 7;  // 0 or 1: which half of the new rows
-  const int xabs = S.xw + rcol;
+  // per-thread column constants
+  const bool kcol = ct < cN;                         // key column
+  const double phat = ((double)(c0 + min(ct, cN - 1)) - J.midP) * J.invP;
+  const double q_az = S.caz[5] * phat * phat, q_rg = S.crg[5] * phat * phat;
+  const int xabs = S.xw + ct;                        // ring column
   const bool xin = (xabs >= J.sx0 && xabs <= J.sx1);
-  double col_kt = 0, col_tref = 0, col_fdc = 0;
-  if (xin) {
-    col_kt = J.kt[xabs];
-    col_tref = J.tref[xabs];
-    col_fdc = J.fdc[xabs];
-  }
+  DerampQuad colq = {0.0, 0.0, 0.0};
+  if (xin) colq = deramp_quad(J.kt[xabs], J.tref[xabs], J.fdc[xabs]);
+  const float da2 = (float)(colq.a2 - S.ref_a2), da1 = (float)(colq.a1 - S.ref_a1);
+  const DerampQuad refq = {S.ref_a0, S.ref_a1, S.ref_a2};
+  int loaded_lo = INT32_MIN, loaded_hi = INT32_MIN;  // valid ring rows (uniform)
 
   for (int rg = r_begin; rg < r_end; rg += RS_GR) {
     const int gr = min(RS_GR, r_end - rg);
-    if (tid == 0) {
-      S.grp_lmin = INT32_MAX;
-      S.grp_lmax = INT32_MIN;
+    // ---- [A] indexes, bins and regions; per-row statistics
+#pragma unroll 2
+    for (int k = 0; k < RS_GR / 2; k++) {
+      const int r = half + 2 * k;
+      int key = KEY_NONE, kmx = -1, pmn = KEY_NONE, pmx = -KEY_NONE;
+      if (r < gr && kcol) {
+        const int ri = rg - r_begin + r;
+        const double y = fma(S.rowB_az[ri], phat, S.rowA_az[ri] + q_az);
+        const double x = fma(S.rowB_rg[ri], phat, S.rowA_rg[ri] + q_rg);
+        const int l0 = __double2int_rz(y);
+        int bl = __double2int_rz(__dadd_rn(__dmul_rn(y - (double)l0, (double)kInterval), 0.5));
+        const int p0 = __double2int_rz(x);
+        int bp = __double2int_rz(__dadd_rn(__dmul_rn(x - (double)p0, (double)kInterval), 0.5));
+        int reg;
+        if (l0 > J.sy1 || l0 < J.sy0 || p0 > J.sx1 || p0 < J.sx0)
+          reg = REG_OUT;
+        else if (l0 > J.sy1 - 7 || l0 < J.sy0 + 5 || p0 > J.sx1 - 7 || p0 < J.sx0 + 5)
+          reg = REG_EDGE;
+        else
+          reg = REG_IN;
+        bl = min(max(bl, 0), kLutBins - 1);  // the reference's texture clamps
+        bp = min(max(bp, 0), kLutBins - 1);
+        S.kl0[r][pad8(ct)] = l0;
+        S.kp0[r][pad8(ct)] = p0;
+        S.kb[r][pad8(ct)] = bl | (bp << 12) | (reg << 24);
+        if (reg == REG_IN) {
+          key = (l0 << 12) | bl;
+          kmx = key;
+          pmn = pmx = p0;
+        }
+      }
+      if (r < gr) {
+        key = warp_min(key);
+        kmx = warp_max(kmx);
+        pmn = warp_min(pmn);
+        pmx = warp_max(pmx);
+        if ((tid & 31) == 0 && key != KEY_NONE) {
+          atomicMin(&S.st_kmin[r], key);
+          atomicMax(&S.st_kmax[r], kmx);
+          atomicMin(&S.st_pmin[r], pmn);
+          atomicMax(&S.st_pmax[r], pmx);
+        }
+      }
     }
+    __syncthreads();
+
+    // ---- [B] group extent, per-row setup, ring loads
+    int lmin = INT32_MAX, lmax = INT32_MIN;
+#pragma unroll
+    for (int r = 0; r < RS_GR; r++) {
+      const int km = S.st_kmin[r];
+      if (km != KEY_NONE) {
+        lmin = min(lmin, km >> 12);
+        lmax = max(lmax, S.st_kmax[r] >> 12);
+      }
+    }
+    const bool ring_ok = (lmax >= lmin) && (lmax - lmin + 12 <= RS_FR);
     if (tid < RS_GR) {
-      int r = tid;
-      double L = ((double)(rg + r + J.my0) - J.midL) * J.invL;
-      S.row_lhat[r] = L;
-    }
-    __syncthreads();
-
-    // ---- phase A: indexes, bins and regions of the group's pixels
-    for (int p = tid; p < RS_GR * RS_TW; p += RS_NT) {
-      int r = p / RS_TW, c = p - r * RS_TW;
-      if (r >= gr || c >= cN) continue;
-      double L = S.row_lhat[r];
-      double P = S.phat[c];
-      const double *ca = S.caz, *cr = S.crg;
-      double y = ca[0] + ca[1] * L + ca[2] * P + ca[3] * L * L + ca[4] * L * P + ca[5] * P * P;
-      y += shift;
-      double x = cr[0] + cr[1] * L + cr[2] * P + cr[3] * L * L + cr[4] * L * P + cr[5] * P * P;
-      int l0 = (int)trunc(y);
-      int bl = (int)__dadd_rn(__dmul_rn(y - (double)l0, (double)kInterval), 0.5);
-      int p0 = (int)trunc(x);
-      int bp = (int)__dadd_rn(__dmul_rn(x - (double)p0, (double)kInterval), 0.5);
-      int reg;
-      if (l0 > J.sy1 || l0 < J.sy0 || p0 > J.sx1 || p0 < J.sx0)
-        reg = REG_OUT;
-      else if (l0 > J.sy1 - 7 || l0 < J.sy0 + 5 || p0 > J.sx1 - 7 || p0 < J.sx0 + 5)
-        reg = REG_EDGE;
-      else
-        reg = REG_IN;
-      bl = min(max(bl, 0), kLutBins - 1);  // the reference's texture clamps
-      bp = min(max(bp, 0), kLutBins - 1);
-      S.kl0[r][c] = l0;
-      S.kp0[r][c] = p0;
-      S.kb[r][c] = bl | (bp << 12) | (reg << 24);
-      if (reg == REG_IN) {
-        atomicMin(&S.grp_lmin, l0);
-        atomicMax(&S.grp_lmax, l0);
-      }
-    }
-    __syncthreads();
-
-    // ---- phase A2: row analysis (one warp per row)
-    {
-      const int w = tid >> 5, lane = tid & 31;
-      if (w < RS_GR) {
-        int r = w;
-        int first = -1;
-        int pmin = INT32_MAX, pmax = INT32_MIN;
-        int uni = 1;
-        int L0 = 0, bL = 0;
-        if (r < gr) {
-          // first interior pixel of the row (warp-wide)
-          for (int c0i = 0; c0i < cN && first < 0; c0i += 32) {
-            int c = c0i + lane;
-            int in = (c < cN) && ((S.kb[r][c] >> 24) == REG_IN);
-            unsigned m = __ballot_sync(0xffffffffu, in);
-            if (m) first = c0i + __ffs(m) - 1;
+      const int r = tid;
+      const int km = S.st_kmin[r];
+      int flag = 0;
+      if (r < gr && km != KEY_NONE) {
+        const int L0 = km >> 12, bL = km & 0xfff;
+        const int xlo = S.st_pmin[r] - 5 - S.xw, xhi = S.st_pmax[r] + 6 - S.xw;
+        flag = ring_ok && (km == S.st_kmax[r]) && xlo >= 0 && xhi < RS_FW;
+        S.row_L0[r] = L0;
+        S.row_xlo[r] = xlo;
+        S.row_xhi[r] = xhi;
+        if (flag) {
+          const float *kl = lut.kaz + bL * kTaps;
+          float m0 = 0.f, m1 = 0.f, m2 = 0.f;
+#pragma unroll
+          for (int j = 0; j < kTaps; j += 2) {
+            const float w0 = __ldg(kl + j), w1 = __ldg(kl + j + 1);
+            S.wpair[r][j / 2] = make_float4(w0, w0, w1, w1);
+            const float u0 = (float)(j - 5), u1 = (float)(j - 4);
+            m0 += w0 + w1;
+            m1 = fmaf(w0, u0, fmaf(w1, u1, m1));
+            m2 = fmaf(w0, u0 * u0, fmaf(w1, u1 * u1, m2));
           }
-          if (first >= 0) {
-            L0 = S.kl0[r][first];
-            bL = S.kb[r][first] & 0xfff;
-            for (int c = lane; c < cN; c += 32) {
-              int kb = S.kb[r][c];
-              if ((kb >> 24) != REG_IN) continue;
-              if (S.kl0[r][c] != L0 || (kb & 0xfff) != bL) uni = 0;
-              pmin = min(pmin, S.kp0[r][c]);
-              pmax = max(pmax, S.kp0[r][c]);
-            }
-          }
-          uni = __all_sync(0xffffffffu, uni);
-          for (int o = 16; o > 0; o >>= 1) {
-            pmin = min(pmin, __shfl_xor_sync(0xffffffffu, pmin, o));
-            pmax = max(pmax, __shfl_xor_sync(0xffffffffu, pmax, o));
-          }
-        }
-        if (lane == 0) {
-          int xlo = pmin - 5 - S.xw, xhi = pmax + 6 - S.xw;
-          bool ok = (first >= 0) && uni && xlo >= 0 && xhi < RS_FW;
-          S.row_uniform[r] = ok ? 1 : 0;
-          S.row_L0[r] = L0;
-          S.row_bL[r] = bL;
-          S.row_xlo[r] = xlo;
-          S.row_xhi[r] = xhi;
+          const double ta_c = (double)(L0 - J.s_first_line) * J.dt;
+          S.row_M0[r] = m0;
+          S.row_P1[r] = (float)(2.0 * ta_c * J.dt * m1 + J.dt * J.dt * m2);
+          S.row_P2[r] = (float)(J.dt * m1);
         }
       }
-      if (tid == RS_NT - 1) {
-        int lmin = S.grp_lmin, lmax = S.grp_lmax;
-        S.grp_ring_ok = (lmax >= lmin) && (lmax - lmin + 12 <= RS_FR);
-      }
+      S.row_flag[r] = flag;
     }
-    __syncthreads();
-
-    // ---- phase B: bring the needed slave rows into the ring (deramped)
-    if (S.grp_ring_ok) {
-      const int need_lo = S.grp_lmin - 5, need_hi = S.grp_lmax + 6;
-      int k = 0;  // index among rows to load
-      for (int y = need_lo; y <= need_hi; y++) {
-        const int slot = y & (RS_FR - 1);
-        if (S.ring_row[slot] == y) continue;  // uniform across the block
-        if ((k & 1) == rpar) {
-          double ta = (double)(y - J.s_first_line) * J.dt;
-          double phref = deramp_phase(ta, S.ref_kt, S.ref_tref, S.ref_fdc);
+    if (ring_ok) {
+      const int need_lo = lmin - 5, need_hi = lmax + 6;
+      // rows [need_lo, loaded_hi] are already in the ring when the ring holds
+      // them contiguously; otherwise (a jump) the whole range is reloaded
+      const bool cont = need_lo >= loaded_lo && need_lo <= loaded_hi + 1;
+      const int new_lo = cont ? loaded_hi + 1 : need_lo;
+      // loads of up to RS_LB rows are issued before any of the math, so the
+      // HBM latency of a group's new rows is paid once
+      constexpr int RS_LB = 8;
+      for (int y0 = new_lo + half; y0 <= need_hi; y0 += 2 * RS_LB) {
+        short2 sv[RS_LB];
+#pragma unroll
+        for (int u = 0; u < RS_LB; u++) {
+          const int y = y0 + 2 * u;
+          sv[u] = make_short2(0, 0);
+          if (y <= need_hi && xin && y >= J.sy0 && y <= J.sy1)
+            sv[u] = J.slave[(long)(y - J.sy0) * J.slave_pitch + (xabs - J.sx0)];
+        }
+#pragma unroll
+        for (int u = 0; u < RS_LB; u++) {
+          const int y = y0 + 2 * u;
+          if (y > need_hi) break;
+          const int slot = y & (RS_FR - 1);
+          const double ta = (double)(y - J.s_first_line) * J.dt;
+          const double phref = quad_eval(refq, ta);
           float2 d = make_float2(0.f, 0.f);
           float g = 0.f;
           if (xin && y >= J.sy0 && y <= J.sy1) {
-            short2 s = J.slave[(long)(y - J.sy0) * J.slave_pitch + (xabs - J.sx0)];
-            double phi = deramp_phase(ta, col_kt, col_tref, col_fdc);
+            const double phi = quad_eval(colq, ta);
             g = (float)(phi - phref);
             float sn, cs;
             __sincosf(reduce_2pi(phi), &sn, &cs);
-            d.x = (float)s.x * cs - (float)s.y * sn;
-            d.y = (float)s.x * sn + (float)s.y * cs;
+            d.x = (float)sv[u].x * cs - (float)sv[u].y * sn;
+            d.y = (float)sv[u].x * sn + (float)sv[u].y * cs;
           }
-          S.ring_d[slot][rcol] = d;
-          S.ring_g[slot][rcol] = g;
-          if (rcol == 0) S.ring_phiref[slot] = phref;
+          S.ring_d[slot][ct] = d;
+          S.ring_g[slot][ct] = g;
+          if (ct == 0) S.ring_phiref[slot] = phref;
         }
-        k++;
       }
+      if (!cont) loaded_lo = need_lo;
+      loaded_hi = max(loaded_hi, need_hi);
+      loaded_lo = max(loaded_lo, loaded_hi - RS_FR + 1);
     }
     __syncthreads();
-    if (S.grp_ring_ok && tid == 0) {
-      for (int y = S.grp_lmin - 5; y <= S.grp_lmax + 6; y++) S.ring_row[y & (RS_FR - 1)] = y;
-    }
 
-    // ---- phase C0: task list for the shared azimuth pass + row phases
-    if (tid == 0) {
-      int nt = 0, ni = 0;
-      for (int sub = 0; sub < RS_GR; sub += 4) {
-        bool block4 = S.grp_ring_ok && sub + 4 <= gr;
-        int xlo = INT32_MAX, xhi = INT32_MIN;
-        if (block4) {
-          for (int k = 0; k < 4; k++) {
-            int r = sub + k;
-            if (!S.row_uniform[r] || S.row_L0[r] != S.row_L0[sub] + k) block4 = false;
-            xlo = min(xlo, S.row_xlo[r]);
-            xhi = max(xhi, S.row_xhi[r]);
-          }
-        }
-        if (block4) {
-          S.tasks[nt] = RsTask{4, sub, xlo, xhi - xlo + 1, ni};
-          ni += xhi - xlo + 1;
-          nt++;
-        } else if (S.grp_ring_ok) {
-          for (int k = 0; k < 4 && sub + k < gr; k++) {
-            int r = sub + k;
-            if (!S.row_uniform[r]) continue;
-            int n = S.row_xhi[r] - S.row_xlo[r] + 1;
-            S.tasks[nt] = RsTask{1, r, S.row_xlo[r], n, ni};
-            ni += n;
-            nt++;
-          }
-        }
-      }
-      S.ntasks = nt;
-      S.nitems = ni;
-    }
-    if (tid < gr && S.grp_ring_ok && S.row_uniform[tid]) {
+    // ---- [C] shared azimuth pass v(x) and the row phases
+    if (tid < RS_GR && S.row_flag[tid]) {
       const int r = tid;
-      const float *kl = lut.kaz + S.row_bL[r] * kTaps;
+      const int bL = S.st_kmin[r] & 0xfff, L0 = S.row_L0[r];
+      const float *kl = lut.kaz + bL * kTaps;
       double psi = 0.0;
+#pragma unroll
       for (int j = 0; j < kTaps; j++)
-        psi = fma((double)__ldg(kl + j), S.ring_phiref[(S.row_L0[r] - 5 + j) & (RS_FR - 1)], psi);
-      S.row_psi[r] = psi;
+        psi = fma((double)__ldg(kl + j), S.ring_phiref[(L0 - 5 + j) & (RS_FR - 1)], psi);
       S.row_rho[r] = reduce_2pi(psi);
       S.row_psif[r] = (float)psi;
     }
-    __syncthreads();
-
-    // ---- phase C: azimuth pass v(x) = sum_j kAz[j] (d, G)(L0-5+j, x)
-    for (int it = tid; it < S.nitems; it += RS_NT) {
-      int t = 0;
-      while (t + 1 < S.ntasks && S.tasks[t + 1].begin <= it) t++;
-      const RsTask T = S.tasks[t];
-      const int x = T.xlo + (it - T.begin);
-      if (T.kind == 4) {
-        float w[4][kTaps];
+    {
+      const int x = ct;
+#pragma unroll 1
+      for (int qq = 0; qq < 2; qq++) {
+        const int q = half + 2 * qq;  // quad of rows 4q..4q+3
+        const int r0 = 4 * q;
+        if (r0 >= gr) continue;
+        bool blk = r0 + 4 <= gr;
+        int xl = INT32_MAX, xh = INT32_MIN;
+        const int L00 = S.row_L0[r0];
 #pragma unroll
         for (int k = 0; k < 4; k++) {
-          const float *kl = lut.kaz + S.row_bL[T.row + k] * kTaps;
-#pragma unroll
-          for (int j = 0; j < kTaps; j++) w[k][j] = __ldg(kl + j);
+          const int r = min(r0 + k, RS_GR - 1);
+          blk = blk && S.row_flag[r] && S.row_L0[r] == L00 + k;
+          xl = min(xl, S.row_xlo[r]);
+          xh = max(xh, S.row_xhi[r]);
         }
-        float ar[4] = {0.f, 0.f, 0.f, 0.f}, ai[4] = {0.f, 0.f, 0.f, 0.f},
-              ag[4] = {0.f, 0.f, 0.f, 0.f};
-        const int ybase = S.row_L0[T.row] - 5;
+        if (blk) {
+          if (x < xl || x > xh) continue;
+          float2 acc[4];
 #pragma unroll
-        for (int jj = 0; jj < kTaps + 3; jj++) {
-          const int slot = (ybase + jj) & (RS_FR - 1);
-          const float2 d = S.ring_d[slot][x];
-          const float g = S.ring_g[slot][x];
+          for (int k = 0; k < 4; k++) acc[k] = make_float2(0.f, 0.f);
+          const int ybase = L00 - 5;
 #pragma unroll
-          for (int k = 0; k < 4; k++) {
-            const int j = jj - k;
-            if (j >= 0 && j < kTaps) {
-              ar[k] = fmaf(w[k][j], d.x, ar[k]);
-              ai[k] = fmaf(w[k][j], d.y, ai[k]);
-              ag[k] = fmaf(w[k][j], g, ag[k]);
+          for (int jj = 0; jj < kTaps + 3; jj++) {
+            const float2 d = S.ring_d[(ybase + jj) & (RS_FR - 1)][x];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+              const int j = jj - k;
+              if (j >= 0 && j < kTaps) {
+                const float4 wp = S.wpair[r0 + k][j >> 1];
+                const float2 w = (j & 1) ? make_float2(wp.z, wp.w) : make_float2(wp.x, wp.y);
+                acc[k] = __ffma2_rn(w, d, acc[k]);
+              }
             }
           }
-        }
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
-          S.vd[T.row + k][x] = make_float2(ar[k], ai[k]);
-          S.vg[T.row + k][x] = ag[k];
-        }
-      } else {
-        const float *kl = lut.kaz + S.row_bL[T.row] * kTaps;
-        const int ybase = S.row_L0[T.row] - 5;
-        float ar = 0.f, ai = 0.f, ag = 0.f;
+          for (int k = 0; k < 4; k++) {
+            const int r = r0 + k;
+            const float gc = S.ring_g[(L00 + k) & (RS_FR - 1)][x];
+            S.vd[r][pad8(x)] = acc[k];
+            S.vg[r][pad8(x)] = fmaf(S.row_M0[r], gc, fmaf(da2, S.row_P1[r], da1 * S.row_P2[r]));
+          }
+        } else {
+#pragma unroll 1
+          for (int k = 0; k < 4 && r0 + k < gr; k++) {
+            const int r = r0 + k;
+            if (!S.row_flag[r] || x < S.row_xlo[r] || x > S.row_xhi[r]) continue;
+            const int L0 = S.row_L0[r];
+            float2 acc = make_float2(0.f, 0.f);
 #pragma unroll
-        for (int j = 0; j < kTaps; j++) {
-          const int slot = (ybase + j) & (RS_FR - 1);
-          const float w = __ldg(kl + j);
-          const float2 d = S.ring_d[slot][x];
-          ar = fmaf(w, d.x, ar);
-          ai = fmaf(w, d.y, ai);
-          ag = fmaf(w, S.ring_g[slot][x], ag);
+            for (int j = 0; j < kTaps; j++) {
+              const float4 wp = S.wpair[r][j >> 1];
+              const float2 w = (j & 1) ? make_float2(wp.z, wp.w) : make_float2(wp.x, wp.y);
+              acc = __ffma2_rn(w, S.ring_d[(L0 - 5 + j) & (RS_FR - 1)][x], acc);
+            }
+            const float gc = S.ring_g[L0 & (RS_FR - 1)][x];
+            S.vd[r][pad8(x)] = acc;
+            S.vg[r][pad8(x)] = fmaf(S.row_M0[r], gc, fmaf(da2, S.row_P1[r], da1 * S.row_P2[r]));
+          }
         }
-        S.vd[T.row][x] = make_float2(ar, ai);
-        S.vg[T.row][x] = ag;
       }
     }
     __syncthreads();
 
-    // ---- phase D: range pass, reramp, store (4 consecutive columns/item)
-    const int ngrp = (cN + 3) >> 2;
-    for (int it = tid; it < gr * ngrp; it += RS_NT) {
-      const int r = it / ngrp;
-      const int cg = (it - r * ngrp) << 2;
-      const int mr = rg + r;  // master row (0-based in box)
-      float2 res[4];
-      int kbv[4], p0v[4], l0v[4];
+    // ---- [D] range pass, reramp, store: RS_CPI consecutive columns per item
+    constexpr int NG = RS_TW / RS_CPI;
+    for (int it = tid; it < gr * NG; it += RS_NT) {
+      const int r = it / NG;
+      const int cg = (it - r * NG) * RS_CPI;
+      if (cg >= cN) continue;
+      const int mr = rg + r;
+      float2 *orow = J.out + (long)(mr - J.row0) * J.out_pitch + c0 + cg;
+      int kbv[RS_CPI], p0v[RS_CPI];
 #pragma unroll
-      for (int k = 0; k < 4; k++) {
-        const int c = min(cg + k, cN - 1);
+      for (int k = 0; k < RS_CPI; k++) {
+        const int c = pad8(min(cg + k, cN - 1));
         kbv[k] = S.kb[r][c];
         p0v[k] = S.kp0[r][c];
-        l0v[k] = S.kl0[r][c];
       }
-      const bool uni = S.grp_ring_ok && S.row_uniform[r];
-      bool fast = uni;
+      const bool uni = S.row_flag[r];
+      bool fast = uni && (cg + RS_CPI <= cN) && ((reinterpret_cast<uintptr_t>(orow) & 15) == 0);
 #pragma unroll
-      for (int k = 0; k < 4; k++)
-        fast = fast && ((kbv[k] >> 24) == REG_IN) && (p0v[k] == p0v[0] + k) && (cg + k < cN);
+      for (int k = 0; k < RS_CPI; k++)
+        fast = fast && ((kbv[k] >> 24) == REG_IN) && (p0v[k] == p0v[0] + k);
       if (fast) {
-        // 15 shared v loads serve 4 pixels x 12 taps
+        // 19 shared v loads serve 8 pixels x 12 taps; 16-byte stores
         const int xb = p0v[0] - 5 - S.xw;
-        float2 vd[kTaps + 3];
-        float vg[kTaps + 3];
+        float2 vd[kTaps + RS_CPI - 1];
+        float vg[kTaps + RS_CPI - 1];
 #pragma unroll
-        for (int i = 0; i < kTaps + 3; i++) {
-          vd[i] = S.vd[r][xb + i];
-          vg[i] = S.vg[r][xb + i];
+        for (int i = 0; i < kTaps + RS_CPI - 1; i++) {
+          vd[i] = S.vd[r][pad8(xb + i)];
+          vg[i] = S.vg[r][pad8(xb + i)];
         }
         const float rho = S.row_rho[r], psif = S.row_psif[r];
+        float4 *o4 = reinterpret_cast<float4 *>(orow);
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
-          const int bp = (kbv[k] >> 12) & 0xfff;
-          const float4 *kp4 = reinterpret_cast<const float4 *>(lut.krg + bp * kTaps);
-          float kp[kTaps];
+        for (int k = 0; k < RS_CPI; k += 2) {
+          float2 res[2];
 #pragma unroll
-          for (int q = 0; q < 3; q++) {
-            float4 t4 = __ldg(kp4 + q);
-            kp[4 * q] = t4.x;
-            kp[4 * q + 1] = t4.y;
-            kp[4 * q + 2] = t4.z;
-            kp[4 * q + 3] = t4.w;
+          for (int u = 0; u < 2; u++) {
+            const int bp = (kbv[k + u] >> 12) & 0xfff;
+            const float4 *kp4 = lut.krg2 + bp * (kTaps / 2);
+            float2 acc = make_float2(0.f, 0.f);
+            float sg = 0.f;
+#pragma unroll
+            for (int q = 0; q < kTaps / 2; q++) {
+              const float4 w = __ldg(kp4 + q);
+              acc = __ffma2_rn(make_float2(w.x, w.y), vd[k + u + 2 * q], acc);
+              acc = __ffma2_rn(make_float2(w.z, w.w), vd[k + u + 2 * q + 1], acc);
+              sg = fmaf(w.x, vg[k + u + 2 * q], sg);
+              sg = fmaf(w.z, vg[k + u + 2 * q + 1], sg);
+            }
+            const float phi = rho + __ldg(lut.sp1 + bp) * psif + sg;
+            res[u] = cmul_conj_phase(acc, phi);
           }
-          float sre = 0.f, sim = 0.f, sg = 0.f;
-#pragma unroll
-          for (int i = 0; i < kTaps; i++) {
-            sre = fmaf(kp[i], vd[k + i].x, sre);
-            sim = fmaf(kp[i], vd[k + i].y, sim);
-            sg = fmaf(kp[i], vg[k + i], sg);
-          }
-          const float phi = rho + __ldg(lut.sp1 + bp) * psif + sg;
-          res[k] = cmul_conj_phase(make_float2(sre, sim), phi);
+          o4[k / 2] = make_float4(res[0].x, res[0].y, res[1].x, res[1].y);
         }
       } else {
 #pragma unroll 1
-        for (int k = 0; k < 4; k++) {
-          res[k] = make_float2(0.f, 0.f);
-          if (cg + k >= cN) continue;
-          const int reg = kbv[k] >> 24;
-          const int l0 = l0v[k], p0 = p0v[k];
+        for (int k = 0; k < RS_CPI && cg + k < cN; k++) {
+          const int c = pad8(cg + k);
+          const int kb = S.kb[r][c], reg = kb >> 24;
+          const int l0 = S.kl0[r][c], p0 = S.kp0[r][c];
+          float2 res = make_float2(0.f, 0.f);
           if (reg == REG_EDGE) {
-            short2 s = J.slave[(long)(l0 - J.sy0) * J.slave_pitch + (p0 - J.sx0)];
-            res[k] = make_float2((float)s.x, (float)s.y);
+            const short2 sv = J.slave[(long)(l0 - J.sy0) * J.slave_pitch + (p0 - J.sx0)];
+            res = make_float2((float)sv.x, (float)sv.y);
           } else if (reg == REG_IN) {
-            const int bl = kbv[k] & 0xfff, bp = (kbv[k] >> 12) & 0xfff;
+            const int bl = kb & 0xfff, bp = (kb >> 12) & 0xfff;
             const int xb = p0 - 5 - S.xw;
-            const bool in_ring = S.grp_ring_ok && xb >= 0 && xb + kTaps <= RS_FW;
-            if (uni && in_ring) {
-              const float4 *kp4 = reinterpret_cast<const float4 *>(lut.krg + bp * kTaps);
-              float sre = 0.f, sim = 0.f, sg = 0.f;
+            const bool in_win = xb >= 0 && xb + kTaps <= RS_FW;
+            if (uni && in_win) {
+              const float4 *kp4 = lut.krg2 + bp * (kTaps / 2);
+              float2 acc = make_float2(0.f, 0.f);
+              float sg = 0.f;
 #pragma unroll
-              for (int q = 0; q < 3; q++) {
-                float4 t4 = __ldg(kp4 + q);
-                float kq[4] = {t4.x, t4.y, t4.z, t4.w};
-#pragma unroll
-                for (int u = 0; u < 4; u++) {
-                  const float2 v = S.vd[r][xb + 4 * q + u];
-                  sre = fmaf(kq[u], v.x, sre);
-                  sim = fmaf(kq[u], v.y, sim);
-                  sg = fmaf(kq[u], S.vg[r][xb + 4 * q + u], sg);
-                }
+              for (int q = 0; q < kTaps / 2; q++) {
+                const float4 w = __ldg(kp4 + q);
+                acc = __ffma2_rn(make_float2(w.x, w.y), S.vd[r][pad8(xb + 2 * q)], acc);
+                acc = __ffma2_rn(make_float2(w.z, w.w), S.vd[r][pad8(xb + 2 * q + 1)], acc);
+                sg = fmaf(w.x, S.vg[r][pad8(xb + 2 * q)], sg);
+                sg = fmaf(w.z, S.vg[r][pad8(xb + 2 * q + 1)], sg);
               }
               const float phi = S.row_rho[r] + __ldg(lut.sp1 + bp) * S.row_psif[r] + sg;
-              res[k] = cmul_conj_phase(make_float2(sre, sim), phi);
-            } else if (in_ring) {
-              res[k] = interior_from_ring(S, lut, l0, bl, p0, bp);
+              res = cmul_conj_phase(acc, phi);
+            } else if (ring_ok && in_win) {
+              res = interior_from_ring(S, lut, l0, bl, p0, bp);
             } else {
-              res[k] = interior_from_global(J, lut, l0, bl, p0, bp);
+              res = interior_from_global(J, lut, l0, bl, p0, bp);
             }
           }
+          orow[k] = res;
         }
       }
-      // store: vectorised when the 4 outputs are in the strip and aligned
-      float2 *orow = J.out + (long)(mr - J.row0) * J.out_pitch + c0 + cg;
-      if (cg + 4 <= cN && ((reinterpret_cast<uintptr_t>(orow) & 15) == 0)) {
-        float4 *o4 = reinterpret_cast<float4 *>(orow);
-        o4[0] = make_float4(res[0].x, res[0].y, res[1].x, res[1].y);
-        o4[1] = make_float4(res[2].x, res[2].y, res[3].x, res[3].y);
-      } else {
-        for (int k = 0; k < 4 && cg + k < cN; k++) orow[k] = res[k];
-      }
+    }
+    if (tid < RS_GR) {
+      S.st_kmin[tid] = KEY_NONE;
+      S.st_kmax[tid] = -1;
+      S.st_pmin[tid] = KEY_NONE;
+      S.st_pmax[tid] = -KEY_NONE;
     }
     __syncthreads();
   }
@@ -598,6 +606,7 @@ __global__ void __launch_bounds__(RS_NT, 2)
 // ---------------------------------------------------------------- host
 struct LutDev {
   float *kaz = nullptr, *krg = nullptr, *sp1 = nullptr;
+  float4 *krg2 = nullptr;
 };
 
 }  // namespace tops
@@ -611,24 +620,31 @@ using namespace tops;
 extern "C" int tops_lut_create(const float *kaz, const float *krg, tops_lut_dev **out) {
   if (!kaz || !krg || !out) return TOPS_E_INVALID;
   tops_lut_dev *L = new tops_lut_dev();
-  std::vector<float> sp1(kLutBins);
+  std::vector<float> sp1(kLutBins), krg2((size_t)kLutBins * kTaps * 2);
   for (int b = 0; b < kLutBins; b++) {
     double s = 0.0;
-    for (int i = 0; i < kTaps; i++) s += (double)krg[b * kTaps + i];
+    for (int i = 0; i < kTaps; i++) {
+      s += (double)krg[b * kTaps + i];
+      krg2[(size_t)b * kTaps * 2 + 2 * i] = krg[b * kTaps + i];
+      krg2[(size_t)b * kTaps * 2 + 2 * i + 1] = krg[b * kTaps + i];
+    }
     sp1[b] = (float)(s - 1.0);
   }
   size_t nb = sizeof(float) * kLutBins * kTaps;
   cudaError_t e = cudaMalloc(&L->d.kaz, nb);
   if (e == cudaSuccess) e = cudaMalloc(&L->d.krg, nb);
+  if (e == cudaSuccess) e = cudaMalloc(&L->d.krg2, 2 * nb);
   if (e == cudaSuccess) e = cudaMalloc(&L->d.sp1, sizeof(float) * kLutBins);
   if (e == cudaSuccess) e = cudaMemcpy(L->d.kaz, kaz, nb, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(L->d.krg, krg, nb, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(L->d.krg2, krg2.data(), 2 * nb, cudaMemcpyHostToDevice);
   if (e == cudaSuccess)
     e = cudaMemcpy(L->d.sp1, sp1.data(), sizeof(float) * kLutBins, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
     set_cuda_error(e);
     cudaFree(L->d.kaz);
     cudaFree(L->d.krg);
+    cudaFree(L->d.krg2);
     cudaFree(L->d.sp1);
     delete L;
     return e == cudaErrorMemoryAllocation ? TOPS_E_NOMEM : TOPS_E_CUDA;
@@ -641,6 +657,7 @@ extern "C" int tops_lut_destroy(tops_lut_dev *L) {
   if (!L) return TOPS_OK;
   cudaFree(L->d.kaz);
   cudaFree(L->d.krg);
+  cudaFree(L->d.krg2);
   cudaFree(L->d.sp1);
   delete L;
   return TOPS_OK;
@@ -704,7 +721,7 @@ int launch_resample(const LutDev &L, const ResampleJob *jobs, int njobs, cudaStr
                                        (int)sizeof(RsShared)));
     attr_done = true;
   }
-  RsLut lut{L.kaz, L.krg, L.sp1};
+  RsLut lut{L.kaz, L.krg, L.krg2, L.sp1};
   for (int j0 = 0; j0 < njobs; j0 += RS_MAXJOBS) {
     RsBatch B;
     B.njobs = 0;
