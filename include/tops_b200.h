@@ -191,6 +191,24 @@ int tops_esd(const tops_esd_overlap *ovs, int n_ov, int win_az, int win_rg, floa
              double *shifts_dev, double *sums_dev, void *scratch_dev, size_t scratch_bytes,
              void *stream);
 
+/* Allocation-free variant of tops_esd (no counterpart in the reference).
+ * For callers that cannot allocate device memory: code running under an
+ * HBM budget owned by someone else (a serving loop that admits work by
+ * footprint, a framework whose pool owns the device), or latency-critical
+ * loops where cudaMalloc's implicit device synchronisation is not allowed.
+ * The per-CTA partial sums live in a static 256 KB array compiled into the
+ * library (16384 partials: e.g. 8 overlaps of 100 x 21000 need 3008); every
+ * GPU that loads the library holds that array until the process exits.
+ * Larger requests return TOPS_E_INVALID with a message; use tops_esd with a
+ * caller-provided scratch buffer for those.  At most 32 overlaps per call.
+ * The first call on a device looks up the array's device address (once per
+ * device, with that device current); make that first call before any stream
+ * capture.  All calls share the array: calls whose executions overlap on
+ * the GPU (different streams, or concurrent host threads) race and must be
+ * serialised by the caller.  Inputs and outputs are as for tops_esd. */
+int tops_esd_static(const tops_esd_overlap *ovs, int n_ov, int win_az, int win_rg, float coh_thr,
+                    double *shifts_dev, double *sums_dev, void *stream);
+
 /* Geometric coregistration of one burst on a device-resident float DEM
  * window.  Writes cpm_dev[12] (6 azimuth then 6 range coefficients) and
  * status_dev[1] (0 ok, 4 = not positive definite) on the device. */

@@ -22,7 +22,9 @@
 // order (deterministic) and evaluates the shift on the device, so the
 // shifts can feed the corrected resample without a host round trip.
 #include <cuda_runtime.h>
+#include <stdio.h>
 
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -294,4 +296,64 @@ extern "C" int tops_esd(const tops_esd_overlap *ovs, int n_ov, int win_az, int w
   }
   return launch_esd(O.data(), n_ov, win_az, win_rg, coh_thr, shifts_dev, sums_dev, scratch_dev,
                     scratch_bytes, static_cast<cudaStream_t>(stream));
+}
+
+// --------------------------------------------------- allocation-free ESD
+// tops_esd() needs a caller-allocated scratch buffer for the per-CTA partial
+// sums.  Callers that must not allocate device memory use
+// tops_esd_static(), whose scratch is this file-scope array.  Every GPU
+// that loads the library holds it (256 KB) until the process exits.
+namespace tops {
+
+constexpr int ESD_STATIC_PARTIALS = 16384;
+static __device__ __align__(256) double2 g_esd_static_partials[ESD_STATIC_PARTIALS];
+constexpr int ESD_STATIC_MAX_DEVICES = 64;
+
+// Device address of the array on the current device.  Host code cannot use
+// the symbol itself (it names a host-side stand-in), so the address is
+// fetched once per device with cudaGetSymbolAddress and cached.
+static int esd_static_scratch(double2 **out) {
+  static std::mutex mu;
+  static double2 *addr[ESD_STATIC_MAX_DEVICES] = {};
+  int dev = -1;
+  TOPS_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= ESD_STATIC_MAX_DEVICES) return TOPS_E_INVALID;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[dev]) {
+    void *p = nullptr;
+    TOPS_CUDA_TRY(cudaGetSymbolAddress(&p, g_esd_static_partials));
+    addr[dev] = static_cast<double2 *>(p);
+  }
+  *out = addr[dev];
+  return TOPS_OK;
+}
+
+}  // namespace tops
+
+extern "C" int tops_esd_static(const tops_esd_overlap *ovs, int n_ov, int win_az, int win_rg,
+                               float coh_thr, double *shifts_dev, double *sums_dev,
+                               void *stream) {
+  if (!ovs || n_ov < 1 || n_ov > ES_MAXOV) return TOPS_E_INVALID;
+  EsdOverlap O[ES_MAXOV];  // host stack: no heap allocation either
+  size_t items = 0;
+  for (int i = 0; i < n_ov; i++) {
+    int s = fill_esd_overlap(ovs[i], O[i]);
+    if (s != TOPS_OK) return s;
+    items += (size_t)esd_items(O[i]);
+  }
+  if (items > (size_t)ESD_STATIC_PARTIALS) {
+    fprintf(stderr,
+            "tops_esd_static: %zu partial sums needed, the static scratch holds %d "
+            "(use tops_esd with a caller-provided scratch buffer)\n",
+            items, ESD_STATIC_PARTIALS);
+    return TOPS_E_INVALID;
+  }
+  double2 *scratch = nullptr;
+  int s = esd_static_scratch(&scratch);
+  if (s != TOPS_OK) return s;
+  // every partial this call reads is written by this call's own launch, so
+  // nothing in the shared array has to be cleared first
+  return launch_esd(O, n_ov, win_az, win_rg, coh_thr, shifts_dev, sums_dev, scratch,
+                    (size_t)ESD_STATIC_PARTIALS * sizeof(double2),
+                    static_cast<cudaStream_t>(stream));
 }

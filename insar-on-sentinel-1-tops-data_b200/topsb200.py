@@ -230,6 +230,8 @@ _proto("tops_coherence", C.c_int, [C.POINTER(CohJob), C.c_int, C.c_int, C.c_int,
 _proto("tops_esd_scratch_bytes", C.c_size_t, [C.POINTER(EsdOverlap), C.c_int])
 _proto("tops_esd", C.c_int, [C.POINTER(EsdOverlap), C.c_int, C.c_int, C.c_int, C.c_float, _vp,
                              _vp, _vp, C.c_size_t, _vp])
+_proto("tops_esd_static", C.c_int, [C.POINTER(EsdOverlap), C.c_int, C.c_int, C.c_int, C.c_float,
+                                    _vp, _vp, _vp])
 _proto("tops_geocoreg_scratch_bytes", C.c_size_t, [C.POINTER(GeoJob), C.c_int])
 _proto("tops_geocoreg", C.c_int, [C.POINTER(GeoJob), C.c_int, _vp, C.c_size_t, _vp])
 

@@ -1,0 +1,81 @@
+"""tops_esd_static: the ESD entry point that allocates no device memory.
+
+Some callers cannot call cudaMalloc -- code that runs inside an HBM budget
+it does not own, or loops where the allocator's implicit synchronisation is
+not allowed.  tops_esd_static keeps its scratch in a static device array of
+the library.  This checks it against tops_esd (caller-provided scratch) on
+the same device inputs, on two calls in a row, and that requests larger than
+the static array are refused.  This file is collected last on purpose.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ESD_TOL = 1e-5   # pixels, as the other ESD parity tests
+
+
+def _overlaps(T, S, torch):
+    nb, L, W = S.cfg.n_bursts, S.cfg.lines_per_burst, S.cfg.samples_per_burst
+    m = S.swath[0]
+    ov, _, _ = T.overlap_size(np.array(m.burst_first_line_time[:nb]),
+                              np.array(m.burst_last_line_time[:nb]), m.dt)
+    master = torch.from_numpy(S.slc[0]).cuda()
+    slave = torch.from_numpy(S.slc[1].astype(np.float32)).cuda()   # complex64 stand-in
+    ss = T.spectral_sep(S.deramp[0]["kt"], L, m.dt)
+    arr = (T.EsdOverlap * (nb - 1))()
+    for i in range(nb - 1):
+        f, b = (i + 1) * L - int(ov[i]), (i + 1) * L
+        e = arr[i]
+        e.mF = master.data_ptr() + f * W * 4
+        e.mB = master.data_ptr() + b * W * 4
+        e.m_pitch = W * 4
+        e.sF = slave.data_ptr() + f * W * 8
+        e.sB = slave.data_ptr() + b * W * 8
+        e.s_pitch = W * 8
+        e.lines, e.pixels = int(ov[i]), W
+        e.spec_sep, e.dt = ss, m.dt
+    return arr, nb - 1, (master, slave)
+
+
+def test_esd_static_matches_esd(T, scene_esd):
+    import torch
+    arr, n, keep = _overlaps(T, scene_esd, torch)
+    stream = torch.cuda.current_stream().cuda_stream
+    nbytes = T.lib.tops_esd_scratch_bytes(arr, n)
+    assert nbytes > 0
+    scratch = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    ref = torch.zeros(n, dtype=torch.float64, device="cuda")
+    ref_sums = torch.zeros(2 * n, dtype=torch.float64, device="cuda")
+    T.check(T.lib.tops_esd(arr, n, 3, 10, C.c_float(0.3), C.c_void_p(ref.data_ptr()),
+                           C.c_void_p(ref_sums.data_ptr()), C.c_void_p(scratch.data_ptr()),
+                           nbytes, C.c_void_p(stream)), "tops_esd")
+    torch.cuda.synchronize()
+    for call in range(2):
+        out = torch.full((n,), float("nan"), dtype=torch.float64, device="cuda")
+        sums = torch.zeros(2 * n, dtype=torch.float64, device="cuda")
+        T.check(T.lib.tops_esd_static(arr, n, 3, 10, C.c_float(0.3),
+                                      C.c_void_p(out.data_ptr()), C.c_void_p(sums.data_ptr()),
+                                      C.c_void_p(stream)), "tops_esd_static")
+        torch.cuda.synchronize()
+        a, r = out.cpu().numpy(), ref.cpu().numpy()
+        assert np.all(np.isfinite(a)), (call, a)
+        assert np.abs(a - r).max() <= ESD_TOL, (call, a, r)
+        assert np.array_equal(sums.cpu().numpy(), ref_sums.cpu().numpy()), call
+
+
+def test_esd_static_rejects_oversized_request(T, scene_esd):
+    import torch
+    arr, n, keep = _overlaps(T, scene_esd, torch)
+    big = (T.EsdOverlap * 1)()
+    big[0] = arr[0]
+    big[0].pixels = 224 * 200           # 200 strips
+    big[0].lines = 32 * 200             # x 200 segments = 40000 partial sums
+    big[0].m_pitch = big[0].pixels * 4
+    big[0].s_pitch = big[0].pixels * 8
+    out = torch.zeros(1, dtype=torch.float64, device="cuda")
+    st = T.lib.tops_esd_static(big, 1, 3, 10, C.c_float(0.3), C.c_void_p(out.data_ptr()), None,
+                               C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert st == T.TOPS_E_INVALID
