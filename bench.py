@@ -19,7 +19,9 @@ step processes 9 burst pairs.
 Multi-GPU: one process per GPU (torchrun); each rank processes its own
 sub-swath pair (replicas, no data exchange): weak scaling, timed as the max
 over ranks.  `--impl reference` times the CPU FP64 port of the reference
-path (the oracle) on the host cores, on bounded samples of the same work.
+path (the oracle) on the host cores, one burst pair of the workload per step;
+the `cpu_baseline` object of the default run is the same path on a sample of
+about 12 s.
 """
 import argparse
 import json
@@ -39,10 +41,10 @@ METRIC = "burst-pairs/s (coreg+resample+ESD+coh)"
 UNIT = "burst-pairs/s"
 
 CONFIGS = {
-    # BASELINE config "Plain method, full subswath"
+    # one full sub-swath pair
     "subswath": dict(n_bursts=9, lines_per_burst=1500, samples_per_burst=21000,
                      overlap_lines=100, dem_lines=3600, dem_pixels=3600, seed=2),
-    # BASELINE config "Plain method, small" (parity-scale)
+    # two bursts of a narrow swath (parity scale)
     "small": dict(n_bursts=2, lines_per_burst=1500, samples_per_burst=4096, overlap_lines=100,
                   dem_lines=512, dem_pixels=512, seed=1),
 }
@@ -109,76 +111,113 @@ def build_scene(T, cfg, rank):
     return T.Scene(**c)
 
 
-def cpu_sample(scene_cfg, seconds_target=15.0):
-    """FP64 oracle on a bounded sample of one burst pair; returns
-    (burst-pairs/s, threads, sample description)."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
-    import topsb200 as T
-    nthreads = os.cpu_count() or 1
-    O.set_num_threads(nthreads)
-    L, W = scene_cfg["lines_per_burst"], scene_cfg["samples_per_burst"]
-    # a small scene with the same sampling and 2 bursts to take stage timings from
-    S = T.Scene(n_bursts=2, lines_per_burst=L, samples_per_burst=min(W, 2048), overlap_lines=100,
-                dem_lines=256, dem_pixels=256, seed=7)
-    Ws = S.cfg.samples_per_burst
-    b = 1
-    g = S.geo_args(b)
-    t0 = time.perf_counter()
-    az, rg, st, nv = O.geocoreg(g["dem"], g["lat0"], g["lon0"], g["dlat"], g["dlon"], g["xmin"],
-                                g["xmax"], g["ymin"], g["ymax"], g["dt"], g["first_line_time"],
-                                g["slr_time"], g["range_spacing"], g["mid_time"], g["azi_init"],
-                                g["line_offset"], g["coefs"])
-    t_geo_px = (time.perf_counter() - t0) / g["dem"].size
-    mb, sb = S.boxes(b)
-    d = S.deramp[1]
-    rows = 256
-    t0 = time.perf_counter()
-    out = O.resample(S.burst(1, b), az, rg, 0.0, S.kaz, S.krg, b, mb, sb, L, S.swath[1].dt,
-                     d["kt"][0], d["tref"][0], d["dc"][0], rows=(600, rows))
-    t_rs_px = (time.perf_counter() - t0) / (rows * Ws)
-    sl = np.ascontiguousarray(out.astype(np.complex64)).view(np.float32).reshape(rows, Ws, 2)
-    t0 = time.perf_counter()
-    O.coherence(S.burst(0, b)[600:600 + rows], sl, WIN_RG, WIN_AZ)
-    t_coh_px = (time.perf_counter() - t0) / (rows * Ws)
-    ov = 100
-    t0 = time.perf_counter()
-    O.esd(S.burst(0, b)[:ov], S.burst(0, b)[ov:2 * ov], sl[:ov], sl[ov:2 * ov], np.array([ov]), WIN_AZ,
-          WIN_RG, 0.3, 1500.0, 2.055e-3)
-    t_esd_px = (time.perf_counter() - t0) / (ov * Ws)
-    # per burst pair of the configured workload: 2 resamples + coherence of
-    # L*W pixels, the ESD share of one overlap, and the burst's DEM window
-    nb = scene_cfg["n_bursts"]
-    dem_px = scene_cfg["dem_lines"] * scene_cfg["dem_pixels"] / nb
-    per_pair = (2 * t_rs_px + t_coh_px) * L * W + t_esd_px * ov * W * (nb - 1) / nb + \
-        t_geo_px * dem_px
-    sample = (f"FP64 oracle, {nthreads} threads: geocoreg of a {g['dem'].shape[0]}x"
-              f"{g['dem'].shape[1]} DEM window, resample + coherence of {rows} lines x {Ws}, ESD of "
-              f"{ov} x {Ws}; per-pixel times scaled to one {L}x{W} burst pair")
-    return 1.0 / per_pair, nthreads, sample
+class CpuPath:
+    """The FP64 oracle (OpenMP over rows, all host threads) run burst pair by
+    burst pair over a scene of the workload, in the order of the reference's
+    stage drivers: geocoreg of the burst's DEM window, the resample, ESD of the
+    overlap with the previous burst, the ESD-corrected resample and the
+    coherence.  Used only for the CPU baseline."""
+
+    def __init__(self, S):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        self.O, self.S = O, S
+        self.threads = os.cpu_count() or 1
+        O.set_num_threads(self.threads)
+        m = S.swath[0]
+        nb = S.cfg.n_bursts
+        self.ov, _, _ = O.overlap_size(np.array(m.burst_first_line_time[:nb]),
+                                       np.array(m.burst_last_line_time[:nb]), m.dt)
+        self.spec = O.spectral_sep(S.deramp[0]["kt"], S.cfg.lines_per_burst, m.dt)
+        self.prev = None
+        self.next_burst = 0
+
+    def pair(self):
+        """Process the next burst pair; returns its wall time in seconds."""
+        O, S = self.O, self.S
+        nb, L = S.cfg.n_bursts, S.cfg.lines_per_burst
+        b = self.next_burst
+        self.next_burst = (b + 1) % nb
+        t0 = time.perf_counter()
+        g = S.geo_args(b)
+        az, rg, st, nv = O.geocoreg(g["dem"], g["lat0"], g["lon0"], g["dlat"], g["dlon"],
+                                    g["xmin"], g["xmax"], g["ymin"], g["ymax"], g["dt"],
+                                    g["first_line_time"], g["slr_time"], g["range_spacing"],
+                                    g["mid_time"], g["azi_init"], g["line_offset"], g["coefs"])
+        mb, sb = S.boxes(b)
+        d = S.deramp[1]
+        kw = dict(slave=S.burst(1, b), cpm_az=az, cpm_rg=rg, kaz=S.kaz, krg=S.krg,
+                  s_burst_idx=b, mbox=mb, sbox=sb, lines_per_burst=L, kt=d["kt"][0],
+                  tref=d["tref"][0], fdc=d["dc"][0])
+        rs, _ = O.resample(az_shift=0.0, dt=S.swath[1].dt, **kw)
+        rs = rs.astype(np.complex64)
+        master = S.burst(0, b)
+        if b == 0 or self.prev is None:
+            rse = rs
+        else:
+            o = int(self.ov[b - 1])
+            band = lambda a: np.ascontiguousarray(a).view(np.float32).reshape(a.shape[0], -1, 2)
+            mF = S.burst(0, b - 1)[L - o:]
+            mB = master[:o]
+            shift, _, _ = O.esd(mF, mB, band(self.prev[L - o:]), band(rs[:o]), np.array([o]),
+                                WIN_AZ, WIN_RG, 0.3, self.spec, S.swath[0].dt)
+            sh = float(shift[0]) if abs(shift[0]) <= 100 else 0.0
+            rse, _ = O.resample(az_shift=sh, dt=S.swath[0].dt, **kw)
+            rse = rse.astype(np.complex64)
+        O.coherence(master, np.ascontiguousarray(rse).view(np.float32).reshape(L, -1, 2),
+                    WIN_RG, WIN_AZ)
+        self.prev = rs
+        return time.perf_counter() - t0
+
+    def describe(self, pairs):
+        S = self.S
+        return (f"FP64 oracle (C, OpenMP, {self.threads} threads) on {pairs} burst pairs of the "
+                f"workload ({S.cfg.lines_per_burst}x{S.cfg.samples_per_burst} each, in burst "
+                f"order): geocoreg of the burst's DEM window, resample, ESD of the overlap with "
+                f"the previous burst, ESD-corrected resample, coherence {WIN_RG}x{WIN_AZ}")
+
+
+def cpu_baseline(S, seconds=12.0):
+    """Burst pairs/s of the CPU path on a bounded sample: bursts in order
+    until `seconds` have passed (at least two, at most all of them)."""
+    cp = CpuPath(S)
+    times = []
+    while len(times) < S.cfg.n_bursts and (len(times) < 2 or sum(times) < seconds):
+        times.append(cp.pair())
+    return len(times) / sum(times), cp.threads, cp.describe(len(times))
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the CPU path (the FP64 oracle port of the reference's
+    algorithm) on the host cores, one burst pair of the workload per step."""
     if rank != 0:
         return
+    import topsb200 as T
     cfg = CONFIGS[args.config]
+    S = build_scene(T, cfg, 0)
+    cp = CpuPath(S)
     for _ in range(args.warmup):
-        cpu_sample(cfg)
-    vals = []
-    for _ in range(args.steps):
-        v, nthreads, sample = cpu_sample(cfg)
-        vals.append(v)
-    value = float(np.mean(vals))
+        cp.pair()
+    times = [cp.pair() for _ in range(args.steps)]
+    value = len(times) / sum(times)
+    nb, L, W = cfg["n_bursts"], cfg["lines_per_burst"], cfg["samples_per_burst"]
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded)",
-            "config": {"workload": args.config, **{k: v for k, v in cfg.items() if k != "seed"}},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port",
-                             "sample": sample},
+            "config": {"workload": workload_name(args.config, cfg),
+                       "window": f"{WIN_RG}x{WIN_AZ}", "step": "one burst pair"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cp.threads, "kind": "port",
+                             "sample": cp.describe(len(times))},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def workload_name(name, cfg):
+    return (f"{name}: {cfg['n_bursts']} burst pairs of {cfg['lines_per_burst']}x"
+            f"{cfg['samples_per_burst']} CInt16, {cfg['overlap_lines']}-line overlaps, DEM "
+            f"{cfg['dem_lines']}x{cfg['dem_pixels']}")
 
 
 def main():
@@ -241,8 +280,6 @@ def main():
     stream.synchronize()
 
     # ---- device-resident batched form
-    B = P.buffers()
-
     def step():
         T.check(T.lib.tops_pair_run_graph(P._h, C.c_void_p(sp)), "run_graph")
 
@@ -264,6 +301,7 @@ def main():
     if world > 1:
         dist.barrier()
     ms = e0.elapsed_time(e1) / args.steps
+    launches_per_step = P.buffers().n_launches   # counted by the runs above
     ms_t = torch.tensor([ms], device="cuda")
     if world > 1:
         dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
@@ -320,9 +358,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 geometry)",
         "data": "synthetic (seeded); inputs > L2, no flush needed",
-        "config": {"workload": f"{args.config}: {nb} burst pairs of {L}x{W} CInt16, "
-                               f"{cfg['overlap_lines']}-line overlaps, DEM "
-                               f"{cfg['dem_lines']}x{cfg['dem_pixels']}",
+        "config": {"workload": workload_name(args.config, cfg),
                    "window": f"{WIN_RG}x{WIN_AZ}", "form": "device-resident batched, CUDA graph",
                    "l2": "inputs larger than L2 (no flush)"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
@@ -333,7 +369,8 @@ def main():
                   "ms_per_step": float(np.mean(plain_ms)) if plain_ms else None,
                   "batched_over_plain_device": (value / world / plain_value) if plain_value else None,
                   "e2e_over_plain": (e2e_value / world / plain_value) if plain_value else None},
-        "gpu_launches": args.steps * B.n_launches if B.n_launches else None,
+        "gpu_launches": args.steps * launches_per_step,
+        "gpu_launches_per_step": launches_per_step,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "kernel": "resample_kernel",
                      "algorithmic_bytes_per_launch": rs_bytes, "launch_ms": rs_ms,
@@ -342,8 +379,8 @@ def main():
         "clocks": clk.summary(),
         "scene_gen_s": gen_s,
     }
-    if not args.no_cpu and rank == 0:
-        v, nthreads, sample = cpu_sample(cfg)
+    if not args.no_cpu and rank == 0 and world == 1:
+        v, nthreads, sample = cpu_baseline(S)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port",
                                 "sample": sample}
     if rank == 0:

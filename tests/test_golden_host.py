@@ -1,0 +1,76 @@
+"""Oracle and product host code against the reference's own host precomputes.
+
+tests/golden/ref_host.npz was written by tests/golden/make_golden.py from the
+reference's Func.cpp functions (built into oracle/_ref/ by oracle/ref/):
+Polyfit_Orbit (Func.cpp:1050-1126), ComputeDerampPara (1868-2099),
+InKernelInit (2105-2158), EstOverlapSize and GetSpectralSep (2935-2976).
+Both the product's host code and the oracle reproduce every value bit for bit.
+"""
+import hashlib
+
+import numpy as np
+import pytest
+
+from golden_io import load, swath_info
+
+H = load("ref_host.npz")
+TAGS = ("m", "s")
+
+
+def _rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def _sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a, np.float32).tobytes()).hexdigest()
+
+
+@pytest.mark.parametrize("case", range(len(H["lut_params"])))
+def test_lut_bit_identical_to_reference(T, O, case):
+    prf, abw, rsr2x = (float(v) for v in H["lut_params"][case])
+    want_az, want_rg = H["lut_sha256"][case]
+    kaz, krg = T.lut(prf, abw, rsr2x)
+    assert _sha(kaz) == want_az and _sha(krg) == want_rg
+    oaz, org = O.lut(prf, abw, rsr2x)
+    assert _sha(oaz) == want_az and _sha(org) == want_rg
+    if case == 0:
+        assert np.array_equal(kaz, H["lut_kaz"]) and np.array_equal(krg, H["lut_krg"])
+
+
+@pytest.mark.parametrize("tag", TAGS)
+def test_polyfit_orbit_matches_reference(T, O, tag):
+    t, x, y, z = H[f"{tag}_sv"]
+    want = [H[f"{tag}_c{a}"] for a in "xyz"]
+    for got in (T.polyfit_orbit(t, x, y, z), O.polyfit_orbit(t, x, y, z)):
+        for g, w in zip(got, want):
+            assert np.array_equal(g, w), (g, w)
+
+
+@pytest.mark.parametrize("tag", TAGS)
+@pytest.mark.parametrize("dc", ["", "_interp"])
+def test_deramp_params_match_reference(T, O, tag, dc):
+    """Per-burst DC (copied per burst when the annotation has more estimates
+    than bursts, interpolated by computeDC otherwise), FM rate, reference
+    time and kt (Func.cpp:1938-2093)."""
+    info = swath_info(T, H, tag, "dc_list" + dc)
+    coefs = [H[f"{tag}_c{a}"] for a in "xyz"]
+    got_p = T.swath_deramp_params(info, coefs, len(coefs[0]))
+    got_o = O.deramp_params(info, coefs)
+    for got in (got_p, got_o):
+        for k, ref in (("dc", "dc"), ("fmrate", "fm"), ("tref", "tref"), ("kt", "kt")):
+            want = H[f"{tag}_{ref}{dc}"]
+            assert np.array_equal(got[k], want), (k, _rel(got[k], want))
+
+
+@pytest.mark.parametrize("tag", TAGS)
+def test_overlap_and_spectral_sep_match_reference(T, O, tag):
+    first, last = H[f"{tag}_burst_first"], H[f"{tag}_burst_last"]
+    dt = float(H[f"{tag}_reals"][0])
+    L = int(H[f"{tag}_ints"][1])
+    for ov, tot, mx in (T.overlap_size(first, last, dt), O.overlap_size(first, last, dt)):
+        assert np.array_equal(ov, H[f"{tag}_ov"])
+        assert [tot, mx] == list(H[f"{tag}_ov_total_max"])
+    kt = H[f"{tag}_kt"]
+    want = float(H[f"{tag}_spec_sep"])
+    assert T.spectral_sep(kt, L, dt) == want
+    assert O.spectral_sep(kt, L, dt) == want
