@@ -156,7 +156,14 @@ __global__ void __launch_bounds__(ES_NT) esd_kernel(const __grid_constant__ EsBa
           accr += dre * inv;
           acci += dim * inv;
         } else {
-          accr += 1.f;  // atan2(0, 0) = 0 -> (1, 0), as the reference
+          // An exactly-zero double difference (a slave sample outside its
+          // box) has the phase atan2 gives its signed zeros: 0, -0, pi or
+          // -pi, as in MaskOut (EstESD.cu:149-155).  dre and dim carry the
+          // same signs of zero as the reference's cuCmulf products.
+          float sn, cs;
+          sincosf(atan2f(dim, dre), &sn, &cs);
+          accr += cs;
+          acci += sn;
         }
       }
     }

@@ -6,20 +6,33 @@
 // copies the int DEM with N * sizeof(short) bytes (Geocoreg_cuda.cu:788), so
 // the second half of its device DEM is never written and the fit would depend
 // on whatever that memory holds.  While GeoCoreg_warp_cuda_full_dem runs, the
-// one host-to-device copy whose source is the caller's DEM is widened to the
-// whole array.  Nothing else in the reference's code path changes.
+// one host-to-device copy whose source is the caller's DEM copies the whole
+// array instead, from a private copy of it: the reference page-locks only the
+// first N * sizeof(short) bytes of the caller's buffer (Geocoreg_cuda.cu:684),
+// and a whole-array copy from that buffer would straddle the page-locked
+// range.  Nothing else in the reference's code path changes.  Failing copies are reported on stderr,
+// because the reference ends the process with exit(0) on any CUDA error.
 #include <cuda_runtime.h>
 
 #include <cstddef>
+#include <cstdio>
+#include <cstring>
+#include <vector>
 
 namespace {
 const void *g_dem_host = nullptr;
-size_t g_dem_bytes = 0;
+std::vector<int> g_dem_copy;
 
 cudaError_t full_dem_memcpy(void *dst, const void *src, size_t bytes, cudaMemcpyKind kind) {
-  if (kind == cudaMemcpyHostToDevice && src != nullptr && src == g_dem_host && bytes < g_dem_bytes)
-    bytes = g_dem_bytes;
-  return cudaMemcpy(dst, src, bytes, kind);
+  cudaError_t e;
+  if (kind == cudaMemcpyHostToDevice && src != nullptr && src == g_dem_host)
+    e = cudaMemcpy(dst, g_dem_copy.data(), g_dem_copy.size() * sizeof(int), kind);
+  else
+    e = cudaMemcpy(dst, src, bytes, kind);
+  if (e != cudaSuccess)
+    fprintf(stderr, "geocoreg_full_dem: cudaMemcpy of %zu bytes failed: %s\n", bytes,
+            cudaGetErrorString(e));
+  return e;
 }
 }  // namespace
 
@@ -41,7 +54,7 @@ extern "C" void GeoCoreg_warp_cuda_full_dem(
     double *m_x_coef, double *m_y_coef, double *m_z_coef, double *s_x_coef, double *s_y_coef,
     double *s_z_coef, double m_aziInitial, double s_aziInitial) {
   g_dem_host = inputDEM;
-  g_dem_bytes = (size_t)DemLines * (size_t)DemPixels * sizeof(int);
+  g_dem_copy.assign(inputDEM, inputDEM + (size_t)DemLines * (size_t)DemPixels);
   GeoCoreg_warp_cuda(m_burstIdx, s_burstIdx, xmin, xmax, ymin, ymax, dem_DeltaLat, dem_DeltaLon,
                      DemLines, DemPixels, AzCpm, RgCpm, lat0, lon0, demnodata,
                      m_azimuthTimeInterval, s_azimuthTimeInterval, wavelength, m_linesPerBurst,
@@ -52,5 +65,5 @@ extern "C" void GeoCoreg_warp_cuda_full_dem(
                      m_nearRangeOnLeft, s_nearRangeOnLeft, inputDEM, m_x_coef, m_y_coef, m_z_coef,
                      s_x_coef, s_y_coef, s_z_coef, m_aziInitial, s_aziInitial);
   g_dem_host = nullptr;
-  g_dem_bytes = 0;
+  g_dem_copy.clear();
 }

@@ -135,7 +135,7 @@ int orc_polyfit_orbit(int npts, const double *t, const double *x, const double *
   int degree = (npts > 6) ? 5 : npts - 2;
   int nu = degree + 1;
   double *a = (double *)malloc(sizeof(double) * npts * nu);
-  double n[64], rx[8], ry[8], rz[8];
+  double n[64] = {0}, rx[8] = {0}, ry[8] = {0}, rz[8] = {0};
   for (int i = 0; i < npts; i++)
     for (int j = 0; j < nu; j++) a[i * nu + j] = pow(nt[i], j);
   mat_t_mat(a, a, n, npts, nu, nu);
@@ -656,11 +656,11 @@ void orc_esd(const int16_t *mF, const int16_t *mB, const float *sF, const float 
         double dre = fr * br + fi * bi, dim = fi * br - fr * bi;
         /* MaskOut (:130-161) */
         if (g < thr || g >= 1) continue;
-        /* An exactly-zero double difference (slave outside its box) has no
-         * phase; the reference's atan2 then depends on the signs of zero of
-         * its FP32 products.  Both the oracle and the kernel use
-         * atan2(+0, +0) = 0, i.e. the phasor (1, 0). */
-        double th = (dre == 0 && dim == 0) ? 0.0 : atan2(dim, dre);
+        /* An exactly-zero double difference (slave outside its box) gets
+         * the phase atan2 gives its signed zeros (0, -0, pi or -pi), as the
+         * reference's MaskOut does; the products above produce the same
+         * signs of zero as its FP32 cuCmulf chain. */
+        double th = atan2(dim, dre);
         ar += cos(th);
         ai += sin(th);
         used++;

@@ -294,16 +294,29 @@ def _rs_args(F, H, b, cpm_az, cpm_rg, shift, dt, out, kaz, krg):
     return args, keep
 
 
+def _say(msg):
+    print(msg, flush=True)
+
+
+def _loaded_cudart():
+    with open("/proc/self/maps") as f:
+        return sorted({ln.split()[-1] for ln in f if "libcudart" in ln})
+
+
 def stages(out_path, host_path):
     F = make_scene()
     H = dict(np.load(host_path))
     R, Co, E, G = _stage_libs()
+    _say(f"CUDA runtime: {_loaded_cudart()}")
     nb, L, W, _ = (int(v) for v in F["m_ints"])
     kaz = iso(H["lut_kaz"])
     krg = iso(H["lut_krg"])
     res = dict(F)
     # geometric coregistration
-    cpm = [ref_geocoreg(G, F, H, b) for b in range(nb)]
+    cpm = []
+    for b in range(nb):
+        cpm.append(ref_geocoreg(G, F, H, b))
+        _say(f"geocoreg burst {b}: az {cpm[-1][0]} rg {cpm[-1][1]}")
     res["cpm_az"] = np.array([c[0] for c in cpm])
     res["cpm_rg"] = np.array([c[1] for c in cpm])
     assert np.all(np.isfinite(res["cpm_az"])) and np.all(np.isfinite(res["cpm_rg"]))
@@ -316,6 +329,7 @@ def stages(out_path, host_path):
                               s_dt, out, kaz, krg)
         R.DerampDemodResample(*args)
         reslave[b] = out
+        _say(f"resample burst {b}: mean |out| {np.abs(out).mean():.3f}")
     res["reslave"] = reslave
     # ESD on the overlap bands
     ov = iso(H["m_ov"], np.int32)
@@ -334,6 +348,7 @@ def stages(out_path, host_path):
                        int(ov.max()), ESD_THRESHOLD, spec, m_dt)
         assert np.all(np.isfinite(shift)), shift
         res[f"esd_shift_{wr}x{wa}"] = np.array(shift)
+        _say(f"ESD {wr}x{wa}: {shift}")
     # ESD resample + coherence, for each window
     for wr, wa in WINDOWS:
         shifts = res[f"esd_shift_{wr}x{wa}"].copy()
@@ -360,6 +375,7 @@ def stages(out_path, host_path):
                 Co.CoherenceEst(0, b * L, W, L, (wr - 1) // 2, (wa - 1) // 2, wr, wa,
                                 master.ctypes.data, d, _ptr(c, C.c_float))
             coh[b] = c
+            _say(f"ESD resample + coherence {wr}x{wa} burst {b}: mean coh {np.nanmean(c):.4f}")
         res[f"reslave_esd_{wr}x{wa}"] = reslave_esd
         res[f"coh_{wr}x{wa}"] = coh
     np.savez_compressed(out_path, **res)
