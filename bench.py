@@ -214,6 +214,96 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+# Three sub-swaths of 9 bursts with uneven sizes (seeded): lines drawn from
+# 1450-1550 and samples from 18000-25500 per sub-swath.
+BATCH_SEED = 4
+
+
+def batch_shapes():
+    rng = np.random.default_rng(BATCH_SEED)
+    return [dict(n_bursts=9, lines_per_burst=int(rng.integers(1450, 1551)),
+                 samples_per_burst=int(rng.integers(18000, 25501)), overlap_lines=100,
+                 dem_lines=3600, dem_pixels=3600, seed=40 + k) for k in range(3)]
+
+
+def run_batch(args, rank, world):
+    """Batched uneven bursts: the 3 sub-swath pairs as one batch (one launch
+    per stage, autotuned tiles, one CUDA graph) against the per-burst launch
+    loop on the same device-resident data."""
+    import torch
+    import topsb200 as T
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    shapes = batch_shapes()
+    t0 = time.time()
+    scenes = [T.Scene(**sh) for sh in shapes]
+    gen_s = time.time() - t0
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+    opts = T.pair_opts(win_rg=WIN_RG, win_az=WIN_AZ)
+    plans = []
+    for S in scenes:
+        P = T.Pair(S.swath[0], S.swath[1], S.dem.shape, opts)
+        di = S.dem_info
+        P.set_dem(S.dem, di.lat0, di.lon0, di.dlat, di.dlon, T.scene_windows(S), sp)
+        P.upload(S.slc[0], S.slc[1], sp)
+        plans.append(P)
+    stream.synchronize()
+    B = T.Batch(plans)
+    tune, stage_ms = B.autotune(sp)
+    n_pairs = sum(sh["n_bursts"] for sh in shapes)
+    npx = sum(sh["n_bursts"] * sh["lines_per_burst"] * sh["samples_per_burst"] for sh in shapes)
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        stream.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        stream.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        ms_batch = timed(lambda: B.run(sp, graph=True), args.steps, args.warmup)
+    launches_batch = B.launches()
+
+    def loop():
+        for P in plans:
+            P.run_per_burst(sp)
+    ms_loop = timed(loop, max(2, args.steps // 4), 1)
+    launches_loop = sum(P.buffers().n_launches for P in plans)
+    value = world * n_pairs * 1e3 / ms_batch
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_batch, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 geometry)",
+        "data": "synthetic (seeded); inputs > L2, no flush needed",
+        "config": {"workload": "batch: 3 sub-swath pairs x 9 bursts, uneven sizes " +
+                               ", ".join(f"{sh['lines_per_burst']}x{sh['samples_per_burst']}"
+                                         for sh in shapes),
+                   "window": f"{WIN_RG}x{WIN_AZ}",
+                   "form": "one batch: one launch per stage for all 27 bursts, CUDA graph"},
+        "tune": {"rs_seg_rows": tune.rs_seg_rows, "rs_persistent": tune.rs_persistent,
+                 "coh_seg_rows": tune.coh_seg_rows, "coh_persistent": tune.coh_persistent,
+                 "resample_esd_ms": float(stage_ms[0]), "coherence_ms": float(stage_ms[1])},
+        "gpu_launches": args.steps * launches_batch, "gpu_launches_per_step": launches_batch,
+        "per_burst_loop": {"value": n_pairs * 1e3 / ms_loop, "unit": UNIT, "ms_per_step": ms_loop,
+                           "launches_per_step": launches_loop,
+                           "batched_over_loop": ms_loop / ms_batch},
+        "resample_roofline": {"achieved_gbs": 12.0 * npx / (float(stage_ms[0]) * 1e6),
+                              "peak_gbs": peaks()[0],
+                              "frac": 12.0 * npx / (float(stage_ms[0]) * 1e6) / peaks()[0]},
+        "clocks": clk.summary(), "scene_gen_s": gen_s,
+    }
+    print(json.dumps(line), flush=True)
+    B.close()
+    for P in plans:
+        P.close()
+
+
 def workload_name(name, cfg):
     return (f"{name}: {cfg['n_bursts']} burst pairs of {cfg['lines_per_burst']}x"
             f"{cfg['samples_per_burst']} CInt16, {cfg['overlap_lines']}-line overlaps, DEM "
@@ -226,7 +316,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="subswath", choices=sorted(CONFIGS))
+    ap.add_argument("--config", default="subswath", choices=sorted(CONFIGS) + ["batch"])
     ap.add_argument("--e2e-steps", type=int, default=6)
     ap.add_argument("--plain-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
@@ -236,6 +326,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.config == "batch":
+        return run_batch(args, rank, world)
 
     import torch
     import torch.distributed as dist

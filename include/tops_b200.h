@@ -160,9 +160,21 @@ typedef struct {
                                       `out` points at the row out_row0 */
 } tops_resample_job;
 
+/* Precision of the deramp phase inside the resample kernel.
+ *   TOPS_PREC_SPLIT  FP32 phase residual and reduced phase per sample,
+ *                    relative to an FP64 reference-column phase reduced
+ *                    mod 2 pi once per row (double-single); the default.
+ *   TOPS_PREC_FP64   every sample's deramp phase and its reduction in FP64.
+ * Positions, LUT bins and the row phase are FP64 in both. */
+#define TOPS_PREC_SPLIT 0
+#define TOPS_PREC_FP64 1
+
 /* Resamples njobs bursts in one launch on `stream` (cudaStream_t). */
 int tops_resample(const tops_lut_dev *lut, const tops_resample_job *jobs, int njobs,
                   void *stream);
+/* As tops_resample, with the precision mode (TOPS_PREC_*) chosen explicitly. */
+int tops_resample_ex(const tops_lut_dev *lut, const tops_resample_job *jobs, int njobs,
+                     int precision, void *stream);
 
 /* One burst of windowed coherence (device pointers, byte pitches). */
 typedef struct {

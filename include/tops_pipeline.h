@@ -38,6 +38,8 @@ typedef struct {
                                0: only the overlap bands ESD needs */
   int burst0_deramp_rows;   /* 1: deramp rows of burst 0 for every burst, as
                                the reference passes them (Func.cpp:2383) */
+  int precision;            /* resample deramp phase: TOPS_PREC_SPLIT (default)
+                               or TOPS_PREC_FP64 */
 } tops_pair_opts;
 
 int tops_pair_opts_default(tops_pair_opts *o);
@@ -100,6 +102,44 @@ int tops_plain_pair(const tops_swath_info *master, const tops_swath_info *slave,
                     const tops_dem_window *windows, const void *master_slc,
                     const void *slave_slc, void *reslave, void *reslave_esd, float *coh,
                     double *cpm, double *shifts);
+
+/* Every stage launched once per burst (or overlap), as the reference's
+ * drivers call their stages, on device-resident data: the per-burst launch
+ * loop that the batched forms are compared with.  Same outputs as
+ * tops_pair_run. */
+int tops_pair_run_per_burst(tops_pair *p, void *stream);
+
+/* ============================================== batched sub-swath pairs
+ * Several plans -- e.g. the 3 sub-swaths of a product, whose bursts differ in
+ * lines and samples -- processed together: one launch per stage for all
+ * their bursts (each job keeps its own boxes, LUT and polynomials), the
+ * resample and coherence kernels optionally persistent over a work queue,
+ * and the whole batch capturable as one CUDA graph.  The plans must have
+ * their DEM set and share the window, threshold and precision options; they
+ * stay owned by the caller, and their outputs are read with
+ * tops_pair_download as usual. */
+typedef struct tops_batch tops_batch;
+
+/* Tile and scheduling of the resample and coherence launches. */
+typedef struct {
+  int rs_seg_rows;      /* resample output rows per work item, 16..256 (0: 256) */
+  int rs_persistent;    /* 1: persistent kernel pulling items from a queue */
+  int coh_seg_rows;     /* coherence rows per work item, 8..512 (0: 128) */
+  int coh_persistent;
+} tops_tune;
+
+int tops_batch_create(tops_pair *const *pairs, int n_pairs, tops_batch **out);
+int tops_batch_destroy(tops_batch *b);
+int tops_batch_run(tops_batch *b, void *stream);
+int tops_batch_run_graph(tops_batch *b, void *stream);
+/* Kernels the last tops_batch_run launched. */
+int tops_batch_launches(const tops_batch *b);
+int tops_batch_set_tune(tops_batch *b, const tops_tune *t);
+int tops_batch_get_tune(const tops_batch *b, tops_tune *t);
+/* Times every candidate tile of the resample and coherence stages on this
+ * batch (CUDA events on `stream`, synchronous) and keeps the fastest; best_ms
+ * (optional, 2 doubles) receives the two stage times. */
+int tops_batch_autotune(tops_batch *b, void *stream, tops_tune *best, double *best_ms);
 
 #ifdef __cplusplus
 }

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "launch.h"
 
 namespace tops {
 
@@ -24,7 +25,8 @@ int fill_resample_job(const tops_resample_job &u, ResampleJob &J);
 int fill_coh_job(const tops_coh_job &u, CohJob &J);
 int fill_esd_overlap(const tops_esd_overlap &u, EsdOverlap &O);
 int fill_geo_job(const tops_geo_job &u, GeoJob &J);
-int launch_coherence(const CohJob *jobs, int njobs, int win_rg, int win_az, cudaStream_t st);
+int launch_coherence(const CohJob *jobs, int njobs, int win_rg, int win_az, const TileCfg &cfg,
+                     cudaStream_t st);
 int launch_esd(const EsdOverlap *ovs, int n_ov, int win_az, int win_rg, float thr,
                double *shifts, double *sums, void *scratch, size_t scratch_bytes,
                cudaStream_t st);
@@ -184,7 +186,7 @@ static int coherence_host(int Dw, int Dh, int dx, int dy, int winRg, int winAz,
   tops_coh_job j{d_m, mpitch, d_slave, (size_t)Dw * 8, static_cast<float *>(d_c), cpitch, Dh, Dw};
   CohJob J;
   TOPS_TRY(fill_coh_job(j, J));
-  TOPS_TRY(launch_coherence(&J, 1, winRg, winAz, st));
+  TOPS_TRY(launch_coherence(&J, 1, winRg, winAz, TileCfg(), st));
   TOPS_CUDA_TRY(cudaMemcpy2DAsync(cohdata, (size_t)Dw * 4, d_c, cpitch, (size_t)Dw * 4, Dh,
                                   cudaMemcpyDeviceToHost, st));
   TOPS_CUDA_TRY(cudaStreamSynchronize(st));

@@ -10,48 +10,106 @@
 //
 // B200 design: one CTA per (strip of CO_TW columns, segment of rows).  Each
 // thread owns one loaded column and walks the segment in groups of CO_GR
-// rows: it reads master (CInt16) and slave (complex64) once per row with
-// coalesced loads, forms the four products and accumulates the vertical box
-// sums for the group's rows in registers.  The vertical sums go to shared
-// memory; the horizontal box is a sliding sum over 8 consecutive outputs per
-// thread, written with 16-byte stores.  The azimuth window is a template
-// parameter for the common sizes (3 and the reference's 6).  HBM traffic is the algorithmic
-// 4 + 8 + 4 bytes per pixel plus the column halo.
+// rows.  For the common azimuth windows (template WAZ = 3 and the
+// reference's 6) the products (m s*, |s|^2, |m|^2) of the last WAZ - 1 input
+// rows stay in registers from one group to the next, so every input row is
+// read once, and the loads of the next group are issued before the
+// horizontal pass of the current one, so HBM latency overlaps the shared-
+// memory work.  The vertical sums go to shared memory; the horizontal box is
+// a sliding sum over CO_CPI consecutive outputs per thread, written with
+// 16-byte stores.  Other window heights (WAZ = 0) reload the halo rows of
+// each group.  HBM traffic is the algorithmic 4 + 8 + 4 bytes per pixel plus
+// the column halo.
 #include <cuda_runtime.h>
 
 #include <vector>
 
 #include "common.cuh"
+#include "launch.h"
 
 namespace tops {
 
 constexpr int CO_NT = 256;
 constexpr int CO_TW = 224;   // output columns per strip (win_rg <= 33)
 constexpr int CO_GR = 8;     // rows per group
-constexpr int CO_SEG = 64;   // rows per work item
+constexpr int CO_SEG = 128;  // rows per work item
 constexpr int CO_CPI = 8;    // output columns per horizontal item
 constexpr int CO_MAXJOBS = 32;
 constexpr int CO_MAX_WIN_RG = CO_NT - CO_TW + 1;
 
 struct CoBatch {
   int njobs, total_items, win_rg, win_az;
+  int *counter;            // persistent launch: work-item queue (else null)
   CohJob jobs[CO_MAXJOBS];
 };
 
 struct CoShared {
   float4 V[CO_GR][pad8(CO_NT)];      // vertical sums (re, im, |s|^2, |m|^2), pad8(x)
   float judge[CO_GR][pad8(CO_NT)];   // |s|^2 of the centre pixel, pad8(x)
+  int next_item;                     // persistent launch: the item just taken
 };
 
-// WAZ > 0: azimuth window known at compile time (the vertical box is fully
-// unrolled); WAZ == 0: runtime window.  The amplitude mask |s| < 0.001 of
-// the reference (EstCoh.cu:393, 446) is evaluated as |s|^2 < 1e-6.
+__device__ __forceinline__ float4 coh_product(short2 m, float2 s) {
+  const float mr = m.x, mi = m.y;
+  return make_float4(mr * s.x + mi * s.y,   // m * conj(s)
+                     mi * s.x - mr * s.y, s.x * s.x + s.y * s.y, mr * mr + mi * mi);
+}
+
+__device__ __forceinline__ void add4(float4 &a, const float4 &b) {
+  a.x += b.x;
+  a.y += b.y;
+  a.z += b.z;
+  a.w += b.w;
+}
+
+// Horizontal pass of one group: CO_CPI consecutive outputs per item.  The
+// amplitude mask |s| < 0.001 of the reference (EstCoh.cu:393, 446) is
+// evaluated as |s|^2 < 1e-6.
+__device__ __forceinline__ void coh_horizontal(const CoShared &S, const CohJob &J, int tid,
+                                               int rg, int gr, int c0, int cN, int win_rg,
+                                               int dx) {
+  constexpr int NG = CO_TW / CO_CPI;
+  for (int it = tid; it < gr * NG; it += CO_NT) {
+    const int k = it / NG;
+    const int cg = (it - k * NG) * CO_CPI;
+    if (cg >= cN) continue;
+    float4 w = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int i = 0; i < win_rg; i++) add4(w, S.V[k][pad8(cg + i)]);
+    float out[CO_CPI];
+#pragma unroll
+    for (int u = 0; u < CO_CPI; u++) {
+      if (u > 0) {
+        const float4 a = S.V[k][pad8(cg + u - 1 + win_rg)];
+        const float4 b = S.V[k][pad8(cg + u - 1)];
+        w.x += a.x - b.x;
+        w.y += a.y - b.y;
+        w.z += a.z - b.z;
+        w.w += a.w - b.w;
+      }
+      const float p = w.z * w.w;
+      float g = (p > 0.f) ? sqrtf(w.x * w.x + w.y * w.y) * rsqrtf(p) : 0.f;
+      if (S.judge[k][pad8(cg + u + dx)] < 1e-6f) g = 0.f;
+      out[u] = g;
+    }
+    float *orow = J.coh + (long)(rg + k) * J.coh_pitch + c0 + cg;
+    if (cg + CO_CPI <= cN && ((reinterpret_cast<uintptr_t>(orow) & 15) == 0)) {
+#pragma unroll
+      for (int u = 0; u < CO_CPI; u += 4)
+        *reinterpret_cast<float4 *>(orow + u) = make_float4(out[u], out[u + 1], out[u + 2],
+                                                            out[u + 3]);
+    } else {
+#pragma unroll
+      for (int u = 0; u < CO_CPI; u++)
+        if (cg + u < cN) orow[u] = out[u];
+    }
+  }
+}
+
+// One work item (strip x segment of one job); all threads of the CTA call it
+// with the same item.
 template <int WAZ>
-__global__ void __launch_bounds__(CO_NT) coherence_kernel(const __grid_constant__ CoBatch B) {
-  __shared__ CoShared S;
+__device__ __forceinline__ void coherence_item(CoShared &S, const CoBatch &B, int item) {
   const int tid = threadIdx.x;
-  const int item = blockIdx.x;
-  if (item >= B.total_items) return;
   int jb = 0;
   while (jb + 1 < B.njobs && B.jobs[jb + 1].item_begin <= item) jb++;
   const CohJob &J = B.jobs[jb];
@@ -67,147 +125,183 @@ __global__ void __launch_bounds__(CO_NT) coherence_kernel(const __grid_constant_
   const int r_end = min(r_begin + J.seg_rows, J.lines);
   const int x = c0 - dx + tid;          // this thread's loaded column
   const bool xin = tid < nload && x >= 0 && x < J.pixels;
-
-  for (int rg = r_begin; rg < r_end; rg += CO_GR) {
-    const int gr = min(CO_GR, r_end - rg);
-    // ---- vertical pass: input rows rg-dy .. rg-dy+gr+win_az-2
-    float4 acc[CO_GR];
-    float judge[CO_GR];
-#pragma unroll
-    for (int k = 0; k < CO_GR; k++) {
-      acc[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-      judge[k] = 0.f;
+  auto load = [&](int y, short2 &m, float2 &s) {
+    m = make_short2(0, 0);
+    s = make_float2(0.f, 0.f);
+    if (xin && y >= 0 && y < J.lines) {
+      m = J.master[(long)y * J.master_pitch + x];
+      s = J.slave[(long)y * J.slave_pitch + x];
     }
-    const int nin = gr + win_az - 1;
-    auto product = [&](short2 m, float2 s) {
-      const float mr = m.x, mi = m.y;
-      return make_float4(mr * s.x + mi * s.y,   // m * conj(s)
-                         mi * s.x - mr * s.y, s.x * s.x + s.y * s.y, mr * mr + mi * mi);
-    };
-    auto load = [&](int q, short2 &m, float2 &s) {
-      const int y = rg - dy + q;
-      m = make_short2(0, 0);
-      s = make_float2(0.f, 0.f);
-      if (xin && q < nin && y >= 0 && y < J.lines) {
-        m = J.master[(long)y * J.master_pitch + x];
-        s = J.slave[(long)y * J.slave_pitch + x];
+  };
+
+  if constexpr (WAZ > 0) {
+    // products of input rows: q[0 .. WAZ-2] carried, then the group's rows
+    constexpr int NQ = WAZ > 0 ? WAZ - 1 : 1;
+    float4 q[NQ];
+    {
+      // rows r_begin - dy .. r_begin - dy + WAZ - 2 (the first group's halo)
+#pragma unroll
+      for (int j = 0; j < NQ; j++) {
+        short2 m;
+        float2 s;
+        load(r_begin - dy + j, m, s);
+        q[j] = coh_product(m, s);
       }
-    };
-    if (WAZ > 0) {
-      // all loads of the group first (memory-level parallelism), then math
-      constexpr int NQ = CO_GR + (WAZ > 0 ? WAZ : 1) - 1;
-      short2 mv[NQ];
-      float2 sv[NQ];
+    }
+    // loads of the first group: input rows r_begin - dy + WAZ - 1 + k
+    short2 mv[CO_GR];
+    float2 sv[CO_GR];
 #pragma unroll
-      for (int q = 0; q < NQ; q++) load(q, mv[q], sv[q]);
+    for (int k = 0; k < CO_GR; k++) load(r_begin - dy + WAZ - 1 + k, mv[k], sv[k]);
+    for (int rg = r_begin; rg < r_end; rg += CO_GR) {
+      const int gr = min(CO_GR, r_end - rg);
+      float4 p[NQ + CO_GR];
 #pragma unroll
-      for (int q = 0; q < NQ; q++) {
-        const float4 p = product(mv[q], sv[q]);
+      for (int j = 0; j < NQ; j++) p[j] = q[j];
 #pragma unroll
-        for (int k = 0; k < CO_GR; k++) {
-          if (q - k >= 0 && q - k < WAZ) {
-            acc[k].x += p.x;
-            acc[k].y += p.y;
-            acc[k].z += p.z;
-            acc[k].w += p.w;
-          }
-          if (q == k + (WAZ - 1) / 2) judge[k] = p.z;
-        }
+      for (int k = 0; k < CO_GR; k++) p[NQ + k] = coh_product(mv[k], sv[k]);
+      // issue the next group's loads now; they land during the rest
+      const int rn = rg + CO_GR;
+      if (rn < r_end) {
+#pragma unroll
+        for (int k = 0; k < CO_GR; k++) load(rn - dy + WAZ - 1 + k, mv[k], sv[k]);
       }
-    } else {
-      for (int q = 0; q < nin; q++) {
+#pragma unroll
+      for (int k = 0; k < CO_GR; k++) {
+        float4 a = p[k];
+#pragma unroll
+        for (int j = 1; j < WAZ; j++) add4(a, p[k + j]);
+        S.V[k][pad8(tid)] = a;
+        S.judge[k][pad8(tid)] = p[k + dy].z;
+      }
+#pragma unroll
+      for (int j = 0; j < NQ; j++) q[j] = p[CO_GR + j];
+      __syncthreads();
+      coh_horizontal(S, J, tid, rg, gr, c0, cN, win_rg, dx);
+      __syncthreads();
+    }
+  } else {
+    for (int rg = r_begin; rg < r_end; rg += CO_GR) {
+      const int gr = min(CO_GR, r_end - rg);
+      // vertical pass: input rows rg-dy .. rg-dy+gr+win_az-2
+      float4 acc[CO_GR];
+      float judge[CO_GR];
+#pragma unroll
+      for (int k = 0; k < CO_GR; k++) {
+        acc[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+        judge[k] = 0.f;
+      }
+      const int nin = gr + win_az - 1;
+      for (int qi = 0; qi < nin; qi++) {
         short2 m;
         float2 sl;
-        load(q, m, sl);
-        const float4 p = product(m, sl);
+        load(rg - dy + qi, m, sl);
+        const float4 pr = coh_product(m, sl);
 #pragma unroll
         for (int k = 0; k < CO_GR; k++) {
-          const int j = q - k;
-          if (j >= 0 && j < win_az) {
-            acc[k].x += p.x;
-            acc[k].y += p.y;
-            acc[k].z += p.z;
-            acc[k].w += p.w;
-          }
-          if (q == k + dy) judge[k] = p.z;
+          const int j = qi - k;
+          if (j >= 0 && j < win_az) add4(acc[k], pr);
+          if (qi == k + dy) judge[k] = pr.z;
         }
       }
-    }
 #pragma unroll
-    for (int k = 0; k < CO_GR; k++) {
-      S.V[k][pad8(tid)] = acc[k];
-      S.judge[k][pad8(tid)] = judge[k];
+      for (int k = 0; k < CO_GR; k++) {
+        S.V[k][pad8(tid)] = acc[k];
+        S.judge[k][pad8(tid)] = judge[k];
+      }
+      __syncthreads();
+      coh_horizontal(S, J, tid, rg, gr, c0, cN, win_rg, dx);
+      __syncthreads();
     }
+  }
+}
+
+template <int WAZ>
+__global__ void __launch_bounds__(CO_NT, 3) coherence_kernel(const __grid_constant__ CoBatch B) {
+  __shared__ CoShared S;
+  // one work item per CTA, or (persistent) items from the queue until it
+  // is empty; a single call site keeps one inlined copy of the item code
+  int item = blockIdx.x;
+  if (B.counter) {
+    if (threadIdx.x == 0) S.next_item = atomicAdd(B.counter, 1);
     __syncthreads();
-    // ---- horizontal pass: CO_CPI consecutive outputs per item
-    constexpr int NG = CO_TW / CO_CPI;
-    for (int it = tid; it < gr * NG; it += CO_NT) {
-      const int k = it / NG;
-      const int cg = (it - k * NG) * CO_CPI;
-      if (cg >= cN) continue;
-      float4 w = make_float4(0.f, 0.f, 0.f, 0.f);
-      for (int i = 0; i < win_rg; i++) {
-        const float4 v = S.V[k][pad8(cg + i)];
-        w.x += v.x;
-        w.y += v.y;
-        w.z += v.z;
-        w.w += v.w;
-      }
-      float out[CO_CPI];
-#pragma unroll
-      for (int u = 0; u < CO_CPI; u++) {
-        if (u > 0) {
-          const float4 a = S.V[k][pad8(cg + u - 1 + win_rg)];
-          const float4 b = S.V[k][pad8(cg + u - 1)];
-          w.x += a.x - b.x;
-          w.y += a.y - b.y;
-          w.z += a.z - b.z;
-          w.w += a.w - b.w;
-        }
-        const float p = w.z * w.w;
-        float g = (p > 0.f) ? sqrtf(w.x * w.x + w.y * w.y) * rsqrtf(p) : 0.f;
-        if (S.judge[k][pad8(cg + u + dx)] < 1e-6f) g = 0.f;
-        out[u] = g;
-      }
-      float *orow = J.coh + (long)(rg + k) * J.coh_pitch + c0 + cg;
-      if (cg + CO_CPI <= cN && ((reinterpret_cast<uintptr_t>(orow) & 15) == 0)) {
-#pragma unroll
-        for (int u = 0; u < CO_CPI; u += 4)
-          *reinterpret_cast<float4 *>(orow + u) = make_float4(out[u], out[u + 1], out[u + 2],
-                                                              out[u + 3]);
-      } else {
-#pragma unroll
-        for (int u = 0; u < CO_CPI; u++)
-          if (cg + u < cN) orow[u] = out[u];
-      }
-    }
+    item = S.next_item;
+    __syncthreads();
+  }
+  while (item < B.total_items) {
+    coherence_item<WAZ>(S, B, item);
+    if (!B.counter) break;
+    if (threadIdx.x == 0) S.next_item = atomicAdd(B.counter, 1);
+    __syncthreads();
+    item = S.next_item;
     __syncthreads();
   }
 }
 
-int launch_coherence(const CohJob *jobs, int njobs, int win_rg, int win_az, cudaStream_t st) {
+template <int WAZ>
+static int launch_coh_t(const CoBatch &B, int grid, cudaStream_t st) {
+  coherence_kernel<WAZ><<<grid, CO_NT, 0, st>>>(B);
+  TOPS_CUDA_TRY(cudaGetLastError());
+  return TOPS_OK;
+}
+
+template <int WAZ>
+static int coh_resident(int dev) {
+  static int resident[kMaxDevices] = {};
+  if (!resident[dev]) {
+    int per_sm = 0, sms = 0;
+    TOPS_CUDA_TRY(
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, coherence_kernel<WAZ>, CO_NT, 0));
+    TOPS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    resident[dev] = per_sm * sms;
+  }
+  return resident[dev];
+}
+
+int launch_coherence(const CohJob *jobs, int njobs, int win_rg, int win_az, const TileCfg &cfg,
+                     cudaStream_t st) {
   if (win_rg < 1 || win_az < 1 || win_rg > CO_MAX_WIN_RG) return TOPS_E_INVALID;
-  for (int j0 = 0; j0 < njobs; j0 += CO_MAXJOBS) {
+  if (cfg.seg_rows < 0 || cfg.seg_rows > 512 || (cfg.seg_rows && cfg.seg_rows < CO_GR))
+    return TOPS_E_INVALID;
+  int dev = 0;
+  TOPS_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return TOPS_E_INVALID;
+  for (int j0 = 0, k = 0; j0 < njobs; j0 += CO_MAXJOBS, k++) {
     CoBatch B;
     B.njobs = 0;
     B.win_rg = win_rg;
     B.win_az = win_az;
+    B.counter = cfg.counters ? cfg.counters + k : nullptr;
     int items = 0;
     for (int j = j0; j < njobs && j < j0 + CO_MAXJOBS; j++) {
-      B.jobs[B.njobs] = jobs[j];
-      B.jobs[B.njobs].item_begin = items;
-      items += jobs[j].strips * jobs[j].segs;
+      CohJob &J = B.jobs[B.njobs];
+      J = jobs[j];
+      if (cfg.seg_rows) {
+        J.seg_rows = cfg.seg_rows;
+        J.segs = (J.lines + cfg.seg_rows - 1) / cfg.seg_rows;
+      }
+      J.item_begin = items;
+      items += J.strips * J.segs;
       B.njobs++;
     }
     B.total_items = items;
     if (!items) continue;
+    int grid = items;
+    if (B.counter) {
+      TOPS_CUDA_TRY(cudaMemsetAsync(B.counter, 0, sizeof(int), st));
+      const int res = win_az == 3 ? coh_resident<3>(dev)
+                      : win_az == 6 ? coh_resident<6>(dev) : coh_resident<0>(dev);
+      if (res <= 0) return TOPS_E_CUDA;
+      grid = min(items, cfg.grid > 0 ? cfg.grid : res);
+    }
+    int s;
     if (win_az == 3)
-      coherence_kernel<3><<<items, CO_NT, 0, st>>>(B);
+      s = launch_coh_t<3>(B, grid, st);
     else if (win_az == 6)
-      coherence_kernel<6><<<items, CO_NT, 0, st>>>(B);
+      s = launch_coh_t<6>(B, grid, st);
     else
-      coherence_kernel<0><<<items, CO_NT, 0, st>>>(B);
-    TOPS_CUDA_TRY(cudaGetLastError());
+      s = launch_coh_t<0>(B, grid, st);
+    if (s != TOPS_OK) return s;
   }
   return TOPS_OK;
 }
@@ -245,5 +339,21 @@ extern "C" int tops_coherence(const tops_coh_job *jobs, int njobs, int win_rg, i
     int s = fill_coh_job(jobs[j], J[j]);
     if (s != TOPS_OK) return s;
   }
-  return launch_coherence(J.data(), njobs, win_rg, win_az, static_cast<cudaStream_t>(stream));
+  return launch_coherence(J.data(), njobs, win_rg, win_az, TileCfg(),
+                          static_cast<cudaStream_t>(stream));
 }
+
+namespace tops {
+
+int coherence_launch(const tops_coh_job *jobs, int njobs, int win_rg, int win_az,
+                     const TileCfg &cfg, cudaStream_t st) {
+  if ((!jobs && njobs > 0) || njobs < 0) return TOPS_E_INVALID;
+  std::vector<CohJob> J(njobs);
+  for (int j = 0; j < njobs; j++) {
+    int s = fill_coh_job(jobs[j], J[j]);
+    if (s != TOPS_OK) return s;
+  }
+  return launch_coherence(J.data(), njobs, win_rg, win_az, cfg, st);
+}
+
+}  // namespace tops

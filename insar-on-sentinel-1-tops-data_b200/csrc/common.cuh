@@ -30,6 +30,7 @@ constexpr double kSol = 299792458.0;                // reference Constants.h:6
 constexpr int kInterval = 2047;                     // reference Constants.h:8
 constexpr int kLutBins = 2048;
 constexpr int kTaps = 12;
+constexpr int kMaxDevices = 64;
 constexpr double kTwoPiHi = 6.283185307179586232e+00;
 constexpr double kTwoPiLo = 2.449293598294706414e-16;
 constexpr double kInvTwoPi = 0.15915494309189533577;
@@ -56,12 +57,22 @@ __device__ __forceinline__ float reduce_2pi_f(float x) {
 }
 
 // ------------------------------------------------- internal job layouts
+// Device copies of the interpolation kernels (tops_lut_dev).
+struct LutPtrs {
+  const float *kaz, *krg;  // [2048][12]
+  const float4 *krg2;      // [2048][6]: range taps duplicated (w0,w0,w1,w1), ...
+  const float *sp1;        // [2048]: sum(krg row) - 1
+};
+
 // Device-side view of one resample job (built from tops_resample_job).
 struct ResampleJob {
+  LutPtrs lut;            // interpolation kernels of the job's sub-swath
   const short2 *slave;
   long slave_pitch;       // short2 elements per row
   float2 *out;
   long out_pitch;         // float2 elements per row
+  int slave_al8;          // slave base and pitch 8-byte aligned (pair loads)
+  int out_al16;           // output base and pitch 16-byte aligned (pair stores)
   const double *kt, *tref, *fdc;
   int mx0, mx1, my0, my1;
   int sx0, sx1, sy0, sy1;

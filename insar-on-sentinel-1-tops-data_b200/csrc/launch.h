@@ -1,0 +1,34 @@
+// launch.h -- library-internal launch controls of the resample and coherence
+// kernels, used by the batched plans (host/pipeline.cpp): the work-item tile
+// (rows per item) and the scheduling mode.
+//
+//   seg_rows  output rows per work item (0: the kernel's default); the
+//             resample kernel takes 16..256, the coherence kernel 8..512
+//   counters  if non-null: persistent launch.  `grid` CTAs (0: as many as
+//             fit on the device at once) pull work items from a queue -- the
+//             device int counters[k], set to 0 on the stream before the k-th
+//             launch of the call (a call launches once per 32 jobs).  The
+//             caller provides at least (njobs + 31) / 32 ints.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "tops_b200.h"
+
+namespace tops {
+
+struct TileCfg {
+  int seg_rows = 0;
+  int *counters = nullptr;
+  int grid = 0;
+};
+
+int resample_launch(const tops_lut_dev *lut, const tops_resample_job *jobs, int njobs,
+                    int precision, const TileCfg &cfg, cudaStream_t st);
+// As resample_launch with one LUT per job (sub-swaths of one batch differ in
+// PRF and bandwidth).
+int resample_launch_multi(const tops_lut_dev *const *luts, const tops_resample_job *jobs,
+                          int njobs, int precision, const TileCfg &cfg, cudaStream_t st);
+int coherence_launch(const tops_coh_job *jobs, int njobs, int win_rg, int win_az,
+                     const TileCfg &cfg, cudaStream_t st);
+
+}  // namespace tops

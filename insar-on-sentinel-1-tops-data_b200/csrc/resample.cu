@@ -12,36 +12,48 @@
 //             deramped slave d = s exp(i phi), reramped with the LUT-weighted
 //             sum of the deramp phase phi.
 //
-// B200 design (no textures, no phase array in HBM):
-//   * A CTA owns a strip of RS_TW output columns and sweeps a segment of
-//     output rows in groups of RS_GR rows.  Slave rows are deramped once
-//     into a ring of RS_FR rows x RS_FW columns in shared memory (complex
-//     float + a float phase residual), so the slave is read from HBM about
-//     once (the ring keeps the 11-row azimuth halo between groups).
-//   * Azimuth-first separable filtering shared across the row: when every
-//     interior pixel of a row segment uses the same (azimuth line, LUT bin),
-//     v(x) = sum_j kAz[j] d(L0-5+j, x) is computed once per slave column and
-//     reused by the 12 range taps of all pixels; the azimuth pass is
-//     register-blocked over 4 consecutive rows (15 ring loads serve 4 rows)
-//     and uses the packed FP32x2 FMA of sm_100 for the complex samples.
-//   * Phase: phi(y,x) = phi_ref(y) + G(y,x), phi_ref the FP64 phase of a
-//     reference column, G an FP32 residual of a few radians.  For a column,
-//     G is exactly quadratic in azimuth time, so its azimuth interpolation
-//     is sum_j kAz[j] G(y_j) = M0 G(L0) + dG/dt(L0) dt M1 + d2G dt^2 M2 with
-//     the LUT row moments M0..M2 -- three FMAs instead of twelve taps.  The
-//     interpolated phase is (1 + sp1) Psi_row + sum_i kRg[i] gamma(x_i),
-//     where Psi_row = sum_j kAz[j] phi_ref(y_j) is FP64 (reduced mod 2 pi)
-//     and 1 + sp1 = sum kRg.  This equals the reference's 144-tap FP64 phase
-//     sum in exact arithmetic with FP32 only on few-radian quantities.
-//   * Rows whose bins are not uniform, or pixels whose support leaves the
-//     ring window, take per-pixel paths (from the ring, else from HBM) that
-//     compute the same formula.
+// B200 design (no textures, no phase array in HBM).  A CTA owns a strip of
+// RS_TW output columns and sweeps a segment of output rows in groups of RS_GR
+// rows; per group:
+//   [A] Row statistics from the offset polynomials, not per pixel: along the
+//       strip y and x are quadratics in the column, so their range follows
+//       from the two ends and the vertex.  A row whose whole strip maps to one
+//       (azimuth line, LUT bin) key -- in a TOPS pair nearly every row -- gets
+//       one shared azimuth pass.  The same bounds give the slave lines the
+//       group needs.
+//   [B] New slave rows are deramped once into a ring of RS_FR rows x RS_FW
+//       columns in shared memory: d (complex) and the FP32 residual
+//       G = phi - phi_ref of the deramp phase against a reference column.
+//   [C] Azimuth pass v(x) = sum_j kAz[j] d(L0-5+j, x) for every ring column,
+//       blocked over 4 rows x 2 columns per thread (15 ring loads and 24
+//       weight loads feed 96 packed FP32x2 FMAs).  G is exactly quadratic in
+//       azimuth time per column, so its azimuth interpolation is
+//       M0 G(L0) + g2 P1 + g1 P2 with the LUT row moments -- no taps.
+//   [D] Range pass, reramp, store.  A thread owns 2 adjacent output columns
+//       for 4 rows.  A column's range key (p0, bin) changes only every ~100
+//       rows, so its 12 range weights stay in registers; the 14 v samples of
+//       a column pair are 7 16-byte shared loads, and the phase residuals of
+//       2 rows are range-interpolated together with packed FMAs.
+// The interpolated phase is (1 + sp1) Psi_row + sum_i kRg[i] vg(x_i), where
+// Psi_row = sum_j kAz[j] phi_ref(y_j) is FP64 (reduced mod 2 pi) and
+// 1 + sp1 = sum kRg: equal to the reference's 144-tap FP64 phase sum in exact
+// arithmetic.  Rows or pixels outside these cases (several keys in a row,
+// edge and outside pixels, supports beyond the ring) take per-pixel paths
+// that compute the same formula.
+//
+// Precision modes: TOPS_PREC_SPLIT (default) forms G and the reduced phase of
+// each ring sample in FP32 from per-column coefficients about the burst's
+// centre time, with the FP64 reference-row phase reduced mod 2 pi once per
+// row (double-single).  TOPS_PREC_FP64 evaluates every sample's deramp phase
+// and its reduction in FP64.  Positions, LUT bins and Psi_row are FP64 in
+// both.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include <vector>
 
 #include "common.cuh"
+#include "launch.h"
 
 namespace tops {
 
@@ -49,46 +61,48 @@ constexpr int RS_NT = 256;   // threads per CTA
 constexpr int RS_TW = 112;   // output columns per strip
 constexpr int RS_GR = 16;    // output rows per group
 constexpr int RS_FR = 32;    // ring rows (power of two)
-constexpr int RS_FW = 128;   // ring columns (= threads per half CTA)
+constexpr int RS_FW = 128;   // ring columns
 constexpr int RS_SEG = 256;  // output rows per work item
-constexpr int RS_CPI = 8;    // output columns per range-pass item
 constexpr int RS_MAXJOBS = 32;
-constexpr int KEY_NONE = 0x7fffffff;
+constexpr int RS_DP = RS_TW / 2;   // column pairs of the range pass
+constexpr int RS_DT = RS_DP * 4;   // range-pass threads (4 row quarters of 4 rows)
+static_assert(RS_DT <= RS_NT, "range pass needs RS_DT threads");
+static_assert(RS_GR == 16 && RS_FW == 128 && RS_NT == 256 && RS_FR == 32,
+              "the thread mappings assume these sizes");
 
 enum : int { REG_OUT = 0, REG_EDGE = 1, REG_IN = 2 };
 
-struct RsLut {
-  const float *kaz, *krg;  // [2048][12]
-  const float4 *krg2;      // [2048][6]: range taps duplicated (w0,w0,w1,w1), ...
-  const float *sp1;        // [2048]: sum(krg row) - 1
-};
+using RsLut = LutPtrs;
 
 struct RsBatch {
   int njobs;
   int total_items;
+  int *counter;            // persistent launch: work-item queue (else null)
   ResampleJob jobs[RS_MAXJOBS];
 };
 
 struct __align__(16) RsShared {
-  float2 ring_d[RS_FR][RS_FW];
-  float ring_g[RS_FR][RS_FW];
-  float2 vd[RS_GR][pad8(RS_FW)];   // indexed with pad8(x)
-  float vg[RS_GR][pad8(RS_FW)];
-  float4 wpair[RS_GR][6];        // azimuth taps duplicated: (w0,w0,w1,w1), ...
-  double ring_phiref[RS_FR];
+  float2 ring_d[RS_FR][RS_FW];        // deramped slave rows
+  float ring_g[RS_FR][RS_FW];         // G = phi - phi_ref of each ring sample
+  float2 vd[RS_GR][RS_FW];            // azimuth-interpolated d
+  float2 vgp[RS_GR / 2][RS_FW];       // azimuth-interpolated G of rows (2k, 2k+1)
+  float4 wpair[RS_GR][6];             // azimuth taps duplicated: (w0,w0,w1,w1), ...
+  double ring_phiref[RS_FR];          // FP64 reference-column phase of the ring row
+  double ring_ta[RS_FR];              // burst-local azimuth time of the ring row
+  float ring_rho[RS_FR];              // ring_phiref reduced mod 2 pi
+  float ring_tc[RS_FR];               // ring_ta - tm (FP32, split mode)
   double rowA_az[RS_SEG], rowB_az[RS_SEG], rowA_rg[RS_SEG], rowB_rg[RS_SEG];
-  int kl0[RS_GR][pad8(RS_TW)];     // indexed with pad8(column)
-  int kp0[RS_GR][pad8(RS_TW)];
-  int kb[RS_GR][pad8(RS_TW)];      // binL | binP << 12 | region << 24
-  // per-row statistics of the group (interior pixels)
-  int st_kmin[RS_GR], st_kmax[RS_GR], st_pmin[RS_GR], st_pmax[RS_GR];
-  int row_flag[RS_GR];           // 1: shared azimuth pass
-  int row_L0[RS_GR], row_xlo[RS_GR], row_xhi[RS_GR];
+  double col_phat[RS_TW], col_qaz[RS_TW], col_qrg[RS_TW];
+  int row_v[RS_GR];                   // 1: shared azimuth pass valid for the row
+  int row_L0[RS_GR], row_bL[RS_GR];
   float row_M0[RS_GR], row_P1[RS_GR], row_P2[RS_GR];
   float row_rho[RS_GR], row_psif[RS_GR];
+  int g_lmin, g_lmax;                 // slave lines the group's interior pixels use
   double caz[6], crg[6], shift;
-  int xw;                        // absolute slave column of ring column 0
-  double ref_a0, ref_a1, ref_a2; // deramp quadratic of the reference column
+  int xw;                             // absolute slave column of ring column 0
+  double ref_a0, ref_a1, ref_a2;      // deramp quadratic of the reference column
+  double tm;                          // centre time of the split-mode coefficients
+  int next_item;                      // persistent launch: the item just taken
 };
 
 // Deramp + demodulation phase (DerampAndResample.cu:151-158), FP64, as the
@@ -117,6 +131,42 @@ __device__ __forceinline__ float2 cmul_conj_phase(float2 a, float phi) {
   float s, c;
   __sincosf(reduce_2pi_f(phi), &s, &c);
   return make_float2(a.x * c + a.y * s, a.y * c - a.x * s);
+}
+
+// Integer index and LUT bin of a position (GetIndexes, DerampAndResample.cu:
+// 108-112): trunc, then int(frac * 2047 + 0.5) without FMA contraction; the
+// bin is clamped as the reference's texture fetch clamps.
+__device__ __forceinline__ void split_pos(double v, int &i0, int &bin) {
+  i0 = __double2int_rz(v);
+  const int b = __double2int_rz(__dadd_rn(__dmul_rn(v - (double)i0, (double)kInterval), 0.5));
+  bin = min(max(b, 0), kLutBins - 1);
+}
+
+__device__ __forceinline__ int region_of(const ResampleJob &J, int l0, int p0) {
+  if (l0 > J.sy1 || l0 < J.sy0 || p0 > J.sx1 || p0 < J.sx0) return REG_OUT;
+  if (l0 > J.sy1 - 7 || l0 < J.sy0 + 5 || p0 > J.sx1 - 7 || p0 < J.sx0 + 5) return REG_EDGE;
+  return REG_IN;
+}
+
+// Range [lo, hi] of f(p) = fma(b, p, a + c p^2) -- the per-pixel form -- over
+// p in [p0, p1]: the ends and, when inside, the vertex.  Widened by 1e-9 so
+// that rounding of the per-pixel evaluation cannot leave it.
+__device__ __forceinline__ void quad_span(double a, double b, double c, double p0, double p1,
+                                          double &lo, double &hi) {
+  const double f0 = fma(b, p0, a + c * p0 * p0);
+  const double f1 = fma(b, p1, a + c * p1 * p1);
+  lo = fmin(f0, f1);
+  hi = fmax(f0, f1);
+  // the vertex lies inside only if the slope changes sign over [p0, p1]
+  const double s0 = fma(2.0 * c, p0, b), s1 = fma(2.0 * c, p1, b);
+  if ((s0 < 0.0) != (s1 < 0.0)) {
+    const double pv = -b / (2.0 * c);
+    const double fv = fma(b, pv, a + c * pv * pv);
+    lo = fmin(lo, fv);
+    hi = fmax(hi, fv);
+  }
+  lo -= 1e-9;
+  hi += 1e-9;
 }
 
 // ---------------------------------------------------- HBM slow path
@@ -186,23 +236,87 @@ __device__ float2 interior_from_ring(const RsShared &S, const RsLut &lut, int L0
   return cmul_conj_phase(make_float2(sre, sim), phi);
 }
 
-__device__ __forceinline__ int warp_min(int v) { return __reduce_min_sync(0xffffffffu, v); }
-__device__ __forceinline__ int warp_max(int v) { return __reduce_max_sync(0xffffffffu, v); }
+// Range weights of one output column, held in registers while its key holds.
+struct ColW {
+  float4 w[6];   // (w0,w0,w1,w1), (w2,w2,w3,w3), ...
+  float sp1;
+  int key;       // p0 << 12 | bin of the loaded weights (-1: none)
+};
 
-__global__ void __launch_bounds__(RS_NT, 2)
-    resample_kernel(const __grid_constant__ RsBatch B, RsLut lut) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  RsShared &S = *reinterpret_cast<RsShared *>(smem_raw);
+__device__ __forceinline__ void colw_load(ColW &cw, const RsLut &lut, int key) {
+  if (cw.key == key) return;
+  const int bp = key & 0xfff;
+  const float4 *kp4 = lut.krg2 + bp * (kTaps / 2);
+#pragma unroll
+  for (int q = 0; q < kTaps / 2; q++) cw.w[q] = __ldg(kp4 + q);
+  cw.sp1 = __ldg(lut.sp1 + bp);
+  cw.key = key;
+}
+
+__device__ __forceinline__ float2 wtap(const ColW &cw, int i) {
+  const float4 q = cw.w[i >> 1];
+  return (i & 1) ? make_float2(q.z, q.w) : make_float2(q.x, q.y);
+}
+
+// One interior pixel of a row with a shared azimuth pass: 12-tap range pass
+// over vd / vg of the row (single column).
+__device__ __forceinline__ float2 range_pixel(const RsShared &S, const ColW &cw, int r, int xb) {
+  float2 acc = make_float2(0.f, 0.f);
+  float sg = 0.f;
+  const float *vgrow = reinterpret_cast<const float *>(&S.vgp[r >> 1][0]) + (r & 1);
+#pragma unroll
+  for (int i = 0; i < kTaps; i++) {
+    const float2 w = wtap(cw, i);
+    acc = __ffma2_rn(w, S.vd[r][xb + i], acc);
+    sg = fmaf(w.x, vgrow[2 * (xb + i)], sg);
+  }
+  const float phi = S.row_rho[r] + cw.sp1 * S.row_psif[r] + sg;
+  return cmul_conj_phase(acc, phi);
+}
+
+// 12-tap range pass of two adjacent columns over the 14 samples V (the first
+// column's taps start at V[odd], the second's at V[odd + 1]).
+__device__ __forceinline__ void range_pair(const ColW &c0, const ColW &c1, const float2 (&V)[14],
+                                           bool odd, float2 &s0, float2 &s1) {
+  s0 = make_float2(0.f, 0.f);
+  s1 = s0;
+  if (odd) {
+#pragma unroll
+    for (int i = 0; i < kTaps; i++) {
+      s0 = __ffma2_rn(wtap(c0, i), V[i + 1], s0);
+      s1 = __ffma2_rn(wtap(c1, i), V[i + 2], s1);
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < kTaps; i++) {
+      s0 = __ffma2_rn(wtap(c0, i), V[i], s0);
+      s1 = __ffma2_rn(wtap(c1, i), V[i + 1], s1);
+    }
+  }
+}
+
+__device__ __forceinline__ void load14(const float2 *row, int base, float2 (&V)[14]) {
+  const float4 *p = reinterpret_cast<const float4 *>(row + base);
+#pragma unroll
+  for (int m = 0; m < 7; m++) {
+    const float4 t = p[m];
+    V[2 * m] = make_float2(t.x, t.y);
+    V[2 * m + 1] = make_float2(t.z, t.w);
+  }
+}
+
+// One work item (strip x segment of one job); all threads of the CTA call it
+// with the same item.
+template <bool kSplit>
+__device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int item) {
   const int tid = threadIdx.x;
-  const int ct = tid & (RS_FW - 1);  // column of this thread (key, ring, azimuth passes)
-  const int half = tid >> 7;         // 0 / 1
+  const int lane = tid & 31;
 
   // ---- locate the work item (job, strip, segment)
-  const int item = blockIdx.x;
-  if (item >= B.total_items) return;
   int jb = 0;
   while (jb + 1 < B.njobs && B.jobs[jb + 1].item_begin <= item) jb++;
   const ResampleJob &J = B.jobs[jb];
+  const RsLut &lut = J.lut;
   const int local = item - J.item_begin;
   const int strip = local % J.strips;
   const int seg = local / J.strips;
@@ -212,7 +326,7 @@ __global__ void __launch_bounds__(RS_NT, 2)
   const int r_begin = J.row0 + seg * J.seg_rows;
   const int r_end = min(r_begin + J.seg_rows, J.row0 + J.nrows);
 
-  // ---- per work item setup: polynomials, shift, statistics
+  // ---- per work item setup: polynomials, shift, per-row and per-column terms
   if (tid < 12) {
     const double v = J.cpm_dev ? J.cpm_dev[tid] : (tid < 6 ? J.caz[tid] : J.crg[tid - 6]);
     if (tid < 6)
@@ -230,15 +344,9 @@ __global__ void __launch_bounds__(RS_NT, 2)
     }
     S.shift = sh;
   }
-  if (tid < RS_GR) {
-    S.st_kmin[tid] = KEY_NONE;
-    S.st_kmax[tid] = -1;
-    S.st_pmin[tid] = KEY_NONE;
-    S.st_pmax[tid] = -KEY_NONE;
-  }
   __syncthreads();
-  // per-row polynomial terms: y = A(row) + B(row) P^ + c5 P^2
   {
+    // y = A(row) + B(row) P^ + c5 P^2 (the terms of my_polyval grouped by row)
     const int r = r_begin + tid;
     if (r < r_end) {
       const double L = ((double)(r + J.my0) - J.midL) * J.invL;
@@ -247,6 +355,12 @@ __global__ void __launch_bounds__(RS_NT, 2)
       S.rowB_az[tid] = a[2] + a[4] * L;
       S.rowA_rg[tid] = g[0] + g[1] * L + g[3] * L * L;
       S.rowB_rg[tid] = g[2] + g[4] * L;
+    }
+    if (tid < RS_TW) {
+      const double P = ((double)(c0 + min(tid, cN - 1)) - J.midP) * J.invP;
+      S.col_phat[tid] = P;
+      S.col_qaz[tid] = S.caz[5] * P * P;
+      S.col_qrg[tid] = S.crg[5] * P * P;
     }
   }
   if (tid == 0) {
@@ -264,159 +378,229 @@ __global__ void __launch_bounds__(RS_NT, 2)
         pmax = fmax(pmax, x);
       }
     }
-    int lo = (int)floor(pmin) - 5, hi = (int)floor(pmax) + 6;
-    int slack = RS_FW - (hi - lo + 1);
-    int xw = lo - (slack > 0 ? slack / 2 : 0);
+    // The range pass reads ring columns [p0 - 6, p0 + 8]: the window starts
+    // at the leftmost such column, one column lower when needed for an even
+    // offset from the box edge (8-byte pair loads).  A strip spanning up to
+    // RS_FW - 16 samples then fits; wider spans fall back per pixel.
+    const int lo = (int)floor(pmin) - 6;
+    const int xw = lo - ((lo - J.sx0) & 1);
     S.xw = xw;
     int xr = min(max(xw + RS_FW / 2, J.sx0), J.sx1);
     const DerampQuad q = deramp_quad(J.kt[xr], J.tref[xr], J.fdc[xr]);
     S.ref_a0 = q.a0;
     S.ref_a1 = q.a1;
     S.ref_a2 = q.a2;
+    S.tm = 0.5 * (double)(J.sy0 + J.sy1 - 2 * J.s_first_line) * J.dt;
   }
   __syncthreads();
 
-  // per-thread column constants
-  const bool kcol = ct < cN;                         // key column
-  const double phat = ((double)(c0 + min(ct, cN - 1)) - J.midP) * J.invP;
-  const double q_az = S.caz[5] * phat * phat, q_rg = S.crg[5] * phat * phat;
-  const int xabs = S.xw + ct;                        // ring column
-  const bool xin = (xabs >= J.sx0 && xabs <= J.sx1);
-  DerampQuad colq = {0.0, 0.0, 0.0};
-  if (xin) colq = deramp_quad(J.kt[xabs], J.tref[xabs], J.fdc[xabs]);
-  const float da2 = (float)(colq.a2 - S.ref_a2), da1 = (float)(colq.a1 - S.ref_a1);
+  // ---- per-thread constants of the ring / azimuth-pass column pair
+  const int xr0 = 2 * (tid & 63);            // ring columns xr0, xr0 + 1
+  const int xa0 = S.xw + xr0;                // absolute slave columns xa0, xa0 + 1
+  const bool xin0 = xa0 >= J.sx0 && xa0 <= J.sx1;
+  const bool xin1 = xa0 + 1 >= J.sx0 && xa0 + 1 <= J.sx1;
   const DerampQuad refq = {S.ref_a0, S.ref_a1, S.ref_a2};
+  const double tm = S.tm;
+  DerampQuad cq0 = refq, cq1 = refq;
+  if (xin0) cq0 = deramp_quad(J.kt[xa0], J.tref[xa0], J.fdc[xa0]);
+  if (xin1) cq1 = deramp_quad(J.kt[xa0 + 1], J.tref[xa0 + 1], J.fdc[xa0 + 1]);
+  // G = phi - phi_ref about tm: g2 tc^2 + g1 tc + g0 (tc = ta - tm)
+  float g2c0, g1c0, g0c0, g2c1, g1c1, g0c1;
+  {
+    const double d2 = cq0.a2 - refq.a2, d1 = cq0.a1 - refq.a1, d0 = cq0.a0 - refq.a0;
+    g2c0 = (float)d2;
+    g1c0 = (float)(2.0 * d2 * tm + d1);
+    g0c0 = (float)((d2 * tm + d1) * tm + d0);
+    const double e2 = cq1.a2 - refq.a2, e1 = cq1.a1 - refq.a1, e0 = cq1.a0 - refq.a0;
+    g2c1 = (float)e2;
+    g1c1 = (float)(2.0 * e2 * tm + e1);
+    g0c1 = (float)((e2 * tm + e1) * tm + e0);
+  }
+
+  // ---- per-thread constants of the range pass (2 columns x 4 rows)
+  const int dcp = tid % RS_DP, drq = tid / RS_DP;
+  const bool dthread = tid < RS_DT;
+  const int dc = 2 * dcp;                    // strip-local columns dc, dc + 1
+  const bool dval0 = dthread && dc < cN, dval1 = dthread && dc + 1 < cN;
+  ColW cw0, cw1;   // range weights of the two columns, kept across groups
+  cw0.key = -1;
+  cw1.key = -1;
+  const bool out16 = J.out_al16 != 0;
+
   int loaded_lo = INT32_MIN, loaded_hi = INT32_MIN;  // valid ring rows (uniform)
 
   for (int rg = r_begin; rg < r_end; rg += RS_GR) {
     const int gr = min(RS_GR, r_end - rg);
-    // ---- [A] indexes, bins and regions; per-row statistics
-#pragma unroll 2
-    for (int k = 0; k < RS_GR / 2; k++) {
-      const int r = half + 2 * k;
-      int key = KEY_NONE, kmx = -1, pmn = KEY_NONE, pmx = -KEY_NONE;
-      if (r < gr && kcol) {
-        const int ri = rg - r_begin + r;
-        const double y = fma(S.rowB_az[ri], phat, S.rowA_az[ri] + q_az);
-        const double x = fma(S.rowB_rg[ri], phat, S.rowA_rg[ri] + q_rg);
-        const int l0 = __double2int_rz(y);
-        int bl = __double2int_rz(__dadd_rn(__dmul_rn(y - (double)l0, (double)kInterval), 0.5));
-        const int p0 = __double2int_rz(x);
-        int bp = __double2int_rz(__dadd_rn(__dmul_rn(x - (double)p0, (double)kInterval), 0.5));
-        int reg;
-        if (l0 > J.sy1 || l0 < J.sy0 || p0 > J.sx1 || p0 < J.sx0)
-          reg = REG_OUT;
-        else if (l0 > J.sy1 - 7 || l0 < J.sy0 + 5 || p0 > J.sx1 - 7 || p0 < J.sx0 + 5)
-          reg = REG_EDGE;
-        else
-          reg = REG_IN;
-        bl = min(max(bl, 0), kLutBins - 1);  // the reference's texture clamps
-        bp = min(max(bp, 0), kLutBins - 1);
-        S.kl0[r][pad8(ct)] = l0;
-        S.kp0[r][pad8(ct)] = p0;
-        S.kb[r][pad8(ct)] = bl | (bp << 12) | (reg << 24);
-        if (reg == REG_IN) {
-          key = (l0 << 12) | bl;
-          kmx = key;
-          pmn = pmx = p0;
-        }
-      }
+    // ---- [A] row statistics (warp 0: one lane per row), ring-row table
+    if (tid < 32) {
+      const int r = lane;
+      int v = 0, lmin = INT32_MAX, lmax = INT32_MIN;
+      int L0 = 0, bL = 0;
       if (r < gr) {
-        key = warp_min(key);
-        kmx = warp_max(kmx);
-        pmn = warp_min(pmn);
-        pmx = warp_max(pmx);
-        if ((tid & 31) == 0 && key != KEY_NONE) {
-          atomicMin(&S.st_kmin[r], key);
-          atomicMax(&S.st_kmax[r], kmx);
-          atomicMin(&S.st_pmin[r], pmn);
-          atomicMax(&S.st_pmax[r], pmx);
+        const int ri = rg - r_begin + r;
+        const double p0 = S.col_phat[0], p1 = S.col_phat[cN - 1];
+        double ylo, yhi, xlo, xhi;
+        quad_span(S.rowA_az[ri], S.rowB_az[ri], S.caz[5], p0, p1, ylo, yhi);
+        quad_span(S.rowA_rg[ri], S.rowB_rg[ri], S.crg[5], p0, p1, xlo, xhi);
+        int l0lo, blo, l0hi, bhi, x0lo, xblo, x0hi, xbhi;
+        split_pos(ylo, l0lo, blo);
+        split_pos(yhi, l0hi, bhi);
+        split_pos(xlo, x0lo, xblo);
+        split_pos(xhi, x0hi, xbhi);
+        const bool az_any = !(l0hi < J.sy0 + 5 || l0lo > J.sy1 - 7);
+        const bool rg_any = !(x0hi < J.sx0 + 5 || x0lo > J.sx1 - 7);
+        if (az_any && rg_any) {
+          lmin = max(l0lo, J.sy0 + 5);
+          lmax = min(l0hi, J.sy1 - 7);
+        }
+        const bool uniform = (l0lo == l0hi) && (blo == bhi);
+        const bool az_in = l0lo >= J.sy0 + 5 && l0hi <= J.sy1 - 7;
+        // the range pass reads ring columns [p0 - 6, p0 + 8] of its pixels
+        const bool win = (x0lo - 6 - S.xw >= 0) && (x0hi + 8 - S.xw < RS_FW);
+        v = uniform && az_in && rg_any && win;
+        L0 = l0lo;
+        bL = blo;
+      }
+      const int gmin = __reduce_min_sync(0xffffffffu, lmin);
+      const int gmax = __reduce_max_sync(0xffffffffu, lmax);
+      const bool ring_ok = gmin <= gmax && (gmax - gmin + 12 <= RS_FR);
+      if (!ring_ok) v = 0;
+      if (r < RS_GR) {
+        S.row_v[r] = v;
+        S.row_L0[r] = L0;
+        S.row_bL[r] = bL;
+      }
+      if (lane == 0) {
+        S.g_lmin = ring_ok ? gmin : 1;
+        S.g_lmax = ring_ok ? gmax : 0;
+      }
+      // ring-row table of the rows this group loads (at most RS_FR rows)
+      if (ring_ok) {
+        const int need_lo = gmin - 5, need_hi = gmax + 6;
+        const bool cont = need_lo >= loaded_lo && need_lo <= loaded_hi + 1;
+        const int new_lo = cont ? loaded_hi + 1 : need_lo;
+        const int y = new_lo + lane;
+        if (y <= need_hi) {
+          const int slot = y & (RS_FR - 1);
+          const double ta = (double)(y - J.s_first_line) * J.dt;
+          const double phref = quad_eval(refq, ta);
+          S.ring_phiref[slot] = phref;
+          S.ring_ta[slot] = ta;
+          S.ring_rho[slot] = reduce_2pi(phref);
+          S.ring_tc[slot] = (float)(ta - tm);
         }
       }
     }
     __syncthreads();
 
-    // ---- [B] group extent, per-row setup, ring loads
-    int lmin = INT32_MAX, lmax = INT32_MIN;
-#pragma unroll
-    for (int r = 0; r < RS_GR; r++) {
-      const int km = S.st_kmin[r];
-      if (km != KEY_NONE) {
-        lmin = min(lmin, km >> 12);
-        lmax = max(lmax, S.st_kmax[r] >> 12);
+    // ---- [B] per-row azimuth setup (threads 0..127: 8 lanes per row) and
+    // ring loads of the new slave rows (2 columns per thread)
+    const int glmin = S.g_lmin, glmax = S.g_lmax;
+    const bool ring_ok = glmin <= glmax;
+    if (tid < 8 * RS_GR) {
+      // azimuth taps (w, w) pairs, their moments M0..M2 and the row phase
+      // Psi = sum_j kAz[j] phi_ref(L0 - 5 + j): lane j < 6 takes taps 2j, 2j+1
+      const int r = tid >> 3, j = tid & 7;
+      const bool rv = S.row_v[r] != 0;
+      float m0 = 0.f, m1 = 0.f, m2 = 0.f;
+      double psi = 0.0;
+      if (rv && j < kTaps / 2) {
+        const int L0 = S.row_L0[r];
+        const float *kl = lut.kaz + S.row_bL[r] * kTaps + 2 * j;
+        const float w0 = __ldg(kl), w1 = __ldg(kl + 1);
+        S.wpair[r][j] = make_float4(w0, w0, w1, w1);
+        const float u0 = (float)(2 * j - 5), u1 = (float)(2 * j - 4);
+        m0 = w0 + w1;
+        m1 = fmaf(w0, u0, w1 * u1);
+        m2 = fmaf(w0, u0 * u0, w1 * (u1 * u1));
+        psi = fma((double)w0, S.ring_phiref[(L0 - 5 + 2 * j) & (RS_FR - 1)],
+                  (double)w1 * S.ring_phiref[(L0 - 4 + 2 * j) & (RS_FR - 1)]);
       }
-    }
-    const bool ring_ok = (lmax >= lmin) && (lmax - lmin + 12 <= RS_FR);
-    if (tid < RS_GR) {
-      const int r = tid;
-      const int km = S.st_kmin[r];
-      int flag = 0;
-      if (r < gr && km != KEY_NONE) {
-        const int L0 = km >> 12, bL = km & 0xfff;
-        const int xlo = S.st_pmin[r] - 5 - S.xw, xhi = S.st_pmax[r] + 6 - S.xw;
-        flag = ring_ok && (km == S.st_kmax[r]) && xlo >= 0 && xhi < RS_FW;
-        S.row_L0[r] = L0;
-        S.row_xlo[r] = xlo;
-        S.row_xhi[r] = xhi;
-        if (flag) {
-          const float *kl = lut.kaz + bL * kTaps;
-          float m0 = 0.f, m1 = 0.f, m2 = 0.f;
 #pragma unroll
-          for (int j = 0; j < kTaps; j += 2) {
-            const float w0 = __ldg(kl + j), w1 = __ldg(kl + j + 1);
-            S.wpair[r][j / 2] = make_float4(w0, w0, w1, w1);
-            const float u0 = (float)(j - 5), u1 = (float)(j - 4);
-            m0 += w0 + w1;
-            m1 = fmaf(w0, u0, fmaf(w1, u1, m1));
-            m2 = fmaf(w0, u0 * u0, fmaf(w1, u1 * u1, m2));
-          }
-          const double ta_c = (double)(L0 - J.s_first_line) * J.dt;
-          S.row_M0[r] = m0;
-          S.row_P1[r] = (float)(2.0 * ta_c * J.dt * m1 + J.dt * J.dt * m2);
-          S.row_P2[r] = (float)(J.dt * m1);
-        }
+      for (int o = 4; o > 0; o >>= 1) {
+        m0 += __shfl_xor_sync(0xffffffffu, m0, o);
+        m1 += __shfl_xor_sync(0xffffffffu, m1, o);
+        m2 += __shfl_xor_sync(0xffffffffu, m2, o);
+        psi += __shfl_xor_sync(0xffffffffu, psi, o);
       }
-      S.row_flag[r] = flag;
+      if (rv && j == 0) {
+        const double tc = (double)(S.row_L0[r] - J.s_first_line) * J.dt - tm;
+        S.row_M0[r] = m0;
+        S.row_P1[r] = (float)(2.0 * tc * J.dt * m1 + J.dt * J.dt * m2);
+        S.row_P2[r] = (float)(J.dt * m1);
+        S.row_rho[r] = reduce_2pi(psi);
+        S.row_psif[r] = (float)psi;
+      }
     }
     if (ring_ok) {
-      const int need_lo = lmin - 5, need_hi = lmax + 6;
-      // rows [need_lo, loaded_hi] are already in the ring when the ring holds
-      // them contiguously; otherwise (a jump) the whole range is reloaded
+      const int need_lo = glmin - 5, need_hi = glmax + 6;
       const bool cont = need_lo >= loaded_lo && need_lo <= loaded_hi + 1;
       const int new_lo = cont ? loaded_hi + 1 : need_lo;
-      // loads of up to RS_LB rows are issued before any of the math, so the
-      // HBM latency of a group's new rows is paid once
-      constexpr int RS_LB = 8;
-      for (int y0 = new_lo + half; y0 <= need_hi; y0 += 2 * RS_LB) {
-        short2 sv[RS_LB];
+      const int rp = tid >> 6;   // row phase: rows new_lo + rp + 4u
+      constexpr int RS_LB = RS_FR / 4;
+      // a group usually brings RS_GR new rows (RS_GR / 4 per thread)
+      const int nu = (need_hi - new_lo - rp + 4) / 4;   // rows of this thread
+      short2 sv0[RS_LB], sv1[RS_LB];
 #pragma unroll
-        for (int u = 0; u < RS_LB; u++) {
-          const int y = y0 + 2 * u;
-          sv[u] = make_short2(0, 0);
-          if (y <= need_hi && xin && y >= J.sy0 && y <= J.sy1)
-            sv[u] = J.slave[(long)(y - J.sy0) * J.slave_pitch + (xabs - J.sx0)];
-        }
-#pragma unroll
-        for (int u = 0; u < RS_LB; u++) {
-          const int y = y0 + 2 * u;
-          if (y > need_hi) break;
-          const int slot = y & (RS_FR - 1);
-          const double ta = (double)(y - J.s_first_line) * J.dt;
-          const double phref = quad_eval(refq, ta);
-          float2 d = make_float2(0.f, 0.f);
-          float g = 0.f;
-          if (xin && y >= J.sy0 && y <= J.sy1) {
-            const double phi = quad_eval(colq, ta);
-            g = (float)(phi - phref);
-            float sn, cs;
-            __sincosf(reduce_2pi(phi), &sn, &cs);
-            d.x = (float)sv[u].x * cs - (float)sv[u].y * sn;
-            d.y = (float)sv[u].x * sn + (float)sv[u].y * cs;
+      for (int u = 0; u < RS_LB; u++) {
+        sv0[u] = make_short2(0, 0);
+        sv1[u] = make_short2(0, 0);
+        const int y = new_lo + rp + 4 * u;
+        if ((u < RS_GR / 4 || u < nu) && y <= need_hi && y >= J.sy0 && y <= J.sy1) {
+          const short2 *row = J.slave + (long)(y - J.sy0) * J.slave_pitch;
+          const int xo = xa0 - J.sx0;
+          if (xin0 && xin1 && J.slave_al8) {
+            const int2 p = *reinterpret_cast<const int2 *>(row + xo);
+            sv0[u] = *reinterpret_cast<const short2 *>(&p.x);
+            sv1[u] = *reinterpret_cast<const short2 *>(&p.y);
+          } else {
+            if (xin0) sv0[u] = row[xo];
+            if (xin1) sv1[u] = row[xo + 1];
           }
-          S.ring_d[slot][ct] = d;
-          S.ring_g[slot][ct] = g;
-          if (ct == 0) S.ring_phiref[slot] = phref;
         }
+        if (u + 1 >= RS_GR / 4 && u + 1 >= nu) break;
+      }
+#pragma unroll
+      for (int u = 0; u < RS_LB; u++) {
+        const int y = new_lo + rp + 4 * u;
+        if (y > need_hi) break;
+        const int slot = y & (RS_FR - 1);
+        float2 d0 = make_float2(0.f, 0.f), d1 = d0;
+        float G0 = 0.f, G1 = 0.f;
+        if (y >= J.sy0 && y <= J.sy1) {
+          float r0, r1;
+          if (kSplit) {
+            const float tc = S.ring_tc[slot], rho = S.ring_rho[slot];
+            G0 = fmaf(fmaf(g2c0, tc, g1c0), tc, g0c0);
+            G1 = fmaf(fmaf(g2c1, tc, g1c1), tc, g0c1);
+            r0 = reduce_2pi_f(rho + G0);
+            r1 = reduce_2pi_f(rho + G1);
+          } else {
+            const double ta = S.ring_ta[slot], phref = S.ring_phiref[slot];
+            const double p0 = quad_eval(cq0, ta), p1 = quad_eval(cq1, ta);
+            G0 = (float)(p0 - phref);
+            G1 = (float)(p1 - phref);
+            r0 = reduce_2pi(p0);
+            r1 = reduce_2pi(p1);
+          }
+          float sn, cs;
+          if (xin0) {
+            __sincosf(r0, &sn, &cs);
+            d0.x = (float)sv0[u].x * cs - (float)sv0[u].y * sn;
+            d0.y = (float)sv0[u].x * sn + (float)sv0[u].y * cs;
+          } else {
+            G0 = 0.f;
+          }
+          if (xin1) {
+            __sincosf(r1, &sn, &cs);
+            d1.x = (float)sv1[u].x * cs - (float)sv1[u].y * sn;
+            d1.y = (float)sv1[u].x * sn + (float)sv1[u].y * cs;
+          } else {
+            G1 = 0.f;
+          }
+        }
+        *reinterpret_cast<float4 *>(&S.ring_d[slot][xr0]) = make_float4(d0.x, d0.y, d1.x, d1.y);
+        *reinterpret_cast<float2 *>(&S.ring_g[slot][xr0]) = make_float2(G0, G1);
       }
       if (!cont) loaded_lo = need_lo;
       loaded_hi = max(loaded_hi, need_hi);
@@ -424,181 +608,238 @@ __global__ void __launch_bounds__(RS_NT, 2)
     }
     __syncthreads();
 
-    // ---- [C] shared azimuth pass v(x) and the row phases
-    if (tid < RS_GR && S.row_flag[tid]) {
-      const int r = tid;
-      const int bL = S.st_kmin[r] & 0xfff, L0 = S.row_L0[r];
-      const float *kl = lut.kaz + bL * kTaps;
-      double psi = 0.0;
-#pragma unroll
-      for (int j = 0; j < kTaps; j++)
-        psi = fma((double)__ldg(kl + j), S.ring_phiref[(L0 - 5 + j) & (RS_FR - 1)], psi);
-      S.row_rho[r] = reduce_2pi(psi);
-      S.row_psif[r] = (float)psi;
-    }
+    // ---- [C] shared azimuth pass: 2 ring columns x 4 rows per thread
     {
-      const int x = ct;
-#pragma unroll 1
-      for (int qq = 0; qq < 2; qq++) {
-        const int q = half + 2 * qq;  // quad of rows 4q..4q+3
-        const int r0 = 4 * q;
-        if (r0 >= gr) continue;
-        bool blk = r0 + 4 <= gr;
-        int xl = INT32_MAX, xh = INT32_MIN;
+      const int q = tid >> 6;      // rows 4q .. 4q+3
+      const int r0 = 4 * q;
+      if (r0 < gr) {
         const int L00 = S.row_L0[r0];
+        bool blk = r0 + 4 <= gr;
 #pragma unroll
         for (int k = 0; k < 4; k++) {
           const int r = min(r0 + k, RS_GR - 1);
-          blk = blk && S.row_flag[r] && S.row_L0[r] == L00 + k;
-          xl = min(xl, S.row_xlo[r]);
-          xh = max(xh, S.row_xhi[r]);
+          blk = blk && S.row_v[r] && S.row_L0[r] == L00 + k;
         }
         if (blk) {
-          if (x < xl || x > xh) continue;
-          float2 acc[4];
+          float2 a0[4], a1[4];
 #pragma unroll
-          for (int k = 0; k < 4; k++) acc[k] = make_float2(0.f, 0.f);
-          const int ybase = L00 - 5;
+          for (int k = 0; k < 4; k++) a0[k] = a1[k] = make_float2(0.f, 0.f);
 #pragma unroll
           for (int jj = 0; jj < kTaps + 3; jj++) {
-            const float2 d = S.ring_d[(ybase + jj) & (RS_FR - 1)][x];
+            const float4 dd =
+                *reinterpret_cast<const float4 *>(&S.ring_d[(L00 - 5 + jj) & (RS_FR - 1)][xr0]);
+            const float2 e0 = make_float2(dd.x, dd.y), e1 = make_float2(dd.z, dd.w);
 #pragma unroll
             for (int k = 0; k < 4; k++) {
               const int j = jj - k;
               if (j >= 0 && j < kTaps) {
                 const float4 wp = S.wpair[r0 + k][j >> 1];
                 const float2 w = (j & 1) ? make_float2(wp.z, wp.w) : make_float2(wp.x, wp.y);
-                acc[k] = __ffma2_rn(w, d, acc[k]);
+                a0[k] = __ffma2_rn(w, e0, a0[k]);
+                a1[k] = __ffma2_rn(w, e1, a1[k]);
               }
             }
           }
+          float vg0[4], vg1[4];
 #pragma unroll
           for (int k = 0; k < 4; k++) {
             const int r = r0 + k;
-            const float gc = S.ring_g[(L00 + k) & (RS_FR - 1)][x];
-            S.vd[r][pad8(x)] = acc[k];
-            S.vg[r][pad8(x)] = fmaf(S.row_M0[r], gc, fmaf(da2, S.row_P1[r], da1 * S.row_P2[r]));
+            const float2 gc =
+                *reinterpret_cast<const float2 *>(&S.ring_g[(L00 + k) & (RS_FR - 1)][xr0]);
+            const float M0 = S.row_M0[r], P1 = S.row_P1[r], P2 = S.row_P2[r];
+            vg0[k] = fmaf(M0, gc.x, fmaf(g2c0, P1, g1c0 * P2));
+            vg1[k] = fmaf(M0, gc.y, fmaf(g2c1, P1, g1c1 * P2));
+            *reinterpret_cast<float4 *>(&S.vd[r][xr0]) =
+                make_float4(a0[k].x, a0[k].y, a1[k].x, a1[k].y);
           }
+          *reinterpret_cast<float4 *>(&S.vgp[2 * q][xr0]) =
+              make_float4(vg0[0], vg0[1], vg1[0], vg1[1]);
+          *reinterpret_cast<float4 *>(&S.vgp[2 * q + 1][xr0]) =
+              make_float4(vg0[2], vg0[3], vg1[2], vg1[3]);
         } else {
 #pragma unroll 1
           for (int k = 0; k < 4 && r0 + k < gr; k++) {
             const int r = r0 + k;
-            if (!S.row_flag[r] || x < S.row_xlo[r] || x > S.row_xhi[r]) continue;
+            if (!S.row_v[r]) continue;
             const int L0 = S.row_L0[r];
-            float2 acc = make_float2(0.f, 0.f);
+            float2 a0 = make_float2(0.f, 0.f), a1 = a0;
 #pragma unroll
             for (int j = 0; j < kTaps; j++) {
               const float4 wp = S.wpair[r][j >> 1];
               const float2 w = (j & 1) ? make_float2(wp.z, wp.w) : make_float2(wp.x, wp.y);
-              acc = __ffma2_rn(w, S.ring_d[(L0 - 5 + j) & (RS_FR - 1)][x], acc);
+              const float4 dd =
+                  *reinterpret_cast<const float4 *>(&S.ring_d[(L0 - 5 + j) & (RS_FR - 1)][xr0]);
+              a0 = __ffma2_rn(w, make_float2(dd.x, dd.y), a0);
+              a1 = __ffma2_rn(w, make_float2(dd.z, dd.w), a1);
             }
-            const float gc = S.ring_g[L0 & (RS_FR - 1)][x];
-            S.vd[r][pad8(x)] = acc;
-            S.vg[r][pad8(x)] = fmaf(S.row_M0[r], gc, fmaf(da2, S.row_P1[r], da1 * S.row_P2[r]));
+            const float2 gc =
+                *reinterpret_cast<const float2 *>(&S.ring_g[L0 & (RS_FR - 1)][xr0]);
+            const float M0 = S.row_M0[r], P1 = S.row_P1[r], P2 = S.row_P2[r];
+            float *vg = reinterpret_cast<float *>(&S.vgp[r >> 1][xr0]) + (r & 1);
+            vg[0] = fmaf(M0, gc.x, fmaf(g2c0, P1, g1c0 * P2));
+            vg[2] = fmaf(M0, gc.y, fmaf(g2c1, P1, g1c1 * P2));
+            *reinterpret_cast<float4 *>(&S.vd[r][xr0]) = make_float4(a0.x, a0.y, a1.x, a1.y);
           }
         }
       }
     }
     __syncthreads();
 
-    // ---- [D] range pass, reramp, store: RS_CPI consecutive columns per item
-    constexpr int NG = RS_TW / RS_CPI;
-    for (int it = tid; it < gr * NG; it += RS_NT) {
-      const int r = it / NG;
-      const int cg = (it - r * NG) * RS_CPI;
-      if (cg >= cN) continue;
-      const int mr = rg + r;
-      float2 *orow = J.out + (long)(mr - J.row0) * J.out_pitch + c0 + cg;
-      int kbv[RS_CPI], p0v[RS_CPI];
-#pragma unroll
-      for (int k = 0; k < RS_CPI; k++) {
-        const int c = pad8(min(cg + k, cN - 1));
-        kbv[k] = S.kb[r][c];
-        p0v[k] = S.kp0[r][c];
-      }
-      const bool uni = S.row_flag[r];
-      bool fast = uni && (cg + RS_CPI <= cN) && ((reinterpret_cast<uintptr_t>(orow) & 15) == 0);
-#pragma unroll
-      for (int k = 0; k < RS_CPI; k++)
-        fast = fast && ((kbv[k] >> 24) == REG_IN) && (p0v[k] == p0v[0] + k);
-      if (fast) {
-        // 19 shared v loads serve 8 pixels x 12 taps; 16-byte stores
-        const int xb = p0v[0] - 5 - S.xw;
-        float2 vd[kTaps + RS_CPI - 1];
-        float vg[kTaps + RS_CPI - 1];
-#pragma unroll
-        for (int i = 0; i < kTaps + RS_CPI - 1; i++) {
-          vd[i] = S.vd[r][pad8(xb + i)];
-          vg[i] = S.vg[r][pad8(xb + i)];
-        }
-        const float rho = S.row_rho[r], psif = S.row_psif[r];
-        float4 *o4 = reinterpret_cast<float4 *>(orow);
-#pragma unroll
-        for (int k = 0; k < RS_CPI; k += 2) {
-          float2 res[2];
-#pragma unroll
-          for (int u = 0; u < 2; u++) {
-            const int bp = (kbv[k + u] >> 12) & 0xfff;
-            const float4 *kp4 = lut.krg2 + bp * (kTaps / 2);
-            float2 acc = make_float2(0.f, 0.f);
-            float sg = 0.f;
-#pragma unroll
-            for (int q = 0; q < kTaps / 2; q++) {
-              const float4 w = __ldg(kp4 + q);
-              acc = __ffma2_rn(make_float2(w.x, w.y), vd[k + u + 2 * q], acc);
-              acc = __ffma2_rn(make_float2(w.z, w.w), vd[k + u + 2 * q + 1], acc);
-              sg = fmaf(w.x, vg[k + u + 2 * q], sg);
-              sg = fmaf(w.z, vg[k + u + 2 * q + 1], sg);
-            }
-            const float phi = rho + __ldg(lut.sp1 + bp) * psif + sg;
-            res[u] = cmul_conj_phase(acc, phi);
-          }
-          o4[k / 2] = make_float4(res[0].x, res[0].y, res[1].x, res[1].y);
-        }
-      } else {
+    // ---- [D] range pass, reramp, store: 2 columns x 4 rows per thread
+    if (dthread) {
 #pragma unroll 1
-        for (int k = 0; k < RS_CPI && cg + k < cN; k++) {
-          const int c = pad8(cg + k);
-          const int kb = S.kb[r][c], reg = kb >> 24;
-          const int l0 = S.kl0[r][c], p0 = S.kp0[r][c];
-          float2 res = make_float2(0.f, 0.f);
-          if (reg == REG_EDGE) {
-            const short2 sv = J.slave[(long)(l0 - J.sy0) * J.slave_pitch + (p0 - J.sx0)];
-            res = make_float2((float)sv.x, (float)sv.y);
-          } else if (reg == REG_IN) {
-            const int bl = kb & 0xfff, bp = (kb >> 12) & 0xfff;
-            const int xb = p0 - 5 - S.xw;
-            const bool in_win = xb >= 0 && xb + kTaps <= RS_FW;
-            if (uni && in_win) {
-              const float4 *kp4 = lut.krg2 + bp * (kTaps / 2);
-              float2 acc = make_float2(0.f, 0.f);
-              float sg = 0.f;
+      for (int h = 0; h < 2; h++) {
+        const int ra = 4 * drq + 2 * h;     // rows ra, ra + 1 (ra even)
+        if (ra >= gr) break;
+        const bool two = ra + 1 < gr;
+        // range keys of the 2 x 2 pixels
+        int p0v[2][2], bpv[2][2];
 #pragma unroll
-              for (int q = 0; q < kTaps / 2; q++) {
-                const float4 w = __ldg(kp4 + q);
-                acc = __ffma2_rn(make_float2(w.x, w.y), S.vd[r][pad8(xb + 2 * q)], acc);
-                acc = __ffma2_rn(make_float2(w.z, w.w), S.vd[r][pad8(xb + 2 * q + 1)], acc);
-                sg = fmaf(w.x, S.vg[r][pad8(xb + 2 * q)], sg);
-                sg = fmaf(w.z, S.vg[r][pad8(xb + 2 * q + 1)], sg);
+        for (int k = 0; k < 2; k++) {
+          const int ri = rg - r_begin + ra + k;
+          const double A = S.rowA_rg[ri], Bc = S.rowB_rg[ri];
+#pragma unroll
+          for (int c = 0; c < 2; c++) {
+            const int col = min(dc + c, cN - 1);
+            const double x = fma(Bc, S.col_phat[col], A + S.col_qrg[col]);
+            split_pos(x, p0v[k][c], bpv[k][c]);
+          }
+        }
+        // Fast pair: both rows with a shared azimuth pass, each row's two
+        // pixels interior, adjacent (p0 steps by one) and inside the ring
+        // window.  A column's range key may change between the two rows
+        // (about once per 100 rows); its weights are then reloaded for the
+        // second row and its phase residual is interpolated per row.
+        bool fast = two && dval1 && out16 && S.row_v[ra] && S.row_v[ra + 1];
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+          const int xbk = p0v[k][0] - 5 - S.xw;
+          fast = fast && p0v[k][1] == p0v[k][0] + 1 && p0v[k][0] >= J.sx0 + 5 &&
+                 p0v[k][1] <= J.sx1 - 7 && xbk >= 1 && xbk + 13 < RS_FW;
+        }
+        if (fast) {
+          const int key00 = (p0v[0][0] << 12) | bpv[0][0], key01 = (p0v[0][1] << 12) | bpv[0][1];
+          const int key10 = (p0v[1][0] << 12) | bpv[1][0], key11 = (p0v[1][1] << 12) | bpv[1][1];
+          const bool same = key00 == key10 && key01 == key11;
+          float2 acc[2][2];
+          float sg[2][2];
+#pragma unroll
+          for (int k = 0; k < 2; k++) {
+            colw_load(cw0, lut, k ? key10 : key00);
+            colw_load(cw1, lut, k ? key11 : key01);
+            const int xb = p0v[k][0] - 5 - S.xw;   // ring column of the first tap
+            const int base = xb & ~1;              // 16-byte aligned start
+            const bool odd = (xb & 1) != 0;
+            {
+              float2 V[14];
+              load14(&S.vd[ra + k][0], base, V);
+              range_pair(cw0, cw1, V, odd, acc[k][0], acc[k][1]);
+            }
+            // phase residuals from the (row ra, row ra+1) pairs: both rows
+            // at once when the keys agree, else each row with its weights
+            if (k == 0 || !same) {
+              float2 Gp[14], g0, g1;
+              load14(&S.vgp[ra >> 1][0], base, Gp);
+              range_pair(cw0, cw1, Gp, odd, g0, g1);
+              if (k == 0) {
+                sg[0][0] = g0.x;
+                sg[0][1] = g1.x;
+                sg[1][0] = g0.y;
+                sg[1][1] = g1.y;
+              } else {
+                sg[1][0] = g0.y;
+                sg[1][1] = g1.y;
               }
-              const float phi = S.row_rho[r] + __ldg(lut.sp1 + bp) * S.row_psif[r] + sg;
-              res = cmul_conj_phase(acc, phi);
-            } else if (ring_ok && in_win) {
-              res = interior_from_ring(S, lut, l0, bl, p0, bp);
-            } else {
-              res = interior_from_global(J, lut, l0, bl, p0, bp);
             }
           }
-          orow[k] = res;
+#pragma unroll
+          for (int k = 0; k < 2; k++) {
+            const int r = ra + k;
+            const float rho = S.row_rho[r], psif = S.row_psif[r];
+            // sp1 of the column's row-k bin (cw holds row 1's weights now)
+            const float sp0 = (k == 0 && !same) ? __ldg(lut.sp1 + bpv[0][0]) : cw0.sp1;
+            const float sp1 = (k == 0 && !same) ? __ldg(lut.sp1 + bpv[0][1]) : cw1.sp1;
+            const float2 o0 = cmul_conj_phase(acc[k][0], rho + sp0 * psif + sg[k][0]);
+            const float2 o1 = cmul_conj_phase(acc[k][1], rho + sp1 * psif + sg[k][1]);
+            float2 *orow = J.out + (long)(rg + r - J.row0) * J.out_pitch + c0 + dc;
+            *reinterpret_cast<float4 *>(orow) = make_float4(o0.x, o0.y, o1.x, o1.y);
+          }
+        } else {
+          // per pixel: any region, any key
+#pragma unroll 1
+          for (int k = 0; k < 2; k++) {
+            const int r = ra + k;
+            if (r >= gr) break;
+            const int ri = rg - r_begin + r;
+            const bool rv = S.row_v[r];
+#pragma unroll 1
+            for (int c = 0; c < 2; c++) {
+              if (!(c ? dval1 : dval0)) continue;
+              const int col = dc + c;
+              int l0, bl;
+              if (rv) {
+                l0 = S.row_L0[r];
+                bl = S.row_bL[r];
+              } else {
+                const double y =
+                    fma(S.rowB_az[ri], S.col_phat[col], S.rowA_az[ri] + S.col_qaz[col]);
+                split_pos(y, l0, bl);
+              }
+              // (selects, not a dynamic index: keeps p0v / bpv in registers)
+              const int p0 = k ? (c ? p0v[1][1] : p0v[1][0]) : (c ? p0v[0][1] : p0v[0][0]);
+              const int bp = k ? (c ? bpv[1][1] : bpv[1][0]) : (c ? bpv[0][1] : bpv[0][0]);
+              const int reg = region_of(J, l0, p0);
+              float2 res = make_float2(0.f, 0.f);
+              if (reg == REG_EDGE) {
+                const short2 sv = J.slave[(long)(l0 - J.sy0) * J.slave_pitch + (p0 - J.sx0)];
+                res = make_float2((float)sv.x, (float)sv.y);
+              } else if (reg == REG_IN) {
+                const int xbp = p0 - 5 - S.xw;
+                const bool in_win = xbp >= 0 && xbp + kTaps <= RS_FW;
+                if (rv && in_win) {
+                  if (c) {
+                    colw_load(cw1, lut, (p0 << 12) | bp);
+                    res = range_pixel(S, cw1, r, xbp);
+                  } else {
+                    colw_load(cw0, lut, (p0 << 12) | bp);
+                    res = range_pixel(S, cw0, r, xbp);
+                  }
+                } else if (ring_ok && in_win && l0 - 5 >= loaded_lo && l0 + 6 <= loaded_hi) {
+                  res = interior_from_ring(S, lut, l0, bl, p0, bp);
+                } else {
+                  res = interior_from_global(J, lut, l0, bl, p0, bp);
+                }
+              }
+              J.out[(long)(rg + r - J.row0) * J.out_pitch + c0 + col] = res;
+            }
+          }
         }
       }
     }
-    if (tid < RS_GR) {
-      S.st_kmin[tid] = KEY_NONE;
-      S.st_kmax[tid] = -1;
-      S.st_pmin[tid] = KEY_NONE;
-      S.st_pmax[tid] = -KEY_NONE;
-    }
+    __syncthreads();
+  }
+}
+
+template <bool kSplit>
+__global__ void __launch_bounds__(RS_NT, 2)
+    resample_kernel(const __grid_constant__ RsBatch B) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  RsShared &S = *reinterpret_cast<RsShared *>(smem_raw);
+  // one work item per CTA, or (persistent) items from the queue until it
+  // is empty; a single call site keeps one inlined copy of the item code
+  int item = blockIdx.x;
+  if (B.counter) {
+    if (threadIdx.x == 0) S.next_item = atomicAdd(B.counter, 1);
+    __syncthreads();
+    item = S.next_item;
+    __syncthreads();
+  }
+  while (item < B.total_items) {
+    resample_item<kSplit>(S, B, item);
+    if (!B.counter) break;
+    if (threadIdx.x == 0) S.next_item = atomicAdd(B.counter, 1);
+    __syncthreads();
+    item = S.next_item;
     __syncthreads();
   }
 }
@@ -678,6 +919,10 @@ int fill_resample_job(const tops_resample_job &u, ResampleJob &J) {
   J.out_pitch = (long)(u.out_pitch / sizeof(float2));
   if (J.slave_pitch < u.sbox[1] - u.sbox[0] + 1 || J.out_pitch < u.mbox[1] - u.mbox[0] + 1)
     return TOPS_E_INVALID;
+  // vector access needs aligned bases and pitches: 8-byte slave pairs and
+  // 16-byte output pairs (scalar access otherwise)
+  J.slave_al8 = ((reinterpret_cast<uintptr_t>(u.slave) & 7) == 0) && (u.slave_pitch % 8 == 0);
+  J.out_al16 = ((reinterpret_cast<uintptr_t>(u.out) & 15) == 0) && (u.out_pitch % 16 == 0);
   J.kt = u.kt;
   J.tref = u.tref;
   J.fdc = u.fdc;
@@ -713,42 +958,95 @@ int fill_resample_job(const tops_resample_job &u, ResampleJob &J) {
   return TOPS_OK;
 }
 
-int launch_resample(const LutDev &L, const ResampleJob *jobs, int njobs, cudaStream_t st) {
-  static bool attr_done = false;
-  if (!attr_done) {
-    TOPS_CUDA_TRY(cudaFuncSetAttribute(resample_kernel,
+template <bool kSplit>
+static int launch_resample_t(const ResampleJob *jobs, int njobs, const TileCfg &cfg,
+                             cudaStream_t st) {
+  // the shared-memory opt-in is a per-device function attribute; the
+  // persistent grid is the number of CTAs resident at once
+  static bool attr_done[kMaxDevices] = {};
+  static int resident[kMaxDevices] = {};
+  int dev = 0;
+  TOPS_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return TOPS_E_INVALID;
+  if (!attr_done[dev]) {
+    TOPS_CUDA_TRY(cudaFuncSetAttribute(resample_kernel<kSplit>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)sizeof(RsShared)));
-    attr_done = true;
+    int per_sm = 0, sms = 0;
+    TOPS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, resample_kernel<kSplit>, RS_NT, sizeof(RsShared)));
+    TOPS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    resident[dev] = per_sm * sms;
+    attr_done[dev] = true;
   }
-  RsLut lut{L.kaz, L.krg, L.krg2, L.sp1};
-  for (int j0 = 0; j0 < njobs; j0 += RS_MAXJOBS) {
+  if (cfg.seg_rows < 0 || cfg.seg_rows > RS_SEG || (cfg.seg_rows && cfg.seg_rows < RS_GR))
+    return TOPS_E_INVALID;
+  for (int j0 = 0, k = 0; j0 < njobs; j0 += RS_MAXJOBS, k++) {
     RsBatch B;
     B.njobs = 0;
+    B.counter = cfg.counters ? cfg.counters + k : nullptr;
     int items = 0;
     for (int j = j0; j < njobs && j < j0 + RS_MAXJOBS; j++) {
-      B.jobs[B.njobs] = jobs[j];
-      B.jobs[B.njobs].item_begin = items;
-      items += jobs[j].strips * jobs[j].segs;
+      ResampleJob &J = B.jobs[B.njobs];
+      J = jobs[j];
+      if (cfg.seg_rows) {
+        J.seg_rows = cfg.seg_rows;
+        J.segs = (J.nrows + cfg.seg_rows - 1) / cfg.seg_rows;
+      }
+      J.item_begin = items;
+      items += J.strips * J.segs;
       B.njobs++;
     }
     B.total_items = items;
     if (items == 0) continue;
-    resample_kernel<<<items, RS_NT, sizeof(RsShared), st>>>(B, lut);
+    int grid = items;
+    if (B.counter) {
+      TOPS_CUDA_TRY(cudaMemsetAsync(B.counter, 0, sizeof(int), st));
+      grid = min(items, cfg.grid > 0 ? cfg.grid : resident[dev]);
+    }
+    resample_kernel<kSplit><<<grid, RS_NT, sizeof(RsShared), st>>>(B);
     TOPS_CUDA_TRY(cudaGetLastError());
   }
   return TOPS_OK;
 }
 
+int launch_resample(const ResampleJob *jobs, int njobs, int precision, const TileCfg &cfg,
+                    cudaStream_t st) {
+  if (precision == TOPS_PREC_FP64) return launch_resample_t<false>(jobs, njobs, cfg, st);
+  if (precision == TOPS_PREC_SPLIT) return launch_resample_t<true>(jobs, njobs, cfg, st);
+  return TOPS_E_INVALID;
+}
+
+int resample_launch_multi(const tops_lut_dev *const *luts, const tops_resample_job *jobs,
+                          int njobs, int precision, const TileCfg &cfg, cudaStream_t st) {
+  if (!luts || (!jobs && njobs > 0) || njobs < 0) return TOPS_E_INVALID;
+  std::vector<ResampleJob> J(njobs);
+  for (int j = 0; j < njobs; j++) {
+    if (!luts[j]) return TOPS_E_INVALID;
+    int s = fill_resample_job(jobs[j], J[j]);
+    if (s != TOPS_OK) return s;
+    const LutDev &L = luts[j]->d;
+    J[j].lut = LutPtrs{L.kaz, L.krg, L.krg2, L.sp1};
+  }
+  return launch_resample(J.data(), njobs, precision, cfg, st);
+}
+
+int resample_launch(const tops_lut_dev *lut, const tops_resample_job *jobs, int njobs,
+                    int precision, const TileCfg &cfg, cudaStream_t st) {
+  if (!lut || (!jobs && njobs > 0) || njobs < 0) return TOPS_E_INVALID;
+  std::vector<const tops_lut_dev *> luts(njobs, lut);
+  return resample_launch_multi(luts.data(), jobs, njobs, precision, cfg, st);
+}
+
 }  // namespace tops
+
+extern "C" int tops_resample_ex(const tops_lut_dev *lut, const tops_resample_job *jobs,
+                                int njobs, int precision, void *stream) {
+  return resample_launch(lut, jobs, njobs, precision, TileCfg(),
+                         static_cast<cudaStream_t>(stream));
+}
 
 extern "C" int tops_resample(const tops_lut_dev *lut, const tops_resample_job *jobs, int njobs,
                              void *stream) {
-  if (!lut || (!jobs && njobs > 0) || njobs < 0) return TOPS_E_INVALID;
-  std::vector<ResampleJob> J(njobs);
-  for (int j = 0; j < njobs; j++) {
-    int st = fill_resample_job(jobs[j], J[j]);
-    if (st != TOPS_OK) return st;
-  }
-  return launch_resample(lut->d, J.data(), njobs, static_cast<cudaStream_t>(stream));
+  return tops_resample_ex(lut, jobs, njobs, TOPS_PREC_SPLIT, stream);
 }

@@ -13,24 +13,13 @@
 
 #include <vector>
 
-#include "tops_pipeline.h"
+#include "pair_impl.h"
 
 namespace {
-
-size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
-
-struct OrbitFit {
-  double cx[8], cy[8], cz[8];
-  int n = 0;
-};
 
 int fit_orbit(const tops_swath_info &s, OrbitFit &f) {
   return tops_polyfit_orbit(s.n_sv, s.sv_t, s.sv_x, s.sv_y, s.sv_z, f.cx, f.cy, f.cz, &f.n);
 }
-
-struct Deramp {
-  std::vector<double> dc, fm, tref, kt;
-};
 
 int deramp_of(const tops_swath_info &s, const OrbitFit &f, Deramp &d) {
   const size_t n = (size_t)s.n_bursts * s.samples_per_burst;
@@ -82,51 +71,6 @@ int deramp_of(const tops_swath_info &s, const OrbitFit &f, Deramp &d) {
 
 }  // namespace
 
-struct tops_pair {
-  tops_swath_info m, s;
-  tops_pair_opts o;
-  int nb, L, W, dem_lines, dem_pixels;
-  OrbitFit fm, fs;
-  Deramp dm, ds;
-  std::vector<float> kaz, krg;
-  std::vector<int> ov;
-  std::vector<int> ov_off;  // line offset of each overlap in the band buffers
-  int ov_total = 0;
-  double spec_sep = 0;
-  // device memory
-  size_t slc_pitch = 0, cplx_pitch = 0, coh_pitch = 0, dem_pitch = 0;
-  char *d_master = nullptr, *d_slave = nullptr, *d_reslave = nullptr, *d_res_esd = nullptr;
-  char *d_fwd = nullptr, *d_back = nullptr;  // overlap bands when !reslave_full
-  float *d_coh = nullptr, *d_dem = nullptr;
-  double *d_kt = nullptr, *d_tref = nullptr, *d_fdc = nullptr;
-  double *d_cpm = nullptr, *d_shift = nullptr, *d_sums = nullptr;
-  int *d_status = nullptr;
-  void *d_geo_scratch = nullptr, *d_esd_scratch = nullptr;
-  size_t geo_scratch = 0, esd_scratch = 0;
-  tops_lut_dev *lut = nullptr;
-  std::vector<tops_geo_job> geo;
-  bool dem_set = false;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t graph_exec = nullptr;
-  cudaStream_t capture_stream = nullptr;  // private: the legacy stream cannot be captured
-  std::vector<void *> allocs;
-  int n_launches = 0;
-
-  int alloc(void **p, size_t bytes) {
-    cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
-    if (e != cudaSuccess) return e == cudaErrorMemoryAllocation ? TOPS_E_NOMEM : TOPS_E_CUDA;
-    allocs.push_back(*p);
-    return TOPS_OK;
-  }
-  ~tops_pair() {
-    if (graph_exec) cudaGraphExecDestroy(graph_exec);
-    if (graph) cudaGraphDestroy(graph);
-    if (capture_stream) cudaStreamDestroy(capture_stream);
-    for (void *p : allocs) cudaFree(p);
-    if (lut) tops_lut_destroy(lut);
-  }
-};
-
 extern "C" {
 
 int tops_pair_opts_default(tops_pair_opts *o) {
@@ -136,6 +80,7 @@ int tops_pair_opts_default(tops_pair_opts *o) {
   o->esd_threshold = 0.3f;
   o->reslave_full = 1;
   o->burst0_deramp_rows = 1;
+  o->precision = TOPS_PREC_SPLIT;
   return TOPS_OK;
 }
 
@@ -166,18 +111,30 @@ size_t tops_pair_footprint(const tops_swath_info *m, const tops_pair_opts *o, in
   b += (size_t)nb * 4096 * 33 * sizeof(double);       // geocoreg partials (upper bound)
   b += (size_t)nb * (W / 224 + 1) * 8 * 16;           // ESD partials (upper bound)
   b += 2 * sizeof(float) * 2048 * 12 + 2048 * 4 + 4096;
+  b += 32 * Arena::kAlign;                             // per-buffer alignment
   return b;
 }
 
 int tops_pair_create(const tops_swath_info *m, const tops_swath_info *s, const tops_pair_opts *o,
                      int dem_lines, int dem_pixels, tops_pair **out) {
+  if (dem_lines <= 0 || dem_pixels <= 0) return TOPS_E_INVALID;
+  return pair_create(m, s, o, dem_lines, dem_pixels, nullptr, nullptr, nullptr, false, out);
+}
+
+}  // extern "C"
+
+int pair_create(const tops_swath_info *m, const tops_swath_info *s, const tops_pair_opts *o,
+                int dem_lines, int dem_pixels, Arena *arena, tops_lut_dev *shared_lut,
+                cudaStream_t stream, bool async_copy, tops_pair **out) {
   if (!m || !s || !o || !out) return TOPS_E_INVALID;
   const int nb = m->n_bursts, L = m->lines_per_burst, W = m->samples_per_burst;
   if (nb < 1 || nb > TOPS_MAX_BURSTS || L < 16 || W < 16 || s->n_bursts != nb ||
-      s->lines_per_burst != L || s->samples_per_burst != W || dem_lines <= 0 || dem_pixels <= 0 ||
-      m->n_sv < 3 || s->n_sv < 3)
+      s->lines_per_burst != L || s->samples_per_burst != W || dem_lines < 0 || dem_pixels < 0 ||
+      m->n_sv < 3 || s->n_sv < 3 ||
+      (o->precision != TOPS_PREC_SPLIT && o->precision != TOPS_PREC_FP64))
     return TOPS_E_INVALID;
   tops_pair *P = new tops_pair();
+  P->arena = arena;
   P->m = *m;
   P->s = *s;
   P->o = *o;
@@ -194,10 +151,12 @@ int tops_pair_create(const tops_swath_info *m, const tops_swath_info *s, const t
   // host precomputes (reference Main.cpp:57-76, Func.cpp:2510-2555)
   if ((st = fit_orbit(*m, P->fm)) || (st = fit_orbit(*s, P->fs))) return fail(st);
   if ((st = deramp_of(*m, P->fm, P->dm)) || (st = deramp_of(*s, P->fs, P->ds))) return fail(st);
-  P->kaz.resize(2048 * 12);
-  P->krg.resize(2048 * 12);
-  if ((st = tops_lut(12, m->prf, m->az_bandwidth, 2 * m->rsr, P->kaz.data(), P->krg.data())))
-    return fail(st);
+  if (!shared_lut) {
+    P->kaz.resize(2048 * 12);
+    P->krg.resize(2048 * 12);
+    if ((st = tops_lut(12, m->prf, m->az_bandwidth, 2 * m->rsr, P->kaz.data(), P->krg.data())))
+      return fail(st);
+  }
   if (nb > 1) {
     P->ov.resize(nb - 1);
     int tot = 0, mx = 0;
@@ -234,7 +193,7 @@ int tops_pair_create(const tops_swath_info *m, const tops_swath_info *s, const t
   }
   P_ALLOC(P->d_res_esd, lines * P->cplx_pitch);
   P_ALLOC(P->d_coh, lines * P->coh_pitch);
-  P_ALLOC(P->d_dem, (size_t)dem_lines * P->dem_pitch);
+  if (dem_lines > 0) P_ALLOC(P->d_dem, (size_t)dem_lines * P->dem_pitch);
   P_ALLOC(P->d_kt, sizeof(double) * lines / L * W);
   P_ALLOC(P->d_tref, sizeof(double) * lines / L * W);
   P_ALLOC(P->d_fdc, sizeof(double) * lines / L * W);
@@ -245,12 +204,25 @@ int tops_pair_create(const tops_swath_info *m, const tops_swath_info *s, const t
   P->geo_scratch = (size_t)nb * 4096 * 33 * sizeof(double);
   P_ALLOC(P->d_geo_scratch, P->geo_scratch);
 #undef P_ALLOC
-  // slave deramp rows (Func.cpp:2383 passes burst 0's rows for every burst)
-  if (cudaMemcpy(P->d_kt, P->ds.kt.data(), sizeof(double) * nb * W, cudaMemcpyHostToDevice) ||
-      cudaMemcpy(P->d_tref, P->ds.tref.data(), sizeof(double) * nb * W, cudaMemcpyHostToDevice) ||
-      cudaMemcpy(P->d_fdc, P->ds.dc.data(), sizeof(double) * nb * W, cudaMemcpyHostToDevice))
+  // slave deramp rows (Func.cpp:2383 passes burst 0's rows for every burst);
+  // the host vectors live in the plan, so an asynchronous copy may be pending
+  const size_t rb = sizeof(double) * nb * W;
+  if (async_copy) {
+    if (cudaMemcpyAsync(P->d_kt, P->ds.kt.data(), rb, cudaMemcpyHostToDevice, stream) ||
+        cudaMemcpyAsync(P->d_tref, P->ds.tref.data(), rb, cudaMemcpyHostToDevice, stream) ||
+        cudaMemcpyAsync(P->d_fdc, P->ds.dc.data(), rb, cudaMemcpyHostToDevice, stream))
+      return fail(TOPS_E_CUDA);
+  } else if (cudaMemcpy(P->d_kt, P->ds.kt.data(), rb, cudaMemcpyHostToDevice) ||
+             cudaMemcpy(P->d_tref, P->ds.tref.data(), rb, cudaMemcpyHostToDevice) ||
+             cudaMemcpy(P->d_fdc, P->ds.dc.data(), rb, cudaMemcpyHostToDevice)) {
     return fail(TOPS_E_CUDA);
-  if ((st = tops_lut_create(P->kaz.data(), P->krg.data(), &P->lut))) return fail(st);
+  }
+  if (shared_lut) {
+    P->lut = shared_lut;
+    P->lut_owned = false;
+  } else if ((st = tops_lut_create(P->kaz.data(), P->krg.data(), &P->lut))) {
+    return fail(st);
+  }
   // ESD scratch
   if (nb > 1) {
     std::vector<tops_esd_overlap> ovs(nb - 1);
@@ -274,6 +246,8 @@ int tops_pair_create(const tops_swath_info *m, const tops_swath_info *s, const t
   return TOPS_OK;
 }
 
+extern "C" {
+
 int tops_pair_destroy(tops_pair *p) {
   delete p;
   return TOPS_OK;
@@ -281,22 +255,32 @@ int tops_pair_destroy(tops_pair *p) {
 
 int tops_pair_set_dem(tops_pair *P, const float *dem, double lat0, double lon0, double dlat,
                       double dlon, const tops_dem_window *win, void *stream) {
-  if (!P || !dem || !win) return TOPS_E_INVALID;
+  if (!P || !dem || !win || !P->d_dem) return TOPS_E_INVALID;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   P_CUDA(cudaMemcpy2DAsync(P->d_dem, P->dem_pitch, dem, (size_t)P->dem_pixels * 4,
                            (size_t)P->dem_pixels * 4, P->dem_lines, cudaMemcpyHostToDevice, st));
+  return pair_bind_dem(P, P->d_dem, P->dem_pitch, P->dem_lines, P->dem_pixels, lat0, lon0, dlat,
+                       dlon, win);
+}
+
+}  // extern "C"
+
+int pair_bind_dem(tops_pair *P, const float *d_dem, size_t dem_pitch, int dem_lines,
+                  int dem_pixels, double lat0, double lon0, double dlat, double dlon,
+                  const tops_dem_window *win) {
+  if (!P || !d_dem || !win) return TOPS_E_INVALID;
   const int nb = P->nb, L = P->L, W = P->W;
   P->geo.assign(nb, tops_geo_job());
   for (int b = 0; b < nb; b++) {
     const tops_dem_window &w = win[b];
-    if (w.row0 < 0 || w.col0 < 0 || w.rows < 1 || w.cols < 1 || w.row0 + w.rows > P->dem_lines ||
-        w.col0 + w.cols > P->dem_pixels)
+    if (w.row0 < 0 || w.col0 < 0 || w.rows < 1 || w.cols < 1 || w.row0 + w.rows > dem_lines ||
+        w.col0 + w.cols > dem_pixels)
       return TOPS_E_INVALID;
     tops_geo_job &g = P->geo[b];
     memset(&g, 0, sizeof(g));
-    g.dem = reinterpret_cast<const float *>(reinterpret_cast<const char *>(P->d_dem) +
-                                            (size_t)w.row0 * P->dem_pitch) + w.col0;
-    g.dem_pitch = P->dem_pitch;
+    g.dem = reinterpret_cast<const float *>(reinterpret_cast<const char *>(d_dem) +
+                                            (size_t)w.row0 * dem_pitch) + w.col0;
+    g.dem_pitch = dem_pitch;
     g.dem_lines = w.rows;
     g.dem_pixels = w.cols;
     g.lat0 = lat0 - w.row0 * dlat;
@@ -335,6 +319,8 @@ int tops_pair_set_dem(tops_pair *P, const float *dem, double lat0, double lon0, 
   return TOPS_OK;
 }
 
+extern "C" {
+
 int tops_pair_upload(tops_pair *P, const void *master, const void *slave, void *stream) {
   if (!P || !master || !slave) return TOPS_E_INVALID;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -371,15 +357,11 @@ static tops_resample_job base_job(const tops_pair *P, int b) {
   return j;
 }
 
-int tops_pair_run(tops_pair *P, void *stream) {
-  if (!P || !P->dem_set) return TOPS_E_INVALID;
-  const int nb = P->nb, L = P->L, W = P->W;
-  int launches = 0;
-  // 1. geometric coregistration of every burst (2 kernels)
-  P_TRY(tops_geocoreg(P->geo.data(), nb, P->d_geo_scratch, P->geo_scratch, stream));
-  launches += 2;
-  // 2. resample without shift: full ReSlave, or only the overlap bands
-  std::vector<tops_resample_job> jobs;
+}  // extern "C"
+
+// ---- stage job lists of one pair (shared by the single-pair and batched runs)
+void pair_rs1_jobs(const tops_pair *P, std::vector<tops_resample_job> &jobs) {
+  const int nb = P->nb, L = P->L;
   if (P->o.reslave_full) {
     for (int b = 0; b < nb; b++) {
       tops_resample_job j = base_job(P, b);
@@ -401,53 +383,52 @@ int tops_pair_run(tops_pair *P, void *stream) {
       jobs.push_back(k);
     }
   }
-  if (!jobs.empty()) {
-    P_TRY(tops_resample(P->lut, jobs.data(), (int)jobs.size(), stream));
-    launches += 1;
-  }
-  // 3. ESD over the overlaps (shifts stay on the device)
-  if (nb > 1) {
-    std::vector<tops_esd_overlap> ovs(nb - 1);
-    for (int i = 0; i < nb - 1; i++) {
-      tops_esd_overlap &e = ovs[i];
-      const size_t fl = (size_t)(i + 1) * L - P->ov[i], bl = (size_t)(i + 1) * L;
-      e.mF = P->d_master + fl * P->slc_pitch;
-      e.mB = P->d_master + bl * P->slc_pitch;
-      e.m_pitch = P->slc_pitch;
-      if (P->o.reslave_full) {
-        e.sF = P->d_reslave + fl * P->cplx_pitch;
-        e.sB = P->d_reslave + bl * P->cplx_pitch;
-      } else {
-        e.sF = P->d_fwd + (size_t)P->ov_off[i] * P->cplx_pitch;
-        e.sB = P->d_back + (size_t)P->ov_off[i] * P->cplx_pitch;
-      }
-      e.s_pitch = P->cplx_pitch;
-      e.lines = P->ov[i];
-      e.pixels = W;
-      e.spec_sep = P->spec_sep;
-      e.dt = P->m.dt;
+}
+
+void pair_esd_overlaps(const tops_pair *P, std::vector<tops_esd_overlap> &ovs) {
+  const int nb = P->nb, L = P->L, W = P->W;
+  for (int i = 0; i < nb - 1; i++) {
+    tops_esd_overlap e;
+    memset(&e, 0, sizeof(e));
+    const size_t fl = (size_t)(i + 1) * L - P->ov[i], bl = (size_t)(i + 1) * L;
+    e.mF = P->d_master + fl * P->slc_pitch;
+    e.mB = P->d_master + bl * P->slc_pitch;
+    e.m_pitch = P->slc_pitch;
+    if (P->o.reslave_full) {
+      e.sF = P->d_reslave + fl * P->cplx_pitch;
+      e.sB = P->d_reslave + bl * P->cplx_pitch;
+    } else {
+      e.sF = P->d_fwd + (size_t)P->ov_off[i] * P->cplx_pitch;
+      e.sB = P->d_back + (size_t)P->ov_off[i] * P->cplx_pitch;
     }
-    P_TRY(tops_esd(ovs.data(), nb - 1, P->o.win_az, P->o.win_rg, P->o.esd_threshold, P->d_shift,
-                   P->d_sums, P->d_esd_scratch, P->esd_scratch, stream));
-    launches += 2;
+    e.s_pitch = P->cplx_pitch;
+    e.lines = P->ov[i];
+    e.pixels = W;
+    e.spec_sep = P->spec_sep;
+    e.dt = P->m.dt;
+    ovs.push_back(e);
   }
-  // 4. resample with the ESD shift of the preceding overlap (first burst
-  //    uncorrected, Func.cpp:2653-2702)
-  jobs.clear();
+}
+
+// shifts: the device ESD shifts of this pair's overlaps
+void pair_rs2_jobs(const tops_pair *P, const double *shifts,
+                   std::vector<tops_resample_job> &jobs) {
+  const int nb = P->nb, L = P->L;
   for (int b = 0; b < nb; b++) {
     tops_resample_job j = base_job(P, b);
     j.out = P->d_res_esd + (size_t)b * L * P->cplx_pitch;
     j.out_rows = -1;
-    if (b > 0) j.az_shift_dev = P->d_shift + (b - 1);
+    if (b > 0) j.az_shift_dev = shifts + (b - 1);
     j.dt = P->m.dt;   // DerampDemodResample_ESD gets the master's interval (Func.cpp:2704)
     jobs.push_back(j);
   }
-  P_TRY(tops_resample(P->lut, jobs.data(), nb, stream));
-  launches += 1;
-  // 5. coherence of master vs ReSlaveESD
-  std::vector<tops_coh_job> cj(nb);
+}
+
+void pair_coh_jobs(const tops_pair *P, std::vector<tops_coh_job> &cj) {
+  const int nb = P->nb, L = P->L, W = P->W;
   for (int b = 0; b < nb; b++) {
-    tops_coh_job &c = cj[b];
+    tops_coh_job c;
+    memset(&c, 0, sizeof(c));
     c.master = P->d_master + (size_t)b * L * P->slc_pitch;
     c.master_pitch = P->slc_pitch;
     c.slave = P->d_res_esd + (size_t)b * L * P->cplx_pitch;
@@ -457,9 +438,87 @@ int tops_pair_run(tops_pair *P, void *stream) {
     c.coh_pitch = P->coh_pitch;
     c.lines = L;
     c.pixels = W;
+    cj.push_back(c);
   }
+}
+
+extern "C" {
+
+int tops_pair_run(tops_pair *P, void *stream) {
+  if (!P || !P->dem_set) return TOPS_E_INVALID;
+  const int nb = P->nb;
+  int launches = 0;
+  // 1. geometric coregistration of every burst (2 kernels)
+  P_TRY(tops_geocoreg(P->geo.data(), nb, P->d_geo_scratch, P->geo_scratch, stream));
+  launches += 2;
+  // 2. resample without shift: full ReSlave, or only the overlap bands
+  std::vector<tops_resample_job> jobs;
+  pair_rs1_jobs(P, jobs);
+  if (!jobs.empty()) {
+    P_TRY(tops_resample_ex(P->lut, jobs.data(), (int)jobs.size(), P->o.precision, stream));
+    launches += 1;
+  }
+  // 3. ESD over the overlaps (shifts stay on the device)
+  if (nb > 1) {
+    std::vector<tops_esd_overlap> ovs;
+    pair_esd_overlaps(P, ovs);
+    P_TRY(tops_esd(ovs.data(), nb - 1, P->o.win_az, P->o.win_rg, P->o.esd_threshold, P->d_shift,
+                   P->d_sums, P->d_esd_scratch, P->esd_scratch, stream));
+    launches += 2;
+  }
+  // 4. resample with the ESD shift of the preceding overlap (first burst
+  //    uncorrected, Func.cpp:2653-2702)
+  jobs.clear();
+  pair_rs2_jobs(P, P->d_shift, jobs);
+  P_TRY(tops_resample_ex(P->lut, jobs.data(), nb, P->o.precision, stream));
+  launches += 1;
+  // 5. coherence of master vs ReSlaveESD
+  std::vector<tops_coh_job> cj;
+  pair_coh_jobs(P, cj);
   P_TRY(tops_coherence(cj.data(), nb, P->o.win_rg, P->o.win_az, stream));
   launches += 1;
+  P->n_launches = launches;
+  return TOPS_OK;
+}
+
+// The per-burst launch loop: every stage launched once per burst (or
+// overlap), as the reference's drivers call their stages; the comparison form
+// for the batched plans.
+int tops_pair_run_per_burst(tops_pair *P, void *stream) {
+  if (!P || !P->dem_set) return TOPS_E_INVALID;
+  const int nb = P->nb;
+  int launches = 0;
+  for (int b = 0; b < nb; b++) {
+    P_TRY(tops_geocoreg(&P->geo[b], 1, P->d_geo_scratch, P->geo_scratch, stream));
+    launches += 2;
+  }
+  std::vector<tops_resample_job> jobs;
+  pair_rs1_jobs(P, jobs);
+  for (const tops_resample_job &j : jobs) {
+    P_TRY(tops_resample_ex(P->lut, &j, 1, P->o.precision, stream));
+    launches += 1;
+  }
+  if (nb > 1) {
+    std::vector<tops_esd_overlap> ovs;
+    pair_esd_overlaps(P, ovs);
+    for (int i = 0; i < nb - 1; i++) {
+      P_TRY(tops_esd(&ovs[i], 1, P->o.win_az, P->o.win_rg, P->o.esd_threshold, P->d_shift + i,
+                     P->d_sums + 2 * i, P->d_esd_scratch, P->esd_scratch, stream));
+      launches += 2;
+    }
+  }
+  jobs.clear();
+  pair_rs2_jobs(P, P->d_shift, jobs);
+  for (const tops_resample_job &j : jobs) {
+    P_TRY(tops_resample_ex(P->lut, &j, 1, P->o.precision, stream));
+    launches += 1;
+  }
+  std::vector<tops_coh_job> cj;
+  pair_coh_jobs(P, cj);
+  for (const tops_coh_job &c : cj) {
+    P_TRY(tops_coherence(&c, 1, P->o.win_rg, P->o.win_az, stream));
+    launches += 1;
+  }
   P->n_launches = launches;
   return TOPS_OK;
 }

@@ -31,6 +31,8 @@ TOPS_E_TIMEOUT = 5
 TOPS_E_BUDGET = 6
 TOPS_E_CONFIG = 7
 TOPS_E_NODEVICE = 8
+PREC_SPLIT = 0
+PREC_FP64 = 1
 LUT_BINS = 2048
 NPOINTS = 12
 MAX_BURSTS = 16
@@ -226,6 +228,7 @@ _proto("tops_free_device", C.c_int, [_vp])
 _proto("tops_lut_create", C.c_int, [_fp, _fp, C.POINTER(_vp)])
 _proto("tops_lut_destroy", C.c_int, [_vp])
 _proto("tops_resample", C.c_int, [_vp, C.POINTER(ResampleJob), C.c_int, _vp])
+_proto("tops_resample_ex", C.c_int, [_vp, C.POINTER(ResampleJob), C.c_int, C.c_int, _vp])
 _proto("tops_coherence", C.c_int, [C.POINTER(CohJob), C.c_int, C.c_int, C.c_int, _vp])
 _proto("tops_esd_scratch_bytes", C.c_size_t, [C.POINTER(EsdOverlap), C.c_int])
 _proto("tops_esd", C.c_int, [C.POINTER(EsdOverlap), C.c_int, C.c_int, C.c_int, C.c_float, _vp,
@@ -515,7 +518,8 @@ def geocoreg_warp(dem_int, lat0, lon0, dlat, dlon, xmin, xmax, ymin, ymax, m_bur
 # ------------------------------------------------------- burst-pair pipeline
 class PairOpts(C.Structure):
     _fields_ = [("win_rg", C.c_int), ("win_az", C.c_int), ("esd_threshold", C.c_float),
-                ("reslave_full", C.c_int), ("burst0_deramp_rows", C.c_int)]
+                ("reslave_full", C.c_int), ("burst0_deramp_rows", C.c_int),
+                ("precision", C.c_int)]
 
 
 class DemWindow(C.Structure):
@@ -548,6 +552,22 @@ _proto("tops_plain_pair", C.c_int, [C.POINTER(SwathInfo), C.POINTER(SwathInfo), 
                                     _ip, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                     C.c_double, C.POINTER(DemWindow), _vp, _vp, _vp, _vp, _fp, _dp,
                                     _dp])
+
+
+class Tune(C.Structure):
+    _fields_ = [("rs_seg_rows", C.c_int), ("rs_persistent", C.c_int),
+                ("coh_seg_rows", C.c_int), ("coh_persistent", C.c_int)]
+
+
+_proto("tops_pair_run_per_burst", C.c_int, [_vp, _vp])
+_proto("tops_batch_create", C.c_int, [C.POINTER(_vp), C.c_int, C.POINTER(_vp)])
+_proto("tops_batch_destroy", C.c_int, [_vp])
+_proto("tops_batch_run", C.c_int, [_vp, _vp])
+_proto("tops_batch_run_graph", C.c_int, [_vp, _vp])
+_proto("tops_batch_launches", C.c_int, [_vp])
+_proto("tops_batch_set_tune", C.c_int, [_vp, C.POINTER(Tune)])
+_proto("tops_batch_get_tune", C.c_int, [_vp, C.POINTER(Tune)])
+_proto("tops_batch_autotune", C.c_int, [_vp, _vp, C.POINTER(Tune), _dp])
 
 
 def pair_opts(**kw) -> PairOpts:
@@ -602,6 +622,9 @@ class Pair:
         f = lib.tops_pair_run_graph if graph else lib.tops_pair_run
         check(f(self._h, C.c_void_p(stream)), "tops_pair_run")
 
+    def run_per_burst(self, stream=0):
+        check(lib.tops_pair_run_per_burst(self._h, C.c_void_p(stream)), "tops_pair_run_per_burst")
+
     def download(self, reslave=True, stream=0):
         n = self.nb * self.L
         rs = np.zeros((n, self.W), np.complex64) if reslave else None
@@ -622,6 +645,197 @@ class Pair:
     def close(self):
         if getattr(self, "_h", None):
             lib.tops_pair_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Several device-resident plans processed together (tops_batch_*): one
+    launch per stage for all their bursts.  The plans stay owned by the
+    caller and must outlive the batch."""
+
+    def __init__(self, pairs):
+        self.pairs = list(pairs)
+        arr = (_vp * len(self.pairs))(*[p._h.value for p in self.pairs])
+        h = _vp()
+        check(lib.tops_batch_create(arr, len(self.pairs), C.byref(h)), "tops_batch_create")
+        self._h = h
+
+    def run(self, stream=0, graph=False):
+        f = lib.tops_batch_run_graph if graph else lib.tops_batch_run
+        check(f(self._h, C.c_void_p(stream)), "tops_batch_run")
+
+    def launches(self) -> int:
+        return lib.tops_batch_launches(self._h)
+
+    def tune(self, t: "Tune" = None) -> "Tune":
+        if t is not None:
+            check(lib.tops_batch_set_tune(self._h, C.byref(t)), "tops_batch_set_tune")
+        out = Tune()
+        check(lib.tops_batch_get_tune(self._h, C.byref(out)), "tops_batch_get_tune")
+        return out
+
+    def autotune(self, stream=0):
+        best = Tune()
+        ms = np.zeros(2)
+        check(lib.tops_batch_autotune(self._h, C.c_void_p(stream), C.byref(best),
+                                      ptr(ms, C.c_double)), "tops_batch_autotune")
+        return best, ms
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.tops_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------ serving loop
+class ServerCfg(C.Structure):
+    _fields_ = [("hbm_budget", C.c_size_t), ("slots", C.c_int)]
+
+
+class JobDesc(C.Structure):
+    _fields_ = [("master", SwathInfo), ("slave", SwathInfo), ("opts", PairOpts),
+                ("dem_id", C.c_int), ("windows", DemWindow * MAX_BURSTS),
+                ("master_slc", C.c_void_p), ("slave_slc", C.c_void_p),
+                ("reslave", C.c_void_p), ("reslave_esd", C.c_void_p), ("coh", C.c_void_p),
+                ("cpm", C.c_void_p), ("shifts", C.c_void_p)]
+
+
+class JobDone(C.Structure):
+    _fields_ = [("job_id", C.c_long), ("status", C.c_int), ("arrival_s", C.c_double),
+                ("admit_s", C.c_double), ("done_s", C.c_double), ("footprint", C.c_size_t)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_long), ("admitted", C.c_long), ("completed", C.c_long),
+                ("rejected", C.c_long), ("queued", C.c_long), ("running", C.c_long),
+                ("hbm_in_use", C.c_size_t), ("hbm_peak", C.c_size_t)]
+
+
+_proto("tops_server_create", C.c_int, [C.POINTER(ServerCfg), C.POINTER(_vp)])
+_proto("tops_server_destroy", C.c_int, [_vp])
+_proto("tops_server_add_dem", C.c_int, [_vp, _fp, C.c_int, C.c_int, C.c_double, C.c_double,
+                                        C.c_double, C.c_double, _ip])
+_proto("tops_server_submit", C.c_int, [_vp, C.POINTER(JobDesc), C.POINTER(C.c_long)])
+_proto("tops_server_progress", C.c_int, [_vp])
+_proto("tops_server_poll", C.c_int, [_vp, C.POINTER(JobDone), C.c_int, _ip])
+_proto("tops_server_drain", C.c_int, [_vp])
+_proto("tops_server_get_stats", C.c_int, [_vp, C.POINTER(ServerStats)])
+_proto("tops_server_job_footprint", C.c_size_t, [C.POINTER(JobDesc)])
+_proto("tops_arena_create", C.c_int, [C.c_size_t, C.c_size_t, C.POINTER(_vp)])
+_proto("tops_arena_destroy", C.c_int, [_vp])
+_proto("tops_arena_alloc", C.c_size_t, [_vp, C.c_size_t])
+_proto("tops_arena_release", C.c_int, [_vp, C.c_size_t])
+_proto("tops_arena_in_use", C.c_size_t, [_vp])
+_proto("tops_arena_largest_free", C.c_size_t, [_vp])
+_proto("tops_arena_free_ranges", C.c_int, [_vp])
+
+
+def sub_swath(info: SwathInfo, b0: int, k: int) -> SwathInfo:
+    """The description of bursts [b0, b0+k) of a sub-swath as a k-burst
+    sub-swath: burst times, the per-burst FM-rate list and (when the
+    annotation holds one estimate per burst) the DC list shift with it."""
+    out = SwathInfo()
+    C.memmove(C.byref(out), C.byref(info), C.sizeof(SwathInfo))
+    out.n_bursts = k
+    for i in range(k):
+        out.burst_first_line_time[i] = info.burst_first_line_time[b0 + i]
+        out.burst_last_line_time[i] = info.burst_last_line_time[b0 + i]
+    for i in range(info.n_fm - b0):
+        out.fm_list[i] = info.fm_list[b0 + i]
+    out.n_fm = info.n_fm - b0
+    if info.n_dc > info.n_bursts:
+        for i in range(info.n_dc - b0):
+            out.dc_list[i] = info.dc_list[b0 + i]
+        out.n_dc = info.n_dc - b0
+    return out
+
+
+class Server:
+    """tops_server_*: burst-pair jobs admitted by HBM footprint, one stream
+    per slot.  Host buffers of a job must stay alive until it is done."""
+
+    def __init__(self, hbm_budget: int, slots: int):
+        cfg = ServerCfg(hbm_budget, slots)
+        h = _vp()
+        check(lib.tops_server_create(C.byref(cfg), C.byref(h)), "tops_server_create")
+        self._h = h
+        self._keep = {}
+
+    def add_dem(self, dem, lat0, lon0, dlat, dlon) -> int:
+        dem = np.ascontiguousarray(dem, np.float32)
+        i = C.c_int()
+        check(lib.tops_server_add_dem(self._h, ptr(dem, C.c_float), dem.shape[0], dem.shape[1],
+                                      lat0, lon0, dlat, dlon, C.byref(i)), "tops_server_add_dem")
+        return i.value
+
+    def job(self, scene: "Scene", dem_id: int, b0: int = 0, k: int = None, opts=None,
+            outputs=None, master_slc=None, slave_slc=None):
+        """A job over bursts [b0, b0+k) of a scene; returns (desc, outputs)."""
+        k = scene.cfg.n_bursts - b0 if k is None else k
+        L, W = scene.cfg.lines_per_burst, scene.cfg.samples_per_burst
+        d = JobDesc()
+        d.master = sub_swath(scene.swath[0], b0, k)
+        d.slave = sub_swath(scene.swath[1], b0, k)
+        d.opts = opts or pair_opts()
+        d.dem_id = dem_id
+        for i in range(k):
+            r0, c0, nr, nc = scene.dem_window(b0 + i)
+            d.windows[i] = DemWindow(r0, c0, nr, nc)
+        m = scene.slc[0] if master_slc is None else master_slc
+        s = scene.slc[1] if slave_slc is None else slave_slc
+        d.master_slc = m.ctypes.data + b0 * L * W * 4
+        d.slave_slc = s.ctypes.data + b0 * L * W * 4
+        if outputs is None:
+            outputs = dict(reslave=np.zeros((k * L, W), np.complex64),
+                           reslave_esd=np.zeros((k * L, W), np.complex64),
+                           coh=np.zeros((k * L, W), np.float32), cpm=np.zeros((k, 12)),
+                           shifts=np.zeros(max(k - 1, 1)))
+        for f in ("reslave", "reslave_esd", "coh", "cpm", "shifts"):
+            a = outputs.get(f)
+            setattr(d, f, a.ctypes.data if a is not None else None)
+        return d, outputs
+
+    def submit(self, desc: JobDesc, keep=None) -> int:
+        jid = C.c_long()
+        check(lib.tops_server_submit(self._h, C.byref(desc), C.byref(jid)), "tops_server_submit")
+        self._keep[jid.value] = (desc, keep)
+        return jid.value
+
+    def progress(self):
+        check(lib.tops_server_progress(self._h), "tops_server_progress")
+
+    def poll(self, max_n=256):
+        arr = (JobDone * max_n)()
+        n = C.c_int()
+        check(lib.tops_server_poll(self._h, arr, max_n, C.byref(n)), "tops_server_poll")
+        out = [arr[i] for i in range(n.value)]
+        for d in out:
+            self._keep.pop(d.job_id, None)
+        return out
+
+    def drain(self):
+        check(lib.tops_server_drain(self._h), "tops_server_drain")
+
+    def stats(self) -> ServerStats:
+        st = ServerStats()
+        check(lib.tops_server_get_stats(self._h, C.byref(st)), "tops_server_get_stats")
+        return st
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.tops_server_destroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -96,6 +96,73 @@ def test_resample_steep_polynomial(T, O, scene_small):
     assert rel_rms(gpu, ref) < RS_TOL
 
 
+def _resample_device(T, kw, precision, out_offset=0, slave_offset=0):
+    """tops_resample_ex on device buffers; out_offset / slave_offset (bytes)
+    misalign the output and slave bases to force the scalar-access paths."""
+    import ctypes as C
+    import torch
+    slave = np.ascontiguousarray(kw["slave"], np.int16)
+    L, W = slave.shape[0], slave.shape[1]
+    s_dev = torch.zeros(slave.nbytes + 64, dtype=torch.uint8, device="cuda")
+    s_dev[slave_offset:slave_offset + slave.nbytes].copy_(
+        torch.from_numpy(slave.view(np.uint8).reshape(-1)))
+    o_dev = torch.zeros(L * W * 8 + 64, dtype=torch.uint8, device="cuda")
+    par = [torch.from_numpy(np.ascontiguousarray(kw[k], np.float64)).cuda()
+           for k in ("kt", "tref", "fdc")]
+    lut = C.c_void_p()
+    kaz = np.ascontiguousarray(kw["kaz"], np.float32)
+    krg = np.ascontiguousarray(kw["krg"], np.float32)
+    T.check(T.lib.tops_lut_create(T.ptr(kaz, C.c_float), T.ptr(krg, C.c_float), C.byref(lut)),
+            "lut")
+    j = T.ResampleJob()
+    j.slave, j.slave_pitch = s_dev.data_ptr() + slave_offset, W * 4
+    j.out, j.out_pitch = o_dev.data_ptr() + out_offset, W * 8
+    j.kt, j.tref, j.fdc = (t.data_ptr() for t in par)
+    for i in range(4):
+        j.mbox[i], j.sbox[i] = int(kw["mbox"][i]), int(kw["sbox"][i])
+    for i in range(6):
+        j.cpm_az[i], j.cpm_rg[i] = kw["cpm_az"][i], kw["cpm_rg"][i]
+    j.az_shift = kw["az_shift"]
+    j.s_first_line = kw["s_burst_idx"] * kw["lines_per_burst"]
+    j.dt = kw["dt"]
+    j.out_row0, j.out_rows = 0, -1
+    stream = torch.cuda.current_stream().cuda_stream
+    T.check(T.lib.tops_resample_ex(lut, C.byref(j), 1, precision, C.c_void_p(stream)),
+            "tops_resample_ex")
+    torch.cuda.synchronize()
+    T.lib.tops_lut_destroy(lut)
+    out = o_dev[out_offset:out_offset + L * W * 8].cpu().numpy().view(np.complex64)
+    return out.reshape(L, W)
+
+
+@pytest.mark.parametrize("prec", ["split", "fp64"])
+def test_resample_precision_modes(T, O, scene_small, prec):
+    """Both deramp-phase precisions against the FP64 oracle; the FP64 mode
+    also agrees with the reference's phase sum to FP32 rounding."""
+    S = scene_small
+    cpm = oracle_cpm(O, S, 1)
+    kw = rs_inputs(S, 1, cpm, 0.0371)
+    mode = T.PREC_SPLIT if prec == "split" else T.PREC_FP64
+    gpu = _resample_device(T, kw, mode)
+    ref, _ = O.resample(**kw)
+    err = rel_rms(gpu, ref)
+    assert err < RS_TOL, err
+    if prec == "fp64":
+        assert err < 1e-5, err
+
+
+def test_resample_unaligned_buffers(T, O, scene_small):
+    """Misaligned slave / output bases take the scalar-access paths."""
+    S = scene_small
+    cpm = oracle_cpm(O, S, 0)
+    kw = rs_inputs(S, 0, cpm)
+    ref, _ = O.resample(**kw)
+    a = _resample_device(T, kw, T.PREC_SPLIT, out_offset=8, slave_offset=4)
+    b = _resample_device(T, kw, T.PREC_SPLIT)
+    assert rel_rms(a, ref) < RS_TOL
+    assert rel_rms(a, b) < 1e-6
+
+
 def test_resample_deterministic(T, O, scene_small):
     S = scene_small
     cpm = oracle_cpm(O, S, 1)
