@@ -304,6 +304,219 @@ def run_batch(args, rank, world):
         P.close()
 
 
+SERVE_RATE = 40.0          # jobs/s (Poisson)
+SERVE_BUDGET = 150 << 30   # bytes of HBM the jobs may hold at once
+SERVE_SLOTS = 8
+
+
+def serve_jobs(n, shapes):
+    """Seeded job stream: arrival time, sub-swath, first burst, bursts (1-9)."""
+    rng = np.random.default_rng(SERVE_SEED)
+    t = np.cumsum(rng.exponential(1.0 / SERVE_RATE, n))
+    jobs = []
+    for i in range(n):
+        s = int(rng.integers(len(shapes)))
+        k = int(rng.integers(1, shapes[s]["n_bursts"] + 1))
+        b0 = int(rng.integers(0, shapes[s]["n_bursts"] - k + 1))
+        jobs.append((float(t[i]), s, b0, k))
+    return jobs
+
+
+SERVE_SEED = 7
+
+
+def run_serve(args, rank, world):
+    """Serving: a seeded Poisson stream of burst-pair jobs (1-9 bursts of the
+    three uneven sub-swaths) through the serving loop -- admission by HBM
+    footprint under a 150 GB budget, one stream per slot, DEM tiles resident.
+    Reports latency percentiles and sustained throughput, then a closed-loop
+    pass (all jobs at once) for the saturation throughput.  Jobs produce the
+    final products (ReSlaveESD, coherence, offsets, shifts); the first-pass
+    resample covers only the overlap bands ESD needs."""
+    import torch
+    import topsb200 as T
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    shapes = batch_shapes()
+    t0 = time.time()
+    scenes = [T.Scene(**sh) for sh in shapes]
+    gen_s = time.time() - t0
+    pin = [(torch.from_numpy(S.slc[0]).pin_memory(), torch.from_numpy(S.slc[1]).pin_memory())
+           for S in scenes]
+    slc = [(a.numpy(), b.numpy()) for a, b in pin]
+    # one pinned sink for every job's outputs (timing only; results are
+    # checked by the tests)
+    mx = max(sh["n_bursts"] * sh["lines_per_burst"] * sh["samples_per_burst"] for sh in shapes)
+    sink_c = torch.empty(mx * 2, dtype=torch.float32).pin_memory().numpy().view(np.complex64)
+    sink_f = torch.empty(mx, dtype=torch.float32).pin_memory().numpy()
+    sink = dict(reslave=None, reslave_esd=sink_c, coh=sink_f, cpm=np.zeros((9, 12)),
+                shifts=np.zeros(8))
+    opts = T.pair_opts(win_rg=WIN_RG, win_az=WIN_AZ, reslave_full=0)
+
+    def one_pass(jobs, closed_loop):
+        srv = T.Server(SERVE_BUDGET, SERVE_SLOTS)
+        dems = [srv.add_dem(S.dem, S.dem_info.lat0, S.dem_info.lon0, S.dem_info.dlat,
+                            S.dem_info.dlon) for S in scenes]
+        descs = [srv.job(scenes[s], dems[s], b0, k, opts=opts, outputs=sink,
+                         master_slc=slc[s][0], slave_slc=slc[s][1])[0] for _, s, b0, k in jobs]
+        torch.cuda.synchronize()
+        start = time.perf_counter()
+        for (ta, s, b0, k), d in zip(jobs, descs):
+            if not closed_loop:
+                while time.perf_counter() - start < ta:
+                    srv.progress()
+            srv.submit(d)
+        srv.drain()
+        done = srv.poll(4096)
+        st = srv.stats()
+        srv.close()
+        assert all(x.status == T.TOPS_OK for x in done), [x.status for x in done]
+        lat = np.array([x.done_s - x.arrival_s for x in done]) * 1e3
+        queue = np.array([x.admit_s - x.arrival_s for x in done]) * 1e3
+        span = max(x.done_s for x in done) - min(x.arrival_s for x in done)
+        pairs = sum(k for _, _, _, k in jobs)
+        return dict(pairs_per_s=pairs / span, jobs=len(done), pairs=pairs, span_s=span,
+                    latency_ms={"p50": float(np.percentile(lat, 50)),
+                                "p99": float(np.percentile(lat, 99)),
+                                "max": float(lat.max())},
+                    queue_ms={"p50": float(np.percentile(queue, 50)),
+                              "p99": float(np.percentile(queue, 99))},
+                    hbm_peak_gb=st.hbm_peak / 1e9)
+
+    jobs = serve_jobs(args.jobs, shapes)
+    one_pass(jobs[:4], True)                        # warm-up: LUTs, kernel attributes
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        open_loop = one_pass(jobs, False)
+    closed = one_pass(jobs, True)
+    # plain per-burst form on one 3-burst job for the comparison
+    S = scenes[0]
+    t = time.perf_counter()
+    T.plain_pair(S, T.pair_opts(win_rg=WIN_RG, win_az=WIN_AZ))
+    plain = S.cfg.n_bursts / (time.perf_counter() - t)
+    line = {
+        "metric": METRIC, "value": closed["pairs_per_s"], "unit": UNIT, "n_gpus": world,
+        "steps": 1, "warmup": 1, "ms_per_step": closed["span_s"] * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 (f64 geometry)", "data": "synthetic (seeded)",
+        "config": {"workload": f"serve: {args.jobs} Poisson jobs ({SERVE_RATE:.0f}/s), 1-9 bursts "
+                               "of 3 uneven sub-swaths",
+                   "budget_gb": SERVE_BUDGET / 2**30, "slots": SERVE_SLOTS,
+                   "window": f"{WIN_RG}x{WIN_AZ}"},
+        "open_loop": open_loop, "closed_loop": closed,
+        "plain": {"value": plain, "unit": UNIT, "job": f"{S.cfg.n_bursts} bursts of "
+                  f"{S.cfg.lines_per_burst}x{S.cfg.samples_per_burst}"},
+        "served_over_plain": closed["pairs_per_s"] / plain,
+        "clocks": clk.summary(), "scene_gen_s": gen_s,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_precision(args, rank, world):
+    """Precision variant on the small workload's inputs (2 bursts of 1500 x
+    4096): the pipeline with the split-precision deramp (default) and with the
+    all-FP64 deramp, each timed on the device and each output compared with
+    the FP64 host oracle run on the same inputs."""
+    import torch
+    import topsb200 as T
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    cfg = CONFIGS["small"]
+    S = build_scene(T, cfg, 0)
+    nb, L, W = cfg["n_bursts"], cfg["lines_per_burst"], cfg["samples_per_burst"]
+    O.set_num_threads(os.cpu_count() or 1)
+    # ---- oracle chain (FP64), as the pipeline chains the stages
+    m, s = S.swath
+    ov, _, _ = O.overlap_size(np.array(m.burst_first_line_time[:nb]),
+                              np.array(m.burst_last_line_time[:nb]), m.dt)
+    spec = O.spectral_sep(S.deramp[0]["kt"], L, m.dt)
+    d = S.deramp[1]
+    cpm, rs1, rse, coh = [], [], [], []
+    for b in range(nb):
+        g = S.geo_args(b)
+        az, rg, st, _ = O.geocoreg(np.rint(g["dem"]).astype(np.float32), g["lat0"], g["lon0"],
+                                   g["dlat"], g["dlon"], g["xmin"], g["xmax"], g["ymin"],
+                                   g["ymax"], g["dt"], g["first_line_time"], g["slr_time"],
+                                   g["range_spacing"], g["mid_time"], g["azi_init"],
+                                   g["line_offset"], g["coefs"])
+        cpm.append((az, rg))
+    kw = lambda b, sh, dt: dict(slave=S.burst(1, b), cpm_az=cpm[b][0], cpm_rg=cpm[b][1],
+                                az_shift=sh, kaz=S.kaz, krg=S.krg, s_burst_idx=b,
+                                mbox=S.boxes(b)[0], sbox=S.boxes(b)[1], lines_per_burst=L, dt=dt,
+                                kt=d["kt"][0], tref=d["tref"][0], fdc=d["dc"][0])
+    for b in range(nb):
+        rs1.append(O.resample(**kw(b, 0.0, s.dt))[0])
+    c64 = lambda a: np.ascontiguousarray(a.astype(np.complex64)).view(np.float32).reshape(
+        a.shape[0], a.shape[1], 2)
+    mF = np.concatenate([S.slc[0][(i + 1) * L - ov[i]:(i + 1) * L] for i in range(nb - 1)])
+    mB = np.concatenate([S.slc[0][(i + 1) * L:(i + 1) * L + ov[i]] for i in range(nb - 1)])
+    sF = np.concatenate([rs1[i][L - ov[i]:] for i in range(nb - 1)])
+    sB = np.concatenate([rs1[i + 1][:ov[i]] for i in range(nb - 1)])
+    shifts, _, _ = O.esd(mF, mB, c64(sF), c64(sB), ov, WIN_AZ, WIN_RG, 0.3, spec, m.dt)
+    for b in range(nb):
+        sh = shifts[b - 1] if b > 0 else 0.0
+        rse.append(O.resample(**kw(b, sh, m.dt))[0])
+        coh.append(O.coherence(S.burst(0, b), c64(rse[b]), WIN_RG, WIN_AZ))
+
+    def grid(c, b):
+        y = np.linspace(b * L, (b + 1) * L - 1, 31)
+        x = np.linspace(0, W - 1, 41)
+        Y, X = np.meshgrid(y, x, indexing="ij")
+        Lh = (Y - (b * L + 0.5 * (L - 1))) / (0.25 * (L - 1))
+        Ph = (X - 0.5 * (W - 1)) / (0.25 * (W - 1))
+        return c[0] + c[1] * Lh + c[2] * Ph + c[3] * Lh * Lh + c[4] * Lh * Ph + c[5] * Ph * Ph
+
+    rel = lambda a, r: float(np.sqrt(np.sum(np.abs(a - r) ** 2) / np.sum(np.abs(r) ** 2)))
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+    modes = {}
+    di = S.dem_info
+    for name, prec in (("split", T.PREC_SPLIT), ("fp64", T.PREC_FP64)):
+        P = T.Pair(S.swath[0], S.swath[1], S.dem.shape,
+                   T.pair_opts(win_rg=WIN_RG, win_az=WIN_AZ, precision=prec))
+        P.set_dem(np.rint(S.dem), di.lat0, di.lon0, di.dlat, di.dlon, T.scene_windows(S), sp)
+        P.upload(S.slc[0], S.slc[1], sp)
+        for _ in range(args.warmup):
+            P.run(sp, graph=True)
+        stream.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            P.run(sp, graph=True)
+        e1.record(stream)
+        stream.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        out = P.download(stream=sp)
+        stream.synchronize()
+        P.close()
+        err = {
+            "offsets_px": max(float(np.abs(grid(out["cpm"][b, :6], b) - grid(cpm[b][0], b)).max())
+                              for b in range(nb)),
+            "offsets_rg_px": max(float(np.abs(grid(out["cpm"][b, 6:], b) -
+                                              grid(cpm[b][1], b)).max()) for b in range(nb)),
+            "reslave_rel_rms": max(rel(out["reslave"][b * L:(b + 1) * L], rs1[b])
+                                   for b in range(nb)),
+            "reslave_esd_rel_rms": max(rel(out["reslave_esd"][b * L:(b + 1) * L], rse[b])
+                                       for b in range(nb)),
+            "esd_shift_px": float(np.abs(out["shifts"] - shifts).max()),
+            "coherence_max_abs": max(float(np.abs(out["coh"][b * L:(b + 1) * L] - coh[b]).max())
+                                     for b in range(nb)),
+        }
+        modes[name] = {"ms_per_step": ms, "pairs_per_s": nb * 1e3 / ms, "error_vs_fp64_oracle": err}
+    line = {
+        "metric": METRIC, "value": modes["split"]["pairs_per_s"], "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": modes["split"]["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 split / f64", "data": "synthetic (seeded)",
+        "config": {"workload": workload_name("precision (small inputs)", cfg),
+                   "window": f"{WIN_RG}x{WIN_AZ}"},
+        "modes": modes,
+        "tolerances": {"offsets_px": 1e-4, "reslave_rel_rms": 1e-4, "esd_shift_px": 1e-5,
+                       "coherence_max_abs": 1e-5},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def workload_name(name, cfg):
     return (f"{name}: {cfg['n_bursts']} burst pairs of {cfg['lines_per_burst']}x"
             f"{cfg['samples_per_burst']} CInt16, {cfg['overlap_lines']}-line overlaps, DEM "
@@ -316,7 +529,9 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="subswath", choices=sorted(CONFIGS) + ["batch"])
+    ap.add_argument("--config", default="subswath",
+                    choices=sorted(CONFIGS) + ["batch", "serve", "precision"])
+    ap.add_argument("--jobs", type=int, default=40, help="serve: number of arriving jobs")
     ap.add_argument("--e2e-steps", type=int, default=6)
     ap.add_argument("--plain-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
@@ -328,6 +543,10 @@ def main():
         return run_reference(args, rank, world)
     if args.config == "batch":
         return run_batch(args, rank, world)
+    if args.config == "serve":
+        return run_serve(args, rank, world)
+    if args.config == "precision":
+        return run_precision(args, rank, world)
 
     import torch
     import torch.distributed as dist

@@ -33,8 +33,10 @@ typedef struct {
 
 /* One job: a burst-pair plan's inputs and where its outputs go.  The swath
  * descriptions and windows are copied at submit; the host buffers must stay
- * valid until the job is reported done (pinned memory gives asynchronous
- * copies). */
+ * valid until the job is reported done.  The SLC and image buffers should be
+ * pinned: a copy between the device and pageable memory makes the enqueue
+ * wait for the job's stream, which serialises the jobs.  cpm and shifts are
+ * staged through the server's own pinned memory and copied at completion. */
 typedef struct {
   tops_swath_info master, slave;
   tops_pair_opts opts;

@@ -64,23 +64,36 @@ __device__ __forceinline__ void add4(float4 &a, const float4 &b) {
 
 // Horizontal pass of one group: CO_CPI consecutive outputs per item.  The
 // amplitude mask |s| < 0.001 of the reference (EstCoh.cu:393, 446) is
-// evaluated as |s|^2 < 1e-6.
+// evaluated as |s|^2 < 1e-6.  WRG > 0: range window known at compile time;
+// an item starts at a multiple of 8 columns, so pad8(cg + i) = pad8(cg) +
+// pad8(i) and every shared-memory offset below is a constant.
+template <int WRG>
 __device__ __forceinline__ void coh_horizontal(const CoShared &S, const CohJob &J, int tid,
-                                               int rg, int gr, int c0, int cN, int win_rg,
-                                               int dx) {
+                                               int rg, int gr, int c0, int cN, int win_rg_rt,
+                                               int dx_rt) {
   constexpr int NG = CO_TW / CO_CPI;
+  static_assert(CO_CPI % 8 == 0, "items must start at multiples of 8 columns");
+  const int win_rg = WRG > 0 ? WRG : win_rg_rt;
+  const int dx = WRG > 0 ? (WRG - 1) / 2 : dx_rt;
   for (int it = tid; it < gr * NG; it += CO_NT) {
     const int k = it / NG;
     const int cg = (it - k * NG) * CO_CPI;
     if (cg >= cN) continue;
+    const float4 *V = &S.V[k][pad8(cg)];
+    const float *Jd = &S.judge[k][pad8(cg)];
     float4 w = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int i = 0; i < win_rg; i++) add4(w, S.V[k][pad8(cg + i)]);
+    if (WRG > 0) {
+#pragma unroll
+      for (int i = 0; i < WRG; i++) add4(w, V[pad8(i)]);
+    } else {
+      for (int i = 0; i < win_rg; i++) add4(w, V[pad8(i)]);
+    }
     float out[CO_CPI];
 #pragma unroll
     for (int u = 0; u < CO_CPI; u++) {
       if (u > 0) {
-        const float4 a = S.V[k][pad8(cg + u - 1 + win_rg)];
-        const float4 b = S.V[k][pad8(cg + u - 1)];
+        const float4 a = V[pad8(u - 1 + win_rg)];
+        const float4 b = V[pad8(u - 1)];
         w.x += a.x - b.x;
         w.y += a.y - b.y;
         w.z += a.z - b.z;
@@ -88,7 +101,7 @@ __device__ __forceinline__ void coh_horizontal(const CoShared &S, const CohJob &
       }
       const float p = w.z * w.w;
       float g = (p > 0.f) ? sqrtf(w.x * w.x + w.y * w.y) * rsqrtf(p) : 0.f;
-      if (S.judge[k][pad8(cg + u + dx)] < 1e-6f) g = 0.f;
+      if (Jd[pad8(u + dx)] < 1e-6f) g = 0.f;
       out[u] = g;
     }
     float *orow = J.coh + (long)(rg + k) * J.coh_pitch + c0 + cg;
@@ -107,7 +120,7 @@ __device__ __forceinline__ void coh_horizontal(const CoShared &S, const CohJob &
 
 // One work item (strip x segment of one job); all threads of the CTA call it
 // with the same item.
-template <int WAZ>
+template <int WAZ, int WRG>
 __device__ __forceinline__ void coherence_item(CoShared &S, const CoBatch &B, int item) {
   const int tid = threadIdx.x;
   int jb = 0;
@@ -177,7 +190,7 @@ __device__ __forceinline__ void coherence_item(CoShared &S, const CoBatch &B, in
 #pragma unroll
       for (int j = 0; j < NQ; j++) q[j] = p[CO_GR + j];
       __syncthreads();
-      coh_horizontal(S, J, tid, rg, gr, c0, cN, win_rg, dx);
+      coh_horizontal<WRG>(S, J, tid, rg, gr, c0, cN, win_rg, dx);
       __syncthreads();
     }
   } else {
@@ -210,13 +223,13 @@ __device__ __forceinline__ void coherence_item(CoShared &S, const CoBatch &B, in
         S.judge[k][pad8(tid)] = judge[k];
       }
       __syncthreads();
-      coh_horizontal(S, J, tid, rg, gr, c0, cN, win_rg, dx);
+      coh_horizontal<WRG>(S, J, tid, rg, gr, c0, cN, win_rg, dx);
       __syncthreads();
     }
   }
 }
 
-template <int WAZ>
+template <int WAZ, int WRG>
 __global__ void __launch_bounds__(CO_NT, 3) coherence_kernel(const __grid_constant__ CoBatch B) {
   __shared__ CoShared S;
   // one work item per CTA, or (persistent) items from the queue until it
@@ -229,7 +242,7 @@ __global__ void __launch_bounds__(CO_NT, 3) coherence_kernel(const __grid_consta
     __syncthreads();
   }
   while (item < B.total_items) {
-    coherence_item<WAZ>(S, B, item);
+    coherence_item<WAZ, WRG>(S, B, item);
     if (!B.counter) break;
     if (threadIdx.x == 0) S.next_item = atomicAdd(B.counter, 1);
     __syncthreads();
@@ -238,24 +251,42 @@ __global__ void __launch_bounds__(CO_NT, 3) coherence_kernel(const __grid_consta
   }
 }
 
-template <int WAZ>
+template <int WAZ, int WRG>
 static int launch_coh_t(const CoBatch &B, int grid, cudaStream_t st) {
-  coherence_kernel<WAZ><<<grid, CO_NT, 0, st>>>(B);
+  coherence_kernel<WAZ, WRG><<<grid, CO_NT, 0, st>>>(B);
   TOPS_CUDA_TRY(cudaGetLastError());
   return TOPS_OK;
 }
 
-template <int WAZ>
+template <int WAZ, int WRG>
 static int coh_resident(int dev) {
   static int resident[kMaxDevices] = {};
   if (!resident[dev]) {
     int per_sm = 0, sms = 0;
-    TOPS_CUDA_TRY(
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, coherence_kernel<WAZ>, CO_NT, 0));
+    TOPS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, coherence_kernel<WAZ, WRG>, CO_NT, 0));
     TOPS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     resident[dev] = per_sm * sms;
   }
   return resident[dev];
+}
+
+// The compiled (azimuth, range) windows: the config's 3 x 10 and the
+// reference driver's 6 x 24 (Func.cpp:2583-2584); others run generic code.
+template <int WAZ>
+static int launch_coh_rg(const CoBatch &B, int grid, int resident_only, int dev,
+                         cudaStream_t st) {
+  if (B.win_rg == 10)
+    return resident_only ? coh_resident<WAZ, 10>(dev) : launch_coh_t<WAZ, 10>(B, grid, st);
+  if (B.win_rg == 24)
+    return resident_only ? coh_resident<WAZ, 24>(dev) : launch_coh_t<WAZ, 24>(B, grid, st);
+  return resident_only ? coh_resident<WAZ, 0>(dev) : launch_coh_t<WAZ, 0>(B, grid, st);
+}
+
+static int coh_dispatch(const CoBatch &B, int grid, int resident_only, int dev, cudaStream_t st) {
+  if (B.win_az == 3) return launch_coh_rg<3>(B, grid, resident_only, dev, st);
+  if (B.win_az == 6) return launch_coh_rg<6>(B, grid, resident_only, dev, st);
+  return launch_coh_rg<0>(B, grid, resident_only, dev, st);
 }
 
 int launch_coherence(const CohJob *jobs, int njobs, int win_rg, int win_az, const TileCfg &cfg,
@@ -289,18 +320,11 @@ int launch_coherence(const CohJob *jobs, int njobs, int win_rg, int win_az, cons
     int grid = items;
     if (B.counter) {
       TOPS_CUDA_TRY(cudaMemsetAsync(B.counter, 0, sizeof(int), st));
-      const int res = win_az == 3 ? coh_resident<3>(dev)
-                      : win_az == 6 ? coh_resident<6>(dev) : coh_resident<0>(dev);
+      const int res = coh_dispatch(B, 0, 1, dev, st);
       if (res <= 0) return TOPS_E_CUDA;
       grid = min(items, cfg.grid > 0 ? cfg.grid : res);
     }
-    int s;
-    if (win_az == 3)
-      s = launch_coh_t<3>(B, grid, st);
-    else if (win_az == 6)
-      s = launch_coh_t<6>(B, grid, st);
-    else
-      s = launch_coh_t<0>(B, grid, st);
+    const int s = coh_dispatch(B, grid, 0, dev, st);
     if (s != TOPS_OK) return s;
   }
   return TOPS_OK;

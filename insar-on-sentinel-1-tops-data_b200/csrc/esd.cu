@@ -251,11 +251,15 @@ int launch_esd(const EsdOverlap *ovs, int n_ov, int win_az, int win_rg, float th
   if (win_rg < 1 || win_az < 1 || win_rg > ES_NT - ES_TW + 1) return TOPS_E_INVALID;
   if (esd_scratch_bytes(ovs, n_ov) > scratch_bytes || (!scratch && n_ov > 0) || !shifts)
     return TOPS_E_INVALID;
-  static bool attr_done = false;
-  if (!attr_done) {
+  // the shared-memory opt-in is a per-device function attribute
+  static bool attr_done[kMaxDevices] = {};
+  int dev = 0;
+  TOPS_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return TOPS_E_INVALID;
+  if (!attr_done[dev]) {
     TOPS_CUDA_TRY(cudaFuncSetAttribute(esd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)sizeof(EsShared)));
-    attr_done = true;
+    attr_done[dev] = true;
   }
   double2 *part = static_cast<double2 *>(scratch);
   for (int o0 = 0; o0 < n_ov; o0 += ES_MAXOV) {

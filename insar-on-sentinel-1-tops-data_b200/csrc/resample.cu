@@ -92,7 +92,11 @@ struct __align__(16) RsShared {
   float ring_rho[RS_FR];              // ring_phiref reduced mod 2 pi
   float ring_tc[RS_FR];               // ring_ta - tm (FP32, split mode)
   double rowA_az[RS_SEG], rowB_az[RS_SEG], rowA_rg[RS_SEG], rowB_rg[RS_SEG];
-  double col_phat[RS_TW], col_qaz[RS_TW], col_qrg[RS_TW];
+  // per-column P^ and c5 P^2 terms; a range-pass thread reads its two
+  // columns with one 16-byte load (conflict-free across the warp)
+  alignas(16) double col_phat[RS_TW];
+  alignas(16) double col_qaz[RS_TW];
+  alignas(16) double col_qrg[RS_TW];
   int row_v[RS_GR];                   // 1: shared azimuth pass valid for the row
   int row_L0[RS_GR], row_bL[RS_GR];
   float row_M0[RS_GR], row_P1[RS_GR], row_P2[RS_GR];
@@ -693,17 +697,16 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
         if (ra >= gr) break;
         const bool two = ra + 1 < gr;
         // range keys of the 2 x 2 pixels
+        // (entries beyond cN - 1 hold the last column's terms)
         int p0v[2][2], bpv[2][2];
+        const double2 cph = *reinterpret_cast<const double2 *>(&S.col_phat[dc]);
+        const double2 cq = *reinterpret_cast<const double2 *>(&S.col_qrg[dc]);
 #pragma unroll
         for (int k = 0; k < 2; k++) {
           const int ri = rg - r_begin + ra + k;
           const double A = S.rowA_rg[ri], Bc = S.rowB_rg[ri];
-#pragma unroll
-          for (int c = 0; c < 2; c++) {
-            const int col = min(dc + c, cN - 1);
-            const double x = fma(Bc, S.col_phat[col], A + S.col_qrg[col]);
-            split_pos(x, p0v[k][c], bpv[k][c]);
-          }
+          split_pos(fma(Bc, cph.x, A + cq.x), p0v[k][0], bpv[k][0]);
+          split_pos(fma(Bc, cph.y, A + cq.y), p0v[k][1], bpv[k][1]);
         }
         // Fast pair: both rows with a shared azimuth pass, each row's two
         // pixels interior, adjacent (p0 steps by one) and inside the ring

@@ -39,6 +39,9 @@ struct Slot {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev = nullptr;
   Job *job = nullptr;
+  // pinned staging of the small outputs: a copy into pageable memory would
+  // make the enqueue wait for the whole job
+  double *h_cpm = nullptr, *h_shift = nullptr;
 };
 
 using LutKey = std::tuple<double, double, double>;
@@ -115,7 +118,7 @@ struct tops_server {
                            d.windows)) != TOPS_OK ||
         (r = tops_pair_upload(P, d.master_slc, d.slave_slc, s.stream)) != TOPS_OK ||
         (r = tops_pair_run(P, s.stream)) != TOPS_OK ||
-        (r = tops_pair_download(P, d.reslave, d.reslave_esd, d.coh, d.cpm, d.shifts,
+        (r = tops_pair_download(P, d.reslave, d.reslave_esd, d.coh, s.h_cpm, s.h_shift,
                                 s.stream)) != TOPS_OK) {
       // nothing may still read the plan's memory before it is released
       cudaStreamSynchronize(s.stream);
@@ -148,6 +151,11 @@ struct tops_server {
       }
       double done = j->done.load();
       if (done < 0) done = now();
+      const int nb = j->desc.master.n_bursts;
+      if (e == cudaSuccess && j->desc.cpm)
+        memcpy(j->desc.cpm, s.h_cpm, sizeof(double) * 12 * nb);
+      if (e == cudaSuccess && j->desc.shifts && nb > 1)
+        memcpy(j->desc.shifts, s.h_shift, sizeof(double) * (nb - 1));
       delete j->P;
       j->P = nullptr;
       finish(j, e == cudaSuccess ? TOPS_OK : TOPS_E_CUDA, done);
@@ -168,15 +176,18 @@ struct tops_server {
           break;
         }
       if (!free_slot) break;
+      j->admit = now();
       const int r = launch(j, *free_slot);
-      if (r == TOPS_E_NOMEM) break;   // wait until running jobs release memory
+      if (r == TOPS_E_NOMEM) {   // wait until running jobs release memory
+        j->admit = -1;
+        break;
+      }
       queue.pop_front();
       st.queued--;
       if (r != TOPS_OK) {
         finish(j, r, now());
         continue;
       }
-      j->admit = now();
       free_slot->job = j;
       st.admitted++;
       st.running++;
@@ -209,7 +220,9 @@ int tops_server_create(const tops_server_cfg *cfg, tops_server **out) {
   S->slots.resize(cfg->slots);
   for (Slot &s : S->slots) {
     if (cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming) != cudaSuccess ||
+        cudaMallocHost(&s.h_cpm, sizeof(double) * 12 * TOPS_MAX_BURSTS) != cudaSuccess ||
+        cudaMallocHost(&s.h_shift, sizeof(double) * TOPS_MAX_BURSTS) != cudaSuccess) {
       (void)cudaGetLastError();
       tops_server_destroy(S);
       return TOPS_E_CUDA;
@@ -226,6 +239,8 @@ int tops_server_destroy(tops_server *S) {
   for (Slot &s : S->slots) {
     if (s.stream) cudaStreamDestroy(s.stream);
     if (s.ev) cudaEventDestroy(s.ev);
+    if (s.h_cpm) cudaFreeHost(s.h_cpm);
+    if (s.h_shift) cudaFreeHost(s.h_shift);
   }
   for (auto &kv : S->luts) tops_lut_destroy(kv.second);
   for (DemTile &t : S->dems) cudaFree(t.d);
