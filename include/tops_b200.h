@@ -48,6 +48,8 @@ const char *tops_status_string(int status);
 int tops_last_cuda_error(void);
 /* Library version string. */
 const char *tops_version(void);
+/* Waits for the work enqueued on `stream` (NULL: the legacy stream). */
+int tops_stream_synchronize(void *stream);
 
 /* ============================================ 1. reference-compatible ABI */
 

@@ -80,6 +80,16 @@ int tops_pair_run_graph(tops_pair *p, void *stream);
 int tops_pair_download(tops_pair *p, void *reslave, void *reslave_esd, float *coh, double *cpm,
                        double *shifts, void *stream);
 
+/* Host to host in one call: uploads the SLCs, runs every stage and
+ * downloads the outputs, pipelined per burst -- the copies of one burst
+ * overlap the kernels of the others, and uploads overlap downloads.  Host
+ * buffers as tops_pair_upload / tops_pair_download (pinned memory; pageable
+ * buffers make the copies synchronous).  Everything is enqueued behind
+ * `stream`'s earlier work; synchronise `stream` for the results.  Same
+ * outputs as upload + run + download. */
+int tops_pair_process(tops_pair *p, const void *master, const void *slave, void *reslave,
+                      void *reslave_esd, float *coh, double *cpm, double *shifts, void *stream);
+
 typedef struct {
   void *master, *slave;            /* CInt16, pitch slc_pitch */
   void *reslave, *reslave_esd;     /* complex64, pitch cplx_pitch */

@@ -219,6 +219,11 @@ int tops_last_cuda_error(void) { return g_last_cuda_error; }
 
 const char *tops_version(void) { return "tops_b200 0.1.0 (sm_100a)"; }
 
+int tops_stream_synchronize(void *stream) {
+  TOPS_CUDA_TRY(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+  return TOPS_OK;
+}
+
 int GeoCoreg_warp_cuda(int m_burstIdx, int s_burstIdx, int xmin, int xmax, int ymin, int ymax,
                        double dem_DeltaLat, double dem_DeltaLon, int DemLines, int DemPixels,
                        double *AzCpm, double *RgCpm, double lat0, double lon0, int demnodata,

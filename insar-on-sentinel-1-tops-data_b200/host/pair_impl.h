@@ -47,6 +47,9 @@ struct tops_pair {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
   cudaStream_t capture_stream = nullptr;  // private: the legacy stream cannot be captured
+  // copy streams and per-burst events of the pipelined host-to-host run
+  cudaStream_t s_up = nullptr, s_down = nullptr;
+  std::vector<cudaEvent_t> pev;
   std::vector<void *> allocs;
   int n_launches = 0;
   Arena *arena = nullptr;      // if set, device buffers come from it (no cudaMalloc)
@@ -68,6 +71,9 @@ struct tops_pair {
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     if (graph) cudaGraphDestroy(graph);
     if (capture_stream) cudaStreamDestroy(capture_stream);
+    if (s_up) cudaStreamDestroy(s_up);
+    if (s_down) cudaStreamDestroy(s_down);
+    for (cudaEvent_t e : pev) cudaEventDestroy(e);
     for (void *p : allocs) {
       if (arena)
         arena->release(reinterpret_cast<uintptr_t>(p));

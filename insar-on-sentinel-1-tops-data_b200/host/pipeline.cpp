@@ -572,6 +572,107 @@ int tops_pair_download(tops_pair *P, void *reslave, void *reslave_esd, float *co
   return TOPS_OK;
 }
 
+// Host to host, pipelined per burst.  Three streams: `up` copies the SLCs of
+// burst b, `stream` runs burst b's kernels as soon as its SLCs are on the
+// device, `down` copies burst b's outputs as soon as its coherence is done.
+// The copies of one burst then overlap the kernels of its neighbours and the
+// two PCIe directions run at once; the dependencies between bursts are those
+// of the stages (ESD of overlap b-1 needs the ReSlave of bursts b-1 and b).
+int tops_pair_process(tops_pair *P, const void *master, const void *slave, void *reslave,
+                      void *reslave_esd, float *coh, double *cpm, double *shifts, void *stream) {
+  if (!P || !P->dem_set || !master || !slave) return TOPS_E_INVALID;
+  if (reslave && !P->o.reslave_full) return TOPS_E_INVALID;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int nb = P->nb, L = P->L, W = P->W;
+  const int n_ev = 3 * nb + 2;
+  if (!P->s_up) {
+    P_CUDA(cudaStreamCreateWithFlags(&P->s_up, cudaStreamNonBlocking));
+    P_CUDA(cudaStreamCreateWithFlags(&P->s_down, cudaStreamNonBlocking));
+  }
+  while ((int)P->pev.size() < n_ev) {
+    cudaEvent_t e;
+    P_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    P->pev.push_back(e);
+  }
+  cudaEvent_t ev_start = P->pev[0], ev_end = P->pev[1];
+  cudaEvent_t *ev_up = &P->pev[2], *ev_rs1 = &P->pev[2 + nb], *ev_done = &P->pev[2 + 2 * nb];
+  // earlier work on `stream` may still read the buffers the uploads overwrite
+  P_CUDA(cudaEventRecord(ev_start, st));
+  P_CUDA(cudaStreamWaitEvent(P->s_up, ev_start, 0));
+  P_CUDA(cudaStreamWaitEvent(P->s_down, ev_start, 0));
+  const size_t row = (size_t)W * 4;
+  for (int b = 0; b < nb; b++) {
+    const size_t off = (size_t)b * L;
+    P_CUDA(cudaMemcpy2DAsync(P->d_master + off * P->slc_pitch, P->slc_pitch,
+                             static_cast<const char *>(master) + off * row, row, row, L,
+                             cudaMemcpyHostToDevice, P->s_up));
+    P_CUDA(cudaMemcpy2DAsync(P->d_slave + off * P->slc_pitch, P->slc_pitch,
+                             static_cast<const char *>(slave) + off * row, row, row, L,
+                             cudaMemcpyHostToDevice, P->s_up));
+    P_CUDA(cudaEventRecord(ev_up[b], P->s_up));
+  }
+  int launches = 0;
+  P_TRY(tops_geocoreg(P->geo.data(), nb, P->d_geo_scratch, P->geo_scratch, stream));
+  launches += 2;
+  std::vector<tops_resample_job> rs1, rs2;
+  pair_rs1_jobs(P, rs1);
+  pair_rs2_jobs(P, P->d_shift, rs2);
+  std::vector<tops_esd_overlap> ovs;
+  pair_esd_overlaps(P, ovs);
+  std::vector<tops_coh_job> cj;
+  pair_coh_jobs(P, cj);
+  const size_t crow = (size_t)W * 8, frow = (size_t)W * 4;
+  for (int b = 0; b < nb; b++) {
+    const size_t off = (size_t)b * L;
+    P_CUDA(cudaStreamWaitEvent(st, ev_up[b], 0));
+    // ReSlave jobs reading slave burst b (the whole burst, or its overlap bands)
+    std::vector<tops_resample_job> mine;
+    for (const tops_resample_job &j : rs1)
+      if (j.s_first_line == b * L) mine.push_back(j);
+    if (!mine.empty()) {
+      P_TRY(tops_resample_ex(P->lut, mine.data(), (int)mine.size(), P->o.precision, stream));
+      launches += 1;
+    }
+    if (reslave) {
+      P_CUDA(cudaEventRecord(ev_rs1[b], st));
+      P_CUDA(cudaStreamWaitEvent(P->s_down, ev_rs1[b], 0));
+      P_CUDA(cudaMemcpy2DAsync(static_cast<char *>(reslave) + off * crow, crow,
+                               P->d_reslave + off * P->cplx_pitch, P->cplx_pitch, crow, L,
+                               cudaMemcpyDeviceToHost, P->s_down));
+    }
+    if (b > 0) {
+      P_TRY(tops_esd(&ovs[b - 1], 1, P->o.win_az, P->o.win_rg, P->o.esd_threshold,
+                     P->d_shift + (b - 1), P->d_sums + 2 * (b - 1), P->d_esd_scratch,
+                     P->esd_scratch, stream));
+      launches += 2;
+    }
+    P_TRY(tops_resample_ex(P->lut, &rs2[b], 1, P->o.precision, stream));
+    P_TRY(tops_coherence(&cj[b], 1, P->o.win_rg, P->o.win_az, stream));
+    launches += 2;
+    P_CUDA(cudaEventRecord(ev_done[b], st));
+    P_CUDA(cudaStreamWaitEvent(P->s_down, ev_done[b], 0));
+    if (reslave_esd)
+      P_CUDA(cudaMemcpy2DAsync(static_cast<char *>(reslave_esd) + off * crow, crow,
+                               P->d_res_esd + off * P->cplx_pitch, P->cplx_pitch, crow, L,
+                               cudaMemcpyDeviceToHost, P->s_down));
+    if (coh)
+      P_CUDA(cudaMemcpy2DAsync(reinterpret_cast<char *>(coh) + off * frow, frow,
+                               reinterpret_cast<char *>(P->d_coh) + off * P->coh_pitch,
+                               P->coh_pitch, frow, L, cudaMemcpyDeviceToHost, P->s_down));
+  }
+  if (cpm)
+    P_CUDA(cudaMemcpyAsync(cpm, P->d_cpm, sizeof(double) * 12 * nb, cudaMemcpyDeviceToHost,
+                           P->s_down));
+  if (shifts && nb > 1)
+    P_CUDA(cudaMemcpyAsync(shifts, P->d_shift, sizeof(double) * (nb - 1),
+                           cudaMemcpyDeviceToHost, P->s_down));
+  // `stream` completes when the last copy has landed
+  P_CUDA(cudaEventRecord(ev_end, P->s_down));
+  P_CUDA(cudaStreamWaitEvent(st, ev_end, 0));
+  P->n_launches = launches;
+  return TOPS_OK;
+}
+
 int tops_pair_buffers_get(const tops_pair *P, tops_pair_buffers *b) {
   if (!P || !b) return TOPS_E_INVALID;
   b->master = P->d_master;

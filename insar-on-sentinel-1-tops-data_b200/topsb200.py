@@ -560,6 +560,8 @@ class Tune(C.Structure):
 
 
 _proto("tops_pair_run_per_burst", C.c_int, [_vp, _vp])
+_proto("tops_stream_synchronize", C.c_int, [_vp])
+_proto("tops_pair_process", C.c_int, [_vp, _vp, _vp, _vp, _vp, _fp, _dp, _dp, _vp])
 _proto("tops_batch_create", C.c_int, [C.POINTER(_vp), C.c_int, C.POINTER(_vp)])
 _proto("tops_batch_destroy", C.c_int, [_vp])
 _proto("tops_batch_run", C.c_int, [_vp, _vp])
@@ -636,6 +638,32 @@ class Pair:
                                      ptr(coh, C.c_float), ptr(cpm, C.c_double),
                                      ptr(sh, C.c_double), C.c_void_p(stream)), "tops_pair_download")
         return dict(reslave=rs, reslave_esd=re, coh=coh, cpm=cpm, shifts=sh[:self.nb - 1])
+
+    def process(self, master_slc, slave_slc, out=None, reslave=True, stream=0):
+        """Host to host in one pipelined call (tops_pair_process).  `out`:
+        preallocated outputs (dict as download returns; pinned for
+        overlapped copies), else fresh arrays.  Returns once enqueued when
+        `out` is given; otherwise synchronises and returns the outputs."""
+        fresh = out is None
+        if fresh:
+            n = self.nb * self.L
+            out = dict(reslave=np.zeros((n, self.W), np.complex64) if reslave else None,
+                       reslave_esd=np.zeros((n, self.W), np.complex64),
+                       coh=np.zeros((n, self.W), np.float32), cpm=np.zeros((self.nb, 12)),
+                       shifts=np.zeros(max(self.nb - 1, 1)))
+        g = lambda k: out.get(k) if out.get(k) is not None else None
+        check(lib.tops_pair_process(
+            self._h, C.c_void_p(master_slc.ctypes.data), C.c_void_p(slave_slc.ctypes.data),
+            vptr(g("reslave")) if g("reslave") is not None else None,
+            vptr(g("reslave_esd")) if g("reslave_esd") is not None else None,
+            ptr(g("coh"), C.c_float) if g("coh") is not None else None,
+            ptr(g("cpm"), C.c_double) if g("cpm") is not None else None,
+            ptr(g("shifts"), C.c_double) if g("shifts") is not None else None,
+            C.c_void_p(stream)), "tops_pair_process")
+        if fresh:
+            check(lib.tops_stream_synchronize(C.c_void_p(stream)), "tops_stream_synchronize")
+            out["shifts"] = out["shifts"][:self.nb - 1]
+        return out
 
     def buffers(self) -> PairBuffers:
         b = PairBuffers()

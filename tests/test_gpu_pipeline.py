@@ -114,3 +114,21 @@ def test_pipeline_reference_window(T, O, scene_small):
     """The reference's own 24 x 6 window and per-burst deramp rows."""
     a = run_pair(T, scene_small, win_rg=24, win_az=6, burst0_deramp_rows=0)
     assert a["coh"].mean() > 0.8
+
+
+@pytest.mark.parametrize("reslave_full", [1, 0])
+def test_process_equals_upload_run_download(T, scene_esd, reslave_full):
+    """The pipelined host-to-host call (per-burst copies beside the kernels,
+    per-overlap ESD) gives the batched run's outputs bit for bit, and a
+    second call on the same plan the same again."""
+    S = scene_esd
+    a = run_pair(T, S, reslave_full=reslave_full)
+    o = T.pair_opts(reslave_full=reslave_full)
+    di = S.dem_info
+    P = T.Pair(S.swath[0], S.swath[1], S.dem.shape, o)
+    P.set_dem(S.dem, di.lat0, di.lon0, di.dlat, di.dlon, T.scene_windows(S))
+    for _ in range(2):
+        b = P.process(S.slc[0], S.slc[1], reslave=bool(reslave_full))
+        for k in ("reslave_esd", "coh", "cpm", "shifts") + (("reslave",) if reslave_full else ()):
+            assert np.array_equal(a[k], b[k]), k
+    P.close()
