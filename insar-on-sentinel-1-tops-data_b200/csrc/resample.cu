@@ -107,7 +107,38 @@ struct __align__(16) RsShared {
   double ref_a0, ref_a1, ref_a2;      // deramp quadratic of the reference column
   double tm;                          // centre time of the split-mode coefficients
   int next_item;                      // persistent launch: the item just taken
+  // per-row key statistics of the whole work item, computed once up front:
+  // azimuth line / LUT bin of a row with one key (bin -1: none) and the
+  // slave lines its interior pixels use
+  int ri_L0[RS_SEG], ri_bL[RS_SEG], ri_lmin[RS_SEG], ri_lmax[RS_SEG];
+  // raw slave rows of the next group, copied asynchronously (cp.async)
+  // while the current group computes; each thread reads back only the
+  // elements it copied
+  alignas(16) short2 stage[RS_FR][RS_FW];
+  int pf_lo, pf_hi;                   // rows staged for this group
+  int nx_lo, nx_hi;                   // rows the next group brings
 };
+
+// Asynchronous global -> shared copies of 4 or 8 bytes; src_bytes 0 fills
+// the destination with zeros without reading.
+__device__ __forceinline__ void cp_async_8(void *dst, const void *src, int src_bytes) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src),
+               "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_4(void *dst, const void *src, int src_bytes) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src),
+               "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
 
 // Deramp + demodulation phase (DerampAndResample.cu:151-158), FP64, as the
 // quadratic a2 ta^2 + a1 ta + a0 of the burst-local azimuth time ta:
@@ -395,8 +426,43 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
     S.ref_a1 = q.a1;
     S.ref_a2 = q.a2;
     S.tm = 0.5 * (double)(J.sy0 + J.sy1 - 2 * J.s_first_line) * J.dt;
+    S.nx_lo = 1;   // nothing staged for the first group
+    S.nx_hi = 0;
   }
   __syncthreads();
+
+  // ---- per-row key statistics of the whole item (one thread per row):
+  // along the strip y and x are quadratics in the column, so their ranges
+  // follow from the ends and the vertex.  A row whose strip maps to one
+  // (azimuth line, LUT bin) key, whose azimuth support is interior and whose
+  // range support fits the ring window gets the shared azimuth pass.
+  if (tid < r_end - r_begin) {
+    const int ri = tid;
+    const double p0 = S.col_phat[0], p1 = S.col_phat[cN - 1];
+    double ylo, yhi, xlo, xhi;
+    quad_span(S.rowA_az[ri], S.rowB_az[ri], S.caz[5], p0, p1, ylo, yhi);
+    quad_span(S.rowA_rg[ri], S.rowB_rg[ri], S.crg[5], p0, p1, xlo, xhi);
+    int l0lo, blo, l0hi, bhi, x0lo, xblo, x0hi, xbhi;
+    split_pos(ylo, l0lo, blo);
+    split_pos(yhi, l0hi, bhi);
+    split_pos(xlo, x0lo, xblo);
+    split_pos(xhi, x0hi, xbhi);
+    const bool az_any = !(l0hi < J.sy0 + 5 || l0lo > J.sy1 - 7);
+    const bool rg_any = !(x0hi < J.sx0 + 5 || x0lo > J.sx1 - 7);
+    int lmin = INT32_MAX, lmax = INT32_MIN;
+    if (az_any && rg_any) {
+      lmin = max(l0lo, J.sy0 + 5);
+      lmax = min(l0hi, J.sy1 - 7);
+    }
+    const bool uniform = (l0lo == l0hi) && (blo == bhi);
+    const bool az_in = l0lo >= J.sy0 + 5 && l0hi <= J.sy1 - 7;
+    // the range pass reads ring columns [p0 - 6, p0 + 8] of its pixels
+    const bool win = (x0lo - 6 - S.xw >= 0) && (x0hi + 8 - S.xw < RS_FW);
+    S.ri_L0[ri] = l0lo;
+    S.ri_bL[ri] = (uniform && az_in && rg_any && win) ? blo : -1;
+    S.ri_lmin[ri] = lmin;
+    S.ri_lmax[ri] = lmax;
+  }
 
   // ---- per-thread constants of the ring / azimuth-pass column pair
   const int xr0 = 2 * (tid & 63);            // ring columns xr0, xr0 + 1
@@ -432,57 +498,55 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
   const bool out16 = J.out_al16 != 0;
 
   int loaded_lo = INT32_MIN, loaded_hi = INT32_MIN;  // valid ring rows (uniform)
+  __syncthreads();
 
   for (int rg = r_begin; rg < r_end; rg += RS_GR) {
     const int gr = min(RS_GR, r_end - rg);
-    // ---- [A] row statistics (warp 0: one lane per row), ring-row table
+    // ---- [A] (warp 0) the group's row keys and ring rows; lanes 0..15 take
+    // the rows of this group, lanes 16..31 those of the next group, whose
+    // ring rows are staged during this one
     if (tid < 32) {
-      const int r = lane;
-      int v = 0, lmin = INT32_MAX, lmax = INT32_MIN;
-      int L0 = 0, bL = 0;
-      if (r < gr) {
-        const int ri = rg - r_begin + r;
-        const double p0 = S.col_phat[0], p1 = S.col_phat[cN - 1];
-        double ylo, yhi, xlo, xhi;
-        quad_span(S.rowA_az[ri], S.rowB_az[ri], S.caz[5], p0, p1, ylo, yhi);
-        quad_span(S.rowA_rg[ri], S.rowB_rg[ri], S.crg[5], p0, p1, xlo, xhi);
-        int l0lo, blo, l0hi, bhi, x0lo, xblo, x0hi, xbhi;
-        split_pos(ylo, l0lo, blo);
-        split_pos(yhi, l0hi, bhi);
-        split_pos(xlo, x0lo, xblo);
-        split_pos(xhi, x0hi, xbhi);
-        const bool az_any = !(l0hi < J.sy0 + 5 || l0lo > J.sy1 - 7);
-        const bool rg_any = !(x0hi < J.sx0 + 5 || x0lo > J.sx1 - 7);
-        if (az_any && rg_any) {
-          lmin = max(l0lo, J.sy0 + 5);
-          lmax = min(l0hi, J.sy1 - 7);
-        }
-        const bool uniform = (l0lo == l0hi) && (blo == bhi);
-        const bool az_in = l0lo >= J.sy0 + 5 && l0hi <= J.sy1 - 7;
-        // the range pass reads ring columns [p0 - 6, p0 + 8] of its pixels
-        const bool win = (x0lo - 6 - S.xw >= 0) && (x0hi + 8 - S.xw < RS_FW);
-        v = uniform && az_in && rg_any && win;
-        L0 = l0lo;
-        bL = blo;
+      const int half = lane >> 4, r = lane & 15;
+      const int rgx = rg + half * RS_GR;
+      int v = 0, lmin = INT32_MAX, lmax = INT32_MIN, L0 = 0, bL = 0;
+      if (rgx + r < r_end) {
+        const int ri = rgx - r_begin + r;
+        L0 = S.ri_L0[ri];
+        bL = S.ri_bL[ri];
+        lmin = S.ri_lmin[ri];
+        lmax = S.ri_lmax[ri];
+        v = bL >= 0;
       }
-      const int gmin = __reduce_min_sync(0xffffffffu, lmin);
-      const int gmax = __reduce_max_sync(0xffffffffu, lmax);
-      const bool ring_ok = gmin <= gmax && (gmax - gmin + 12 <= RS_FR);
-      if (!ring_ok) v = 0;
-      if (r < RS_GR) {
-        S.row_v[r] = v;
+      int gmin = lmin, gmax = lmax;
+#pragma unroll
+      for (int o = 8; o > 0; o >>= 1) {   // within each half
+        gmin = min(gmin, __shfl_xor_sync(0xffffffffu, gmin, o));
+        gmax = max(gmax, __shfl_xor_sync(0xffffffffu, gmax, o));
+      }
+      const int cmin = __shfl_sync(0xffffffffu, gmin, 0);
+      const int cmax = __shfl_sync(0xffffffffu, gmax, 0);
+      const int nmin = __shfl_sync(0xffffffffu, gmin, 16);
+      const int nmax = __shfl_sync(0xffffffffu, gmax, 16);
+      const bool cok = cmin <= cmax && (cmax - cmin + 12 <= RS_FR);
+      const bool nok = rg + RS_GR < r_end && nmin <= nmax && (nmax - nmin + 12 <= RS_FR);
+      if (half == 0) {
+        S.row_v[r] = v && cok;
         S.row_L0[r] = L0;
-        S.row_bL[r] = bL;
+        S.row_bL[r] = max(bL, 0);
       }
       if (lane == 0) {
-        S.g_lmin = ring_ok ? gmin : 1;
-        S.g_lmax = ring_ok ? gmax : 0;
+        S.g_lmin = cok ? cmin : 1;
+        S.g_lmax = cok ? cmax : 0;
+        S.pf_lo = S.nx_lo;   // the rows staged for this group
+        S.pf_hi = S.nx_hi;
       }
-      // ring-row table of the rows this group loads (at most RS_FR rows)
-      if (ring_ok) {
-        const int need_lo = gmin - 5, need_hi = gmax + 6;
-        const bool cont = need_lo >= loaded_lo && need_lo <= loaded_hi + 1;
-        const int new_lo = cont ? loaded_hi + 1 : need_lo;
+      // ring-row table of the rows this group brings (at most RS_FR rows),
+      // and the ring state after it
+      int ll = loaded_lo, lh = loaded_hi;
+      if (cok) {
+        const int need_lo = cmin - 5, need_hi = cmax + 6;
+        const bool cont = need_lo >= ll && need_lo <= lh + 1;
+        const int new_lo = cont ? lh + 1 : need_lo;
         const int y = new_lo + lane;
         if (y <= need_hi) {
           const int slot = y & (RS_FR - 1);
@@ -493,6 +557,20 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
           S.ring_rho[slot] = reduce_2pi(phref);
           S.ring_tc[slot] = (float)(ta - tm);
         }
+        if (!cont) ll = need_lo;
+        lh = max(lh, need_hi);
+        ll = max(ll, lh - RS_FR + 1);
+      }
+      if (lane == 0) {
+        int lo = 1, hi = 0;
+        if (nok) {
+          const int need_lo = nmin - 5, need_hi = nmax + 6;
+          const bool cont = need_lo >= ll && need_lo <= lh + 1;
+          lo = cont ? lh + 1 : need_lo;
+          hi = need_hi;
+        }
+        S.nx_lo = lo;
+        S.nx_hi = hi;
       }
     }
     __syncthreads();
@@ -536,39 +614,46 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
         S.row_psif[r] = (float)psi;
       }
     }
+    // Raw slave rows [lo, hi] (at most RS_FR) into the staging rows: this
+    // thread copies its column pair of rows lo + rp + 4u to stage[4u + rp];
+    // zeros outside the slave box.
+    const int rp = tid >> 6;   // row phase
+    auto stage_rows = [&](int lo, int hi) {
+      const int xo = xa0 - J.sx0;
+#pragma unroll 1
+      for (int u = 0; u < RS_FR / 4; u++) {
+        const int y = lo + rp + 4 * u;
+        if (y > hi) break;
+        short2 *dst = &S.stage[4 * u + rp][xr0];
+        const bool yin = y >= J.sy0 && y <= J.sy1;
+        const short2 *row = J.slave + (long)(yin ? y - J.sy0 : 0) * J.slave_pitch;
+        if (yin && xin0 && xin1 && J.slave_al8) {
+          cp_async_8(dst, row + xo, 8);
+        } else {
+          cp_async_4(dst, (yin && xin0) ? row + xo : J.slave, (yin && xin0) ? 4 : 0);
+          cp_async_4(dst + 1, (yin && xin1) ? row + xo + 1 : J.slave, (yin && xin1) ? 4 : 0);
+        }
+      }
+      cp_async_commit();
+    };
+    // this thread's copies for the group (staged during the previous one)
+    cp_async_wait_all();
     if (ring_ok) {
       const int need_lo = glmin - 5, need_hi = glmax + 6;
       const bool cont = need_lo >= loaded_lo && need_lo <= loaded_hi + 1;
       const int new_lo = cont ? loaded_hi + 1 : need_lo;
-      const int rp = tid >> 6;   // row phase: rows new_lo + rp + 4u
-      constexpr int RS_LB = RS_FR / 4;
-      // a group usually brings RS_GR new rows (RS_GR / 4 per thread)
-      const int nu = (need_hi - new_lo - rp + 4) / 4;   // rows of this thread
-      short2 sv0[RS_LB], sv1[RS_LB];
-#pragma unroll
-      for (int u = 0; u < RS_LB; u++) {
-        sv0[u] = make_short2(0, 0);
-        sv1[u] = make_short2(0, 0);
-        const int y = new_lo + rp + 4 * u;
-        if ((u < RS_GR / 4 || u < nu) && y <= need_hi && y >= J.sy0 && y <= J.sy1) {
-          const short2 *row = J.slave + (long)(y - J.sy0) * J.slave_pitch;
-          const int xo = xa0 - J.sx0;
-          if (xin0 && xin1 && J.slave_al8) {
-            const int2 p = *reinterpret_cast<const int2 *>(row + xo);
-            sv0[u] = *reinterpret_cast<const short2 *>(&p.x);
-            sv1[u] = *reinterpret_cast<const short2 *>(&p.y);
-          } else {
-            if (xin0) sv0[u] = row[xo];
-            if (xin1) sv1[u] = row[xo + 1];
-          }
-        }
-        if (u + 1 >= RS_GR / 4 && u + 1 >= nu) break;
+      if (S.pf_lo != new_lo || S.pf_hi != need_hi) {
+        // not staged (first group of the item): copy now and wait
+        stage_rows(new_lo, need_hi);
+        cp_async_wait_all();
       }
-#pragma unroll
-      for (int u = 0; u < RS_LB; u++) {
+      // deramp of the new rows (column pair of this thread) into the ring
+#pragma unroll 1
+      for (int u = 0; u < RS_FR / 4; u++) {
         const int y = new_lo + rp + 4 * u;
         if (y > need_hi) break;
         const int slot = y & (RS_FR - 1);
+        const short2 a = S.stage[4 * u + rp][xr0], b = S.stage[4 * u + rp][xr0 + 1];
         float2 d0 = make_float2(0.f, 0.f), d1 = d0;
         float G0 = 0.f, G1 = 0.f;
         if (y >= J.sy0 && y <= J.sy1) {
@@ -590,15 +675,15 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
           float sn, cs;
           if (xin0) {
             __sincosf(r0, &sn, &cs);
-            d0.x = (float)sv0[u].x * cs - (float)sv0[u].y * sn;
-            d0.y = (float)sv0[u].x * sn + (float)sv0[u].y * cs;
+            d0.x = (float)a.x * cs - (float)a.y * sn;
+            d0.y = (float)a.x * sn + (float)a.y * cs;
           } else {
             G0 = 0.f;
           }
           if (xin1) {
             __sincosf(r1, &sn, &cs);
-            d1.x = (float)sv1[u].x * cs - (float)sv1[u].y * sn;
-            d1.y = (float)sv1[u].x * sn + (float)sv1[u].y * cs;
+            d1.x = (float)b.x * cs - (float)b.y * sn;
+            d1.y = (float)b.x * sn + (float)b.y * cs;
           } else {
             G1 = 0.f;
           }
@@ -610,6 +695,9 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
       loaded_hi = max(loaded_hi, need_hi);
       loaded_lo = max(loaded_lo, loaded_hi - RS_FR + 1);
     }
+    // stage the next group's new rows (the staged values above are consumed:
+    // their ring stores are issued); they land while this group computes
+    if (S.nx_lo <= S.nx_hi) stage_rows(S.nx_lo, S.nx_hi);
     __syncthreads();
 
     // ---- [C] shared azimuth pass: 2 ring columns x 4 rows per thread
