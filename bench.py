@@ -44,6 +44,10 @@ CONFIGS = {
     # one full sub-swath pair
     "subswath": dict(n_bursts=9, lines_per_burst=1500, samples_per_burst=21000,
                      overlap_lines=100, dem_lines=3600, dem_pixels=3600, seed=2),
+    # three bursts of the full width: a profiling case whose inputs exceed L2
+    # but whose device footprint stays near 3 GB
+    "subswath3": dict(n_bursts=3, lines_per_burst=1500, samples_per_burst=21000,
+                      overlap_lines=100, dem_lines=3600, dem_pixels=3600, seed=2),
     # two bursts of a narrow swath (parity scale)
     "small": dict(n_bursts=2, lines_per_burst=1500, samples_per_burst=4096, overlap_lines=100,
                   dem_lines=512, dem_pixels=512, seed=1),
@@ -637,9 +641,10 @@ def main():
     ms_max = float(ms_t.item())
     value = world * nb * 1e3 / ms_max
 
-    # ---- per-kernel timing of the dominant kernel (resample, ESD-corrected
-    # pass: 9 bursts x 1500 x 21000 outputs per launch) on the launch stream
-    rs_ms, rs_launches = kernel_times(T, P, S, opts, sp, torch, stream, args.steps)
+    # ---- per-stage timing (CUDA events between the stages of one eager run,
+    # on the launch stream), averaged over `steps` runs
+    stages = stage_report(T, P, S, windows, sp, args.steps)
+    rs_ms = stages["resample_esd"]["ms"]
 
     # ---- end-to-end through the C ABI with pinned host buffers: the
     # pipelined host-to-host call (copies of one burst beside the kernels of
@@ -685,6 +690,15 @@ def main():
     npx = n * W
     rs_bytes = 12.0 * npx
     achieved = rs_bytes / (rs_ms * 1e-3) / 1e9
+    # HBM ceilings of a pair (stage-boundary bytes at the measured copy
+    # bandwidth): the plain dataflow (two resamples, coherence, ESD) and a
+    # fused one that only reads the SLCs and writes ReSlaveESD and coherence
+    ov_px = stages["esd"]["bytes"] / 24.0
+    plain_bytes = 40.0 * npx + 24.0 * ov_px
+    fused_bytes = 20.0 * npx
+    ceilings = {"plain_dataflow_pairs_per_s": nb * peak * 1e9 / plain_bytes,
+                "fused_pairs_per_s": nb * peak * 1e9 / fused_bytes,
+                "bytes_per_pair_plain": plain_bytes / nb, "bytes_per_pair_fused": fused_bytes / nb}
     traffic = None
     tf = os.path.join(ROOT, "profiles", "resample_traffic.json")
     if os.path.exists(tf):
@@ -715,7 +729,8 @@ def main():
                      "frac": achieved / peak, "traffic": traffic, "kernel": "resample_kernel",
                      "algorithmic_bytes_per_launch": rs_bytes, "launch_ms": rs_ms,
                      "peak_kind": peak_kind},
-        "stages_ms": rs_launches,
+        "stages": stages,
+        "hbm_ceilings": ceilings,
         "clocks": clk.summary(),
         "scene_gen_s": gen_s,
     }
@@ -730,70 +745,33 @@ def main():
         dist.destroy_process_group()
 
 
-def kernel_times(T, P, S, opts, sp, torch, stream, steps):
-    """Average duration of each stage's launches over `steps` eager runs,
-    measured with CUDA events on the launch stream."""
-    import ctypes as C
+def stage_report(T, P, S, windows, sp, steps):
+    """Per-stage device time of the pair (tops_pair_stage_times, averaged
+    over `steps` eager runs), with each stage's algorithmic bytes, achieved
+    GB/s and fraction of the measured HBM copy bandwidth; geocoreg, which is
+    FP64-compute-bound, also as DEM pixels/s."""
     nb, L, W = S.cfg.n_bursts, S.cfg.lines_per_burst, S.cfg.samples_per_burst
-    B = P.buffers()
-    # Rebuild the stage launches of tops_pair_run through the device API so
-    # events can bracket each stage.
-    lut = C.c_void_p()
-    T.check(T.lib.tops_lut_create(T.ptr(S.kaz, C.c_float), T.ptr(S.krg, C.c_float), C.byref(lut)),
-            "lut")
-    d = S.deramp[1]
-    kt = torch.from_numpy(d["kt"][0].copy()).cuda()
-    tref = torch.from_numpy(d["tref"][0].copy()).cuda()
-    fdc = torch.from_numpy(d["dc"][0].copy()).cuda()
-    jobs = (T.ResampleJob * nb)()
-    for b in range(nb):
-        j = jobs[b]
-        j.slave = B.slave + b * L * B.slc_pitch
-        j.slave_pitch = B.slc_pitch
-        j.out = B.reslave_esd + b * L * B.cplx_pitch
-        j.out_pitch = B.cplx_pitch
-        j.kt, j.tref, j.fdc = kt.data_ptr(), tref.data_ptr(), fdc.data_ptr()
-        mb, sb = S.boxes(b)
-        for i in range(4):
-            j.mbox[i] = int(mb[i])
-            j.sbox[i] = int(sb[i])
-        j.cpm_dev = B.cpm + 12 * b * 8
-        j.az_shift_dev = (B.shifts + (b - 1) * 8) if b > 0 else None
-        j.s_first_line = b * L
-        j.dt = S.swath[0].dt
-        j.out_row0 = 0
-        j.out_rows = -1
-    cj = (T.CohJob * nb)()
-    for b in range(nb):
-        c = cj[b]
-        c.master = B.master + b * L * B.slc_pitch
-        c.master_pitch = B.slc_pitch
-        c.slave = B.reslave_esd + b * L * B.cplx_pitch
-        c.slave_pitch = B.cplx_pitch
-        c.coh = B.coh + b * L * B.coh_pitch
-        c.coh_pitch = B.coh_pitch
-        c.lines, c.pixels = L, W
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-    t_rs, t_coh = [], []
-    for i in range(steps + 2):
-        ev[0].record(stream)
-        T.check(T.lib.tops_resample(lut, jobs, nb, C.c_void_p(sp)), "resample")
-        ev[1].record(stream)
-        T.check(T.lib.tops_coherence(cj, nb, WIN_RG, WIN_AZ, C.c_void_p(sp)), "coherence")
-        ev[2].record(stream)
-        stream.synchronize()
-        if i >= 2:
-            t_rs.append(ev[0].elapsed_time(ev[1]))
-            t_coh.append(ev[1].elapsed_time(ev[2]))
-    T.lib.tops_lut_destroy(lut)
-    # restore the pipeline's own outputs
-    T.check(T.lib.tops_pair_run(P._h, C.c_void_p(sp)), "run")
-    stream.synchronize()
-    rs = float(np.mean(t_rs))
-    coh = float(np.mean(t_coh))
+    runs = [P.stage_times(sp) for _ in range(max(steps, 1))]
+    ms = {k: float(np.mean([r[k] for r in runs])) for k in runs[0]}
+    peak, _ = peaks()
     npx = nb * L * W
-    return rs, {"resample_esd_ms": rs, "resample_gbs": 12.0 * npx / rs / 1e6,
-                "coherence_ms": coh, "coherence_gbs": 16.0 * npx / coh / 1e6}
+    m = S.swath[0]
+    T_first = np.array(m.burst_first_line_time[:nb])
+    T_last = np.array(m.burst_last_line_time[:nb])
+    ov = np.floor((T_last[:-1] - T_first[1:]) / m.dt).astype(np.int64) if nb > 1 else []
+    dem_px = sum(int(windows[b].rows) * int(windows[b].cols) for b in range(nb))
+    nbytes = {"geocoreg": 4.0 * dem_px + 96.0 * nb, "resample": 12.0 * npx,
+              "esd": 24.0 * float(np.sum(ov)) * W, "resample_esd": 12.0 * npx,
+              "coherence": 16.0 * npx}
+    out = {}
+    for k, t in ms.items():
+        gbs = nbytes[k] / (t * 1e-3) / 1e9 if t > 0 else None
+        out[k] = {"ms": t, "bytes": nbytes[k], "gbs": gbs,
+                  "frac_hbm": (gbs / peak) if gbs else None}
+    out["geocoreg"]["dem_px"] = dem_px
+    out["geocoreg"]["dem_mpx_per_s"] = dem_px / (ms["geocoreg"] * 1e-3) / 1e6
+    out["geocoreg"]["bound"] = "fp64"
+    return out
 
 
 if __name__ == "__main__":

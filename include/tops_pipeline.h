@@ -71,6 +71,11 @@ int tops_pair_upload(tops_pair *p, const void *master, const void *slave, void *
 /* All stages on the device, enqueued on `stream` without host sync. */
 int tops_pair_run(tops_pair *p, void *stream);
 
+/* The stages of tops_pair_run timed with CUDA events on `stream` (waits
+ * for them): ms[0..4] = geocoreg, ReSlave resample, ESD, ReSlaveESD
+ * resample, coherence. */
+int tops_pair_stage_times(tops_pair *p, void *stream, float *ms);
+
 /* Same, as one CUDA graph (captured on first use, then replayed). */
 int tops_pair_run_graph(tops_pair *p, void *stream);
 

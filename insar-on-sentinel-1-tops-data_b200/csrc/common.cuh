@@ -120,6 +120,8 @@ struct GeoJob {
   double lat0, lon0, dlat, dlon, nodata;
   int xmin, xmax, ymin, ymax;
   double dt[2], first_line_time[2], slr_time[2], range_spacing[2];
+  double inv_dt[2], inv_range_spacing[2];   // reciprocals (host FP64)
+  double inv_yq, inv_xq;                     // 1 / (span / 4) of the master box
   double mid_time[2], azi_init[2];
   int line_offset[2];
   double coef[2][3][8];

@@ -10,15 +10,22 @@
 //   N = (WA)^T A, rhs = (WA)^T {slave line, slave pixel} by cuBLAS and a
 //   Cholesky solve by cuSOLVER (:822-851).
 //
-// B200 design: one fused kernel.  Each thread geocodes DEM pixels (master
-// and slave share the target position) and accumulates the 21 distinct
+// B200 design: one fused kernel.  A block walks tiles of GC_TR DEM rows x
+// GC_NT columns; the sine, cosine and prime-vertical radius of each tile row
+// and the sine and cosine of each column are computed once per tile (the
+// reference computes them per pixel; the values are the same), then each
+// thread geocodes its column's pixels (master and slave share the target
+// position) and accumulates the 21 distinct
 // entries of N and the two right-hand sides (33 FP64 sums) in registers;
 // the block reduces them with warp shuffles in a fixed order and writes one
 // partial per block.  A one-block kernel per burst sums the partials in a
 // fixed order and solves the 6x6 system with the reference's own Cholesky
 // scheme (Func.cpp:959-1013).  No per-pixel buffers touch HBM; results are
 // bit-for-bit reproducible run to run.  Orbit polynomials and their first
-// two derivatives are evaluated with Horner's rule instead of pow().
+// two derivatives are evaluated with Horner's rule instead of pow(), and
+// the Newton step folds the reference's velocity / 10 and acceleration / 100
+// scalings into one division; the root and the stopping rule are the
+// reference's, the rounding of the iterates differs in the last bits.
 #include <cuda_runtime.h>
 
 #include <vector>
@@ -28,6 +35,7 @@
 namespace tops {
 
 constexpr int GC_NT = 256;
+constexpr int GC_TR = 16;   // DEM rows per tile
 constexpr int GC_MAXJOBS = 16;
 constexpr int GC_NSUM = 33;
 constexpr double kEllA = 6378137.0;                              // cuConstants.cuh:5
@@ -39,8 +47,9 @@ struct GcBatch {
   GeoJob jobs[GC_MAXJOBS];
 };
 
-// Position, velocity/10 and acceleration/100 of an orbit polynomial at the
-// normalised time t (getPos/getVelo/getAcc semantics).
+// Position and the first two derivatives with respect to the normalised time
+// t of an orbit polynomial (getPos/getVelo/getAcc, Geocoreg_cuda.cu:123-205,
+// return the derivatives divided by 10 and 100).
 __device__ __forceinline__ void orbit_eval(const double (*c)[8], int n, double t, double p[3],
                                            double v[3], double a[3]) {
 #pragma unroll
@@ -52,8 +61,8 @@ __device__ __forceinline__ void orbit_eval(const double (*c)[8], int n, double t
       pp = fma(pp, t, c[k][i]);
     }
     p[k] = pp;
-    v[k] = vv / 10.0;
-    a[k] = aa / 100.0;
+    v[k] = vv;
+    a[k] = aa;
   }
 }
 
@@ -73,70 +82,89 @@ __device__ void ell2lp(const GeoJob &J, int k, const double T[3], double &line, 
   const int n = J.ncoef[k];
   double P[3], V[3], A[3];
   for (int it = 0; it <= 10; it++) {
-    const double t = (az - J.mid_time[k]) / 10.0;
+    const double t = (az - J.mid_time[k]) * 0.1;
     orbit_eval(c, n, t, P, V, A);
     const double dx = T[0] - P[0], dy = T[1] - P[1], dz = T[2] - P[2];
-    const double sol = -(V[0] * dx + V[1] * dy + V[2] * dz) /
+    // -(V/10 . d) / ((A/100 . d) - |V/10|^2) (SolveNewtonEq, :101-112)
+    const double sol = -10.0 * (V[0] * dx + V[1] * dy + V[2] * dz) /
                        ((A[0] * dx + A[1] * dy + A[2] * dz) - V[0] * V[0] - V[1] * V[1] -
                         V[2] * V[2]);
     az += sol;
     if (fabs(sol) < 1e-010) break;
   }
-  orbit_pos(c, n, (az - J.mid_time[k]) / 10.0, P);
-  line = J.line_offset[k] + (az - J.first_line_time[k]) / J.dt[k];
+  orbit_pos(c, n, (az - J.mid_time[k]) * 0.1, P);
+  line = J.line_offset[k] + (az - J.first_line_time[k]) * J.inv_dt[k];
   const double r = sqrt((T[0] - P[0]) * (T[0] - P[0]) + (T[1] - P[1]) * (T[1] - P[1]) +
                         (T[2] - P[2]) * (T[2] - P[2]));
-  pixel = (r - J.slr_time[k] * kSol) / J.range_spacing[k];
+  pixel = (r - J.slr_time[k] * kSol) * J.inv_range_spacing[k];
 }
 
 __global__ void __launch_bounds__(GC_NT) geocoreg_kernel(const __grid_constant__ GcBatch B,
                                                          double *partials) {
   __shared__ double red[GC_NT / 32][GC_NSUM];
+  __shared__ double row_s[GC_TR], row_c[GC_TR], row_n[GC_TR];
   const int blk = blockIdx.x;
   if (blk >= B.total_blocks) return;
   int jb = 0;
   while (jb + 1 < B.njobs && B.jobs[jb + 1].block_begin <= blk) jb++;
   const GeoJob &J = B.jobs[jb];
   const int lblk = blk - J.block_begin;
-  const long npx = (long)J.lines * J.pixels;
   const double e2 = 1.0 - (kEllB * kEllB / kEllA / kEllA);
   const double d2r = kPi / 180.0;
+  const int tiles_x = (J.pixels + GC_NT - 1) / GC_NT;
+  const int tiles = tiles_x * ((J.lines + GC_TR - 1) / GC_TR);
+  const double ymid = 0.5 * ((double)J.ymin + (double)J.ymax);
+  const double xmid = 0.5 * ((double)J.xmin + (double)J.xmax);
   double acc[GC_NSUM];
 #pragma unroll
   for (int q = 0; q < GC_NSUM; q++) acc[q] = 0.0;
 
-  for (long id = (long)lblk * GC_NT + threadIdx.x; id < npx; id += (long)J.blocks * GC_NT) {
-    const int row = (int)(id / J.pixels), col = (int)(id - (long)row * J.pixels);
-    float h;
-    if (B.dem_is_int)
-      h = (float)reinterpret_cast<const int *>(J.dem)[(long)row * J.dem_pitch + col];
-    else
-      h = J.dem[(long)row * J.dem_pitch + col];
-    if (h == (float)J.nodata) continue;
-    // llh2xyz (Geocoreg_cuda.cu:87-99)
-    double sphi, cphi, slam, clam;
-    sincos((J.lat0 - J.dlat * row) * d2r, &sphi, &cphi);
+  for (int tile = lblk; tile < tiles; tile += J.blocks) {
+    const int row0 = (tile / tiles_x) * GC_TR;
+    const int col = (tile % tiles_x) * GC_NT + threadIdx.x;
+    // llh2xyz (Geocoreg_cuda.cu:87-99): the latitude terms per tile row, the
+    // longitude terms per column
+    __syncthreads();   // the previous tile's row terms are no longer read
+    if (threadIdx.x < GC_TR && row0 + threadIdx.x < J.lines) {
+      double sphi, cphi;
+      sincos((J.lat0 - J.dlat * (row0 + threadIdx.x)) * d2r, &sphi, &cphi);
+      row_s[threadIdx.x] = sphi;
+      row_c[threadIdx.x] = cphi;
+      row_n[threadIdx.x] = kEllA / sqrt(1.0 - e2 * sphi * sphi);
+    }
+    __syncthreads();
+    if (col >= J.pixels) continue;
+    double slam, clam;
     sincos((J.lon0 + J.dlon * col) * d2r, &slam, &clam);
-    const double nph = kEllA / sqrt(1.0 - e2 * sphi * sphi) + h;
-    const double T[3] = {nph * cphi * clam, nph * cphi * slam, (nph - e2 * (nph - h)) * sphi};
-    double ml, mp, sl, sp;
-    ell2lp(J, 0, T, ml, mp);
-    if (!(ml >= J.ymin && ml <= J.ymax && mp >= J.xmin && mp <= J.xmax)) continue;
-    ell2lp(J, 1, T, sl, sp);
-    const double L = (ml - 0.5 * ((double)J.ymin + (double)J.ymax)) /
-                     (0.25 * ((double)J.ymax - (double)J.ymin));
-    const double P = (mp - 0.5 * ((double)J.xmin + (double)J.xmax)) /
-                     (0.25 * ((double)J.xmax - (double)J.xmin));
-    const double a[6] = {1.0, L, P, L * L, L * P, P * P};
-    int q = 0;
+    const int nr = min(GC_TR, J.lines - row0);
+    for (int rr = 0; rr < nr; rr++) {
+      const long off = (long)(row0 + rr) * J.dem_pitch + col;
+      float h;
+      if (B.dem_is_int)
+        h = (float)reinterpret_cast<const int *>(J.dem)[off];
+      else
+        h = J.dem[off];
+      if (h == (float)J.nodata) continue;
+      const double sphi = row_s[rr], cphi = row_c[rr];
+      const double nph = row_n[rr] + h;
+      const double T[3] = {nph * cphi * clam, nph * cphi * slam, (nph - e2 * (nph - h)) * sphi};
+      double ml, mp, sl, sp;
+      ell2lp(J, 0, T, ml, mp);
+      if (!(ml >= J.ymin && ml <= J.ymax && mp >= J.xmin && mp <= J.xmax)) continue;
+      ell2lp(J, 1, T, sl, sp);
+      const double L = (ml - ymid) * J.inv_yq;
+      const double P = (mp - xmid) * J.inv_xq;
+      const double a[6] = {1.0, L, P, L * L, L * P, P * P};
+      int q = 0;
 #pragma unroll
-    for (int i = 0; i < 6; i++)
+      for (int i = 0; i < 6; i++)
 #pragma unroll
-      for (int j = i; j < 6; j++) acc[q++] += a[i] * a[j];
+        for (int j = i; j < 6; j++) acc[q++] += a[i] * a[j];
 #pragma unroll
-    for (int i = 0; i < 6; i++) {
-      acc[21 + i] += a[i] * sl;
-      acc[27 + i] += a[i] * sp;
+      for (int i = 0; i < 6; i++) {
+        acc[21 + i] += a[i] * sl;
+        acc[27 + i] += a[i] * sp;
+      }
     }
   }
   // fixed-order block reduction
@@ -208,12 +236,12 @@ __global__ void geocoreg_solve_kernel(const __grid_constant__ GcBatch B, const d
   *J.status = TOPS_OK;
 }
 
-static int gc_blocks_for(long npx) {
-  // enough blocks to fill the GPU, each thread handling >= 8 pixels
-  long b = (npx + GC_NT * 8 - 1) / (GC_NT * 8);
-  if (b < 1) b = 1;
-  if (b > 4096) b = 4096;
-  return (int)b;
+static int gc_blocks_for(int lines, int pixels) {
+  // one block per tile up to 4096 blocks (a tile is GC_TR rows x GC_NT columns)
+  long t = (long)((pixels + GC_NT - 1) / GC_NT) * ((lines + GC_TR - 1) / GC_TR);
+  if (t < 1) t = 1;
+  if (t > 4096) t = 4096;
+  return (int)t;
 }
 
 int fill_geo_job(const tops_geo_job &u, GeoJob &J) {
@@ -238,8 +266,12 @@ int fill_geo_job(const tops_geo_job &u, GeoJob &J) {
   J.xmax = u.xmax;
   J.ymin = u.ymin;
   J.ymax = u.ymax;
+  J.inv_yq = 1.0 / (0.25 * ((double)u.ymax - (double)u.ymin));
+  J.inv_xq = 1.0 / (0.25 * ((double)u.xmax - (double)u.xmin));
   for (int k = 0; k < 2; k++) {
     J.dt[k] = u.dt[k];
+    J.inv_dt[k] = 1.0 / u.dt[k];
+    J.inv_range_spacing[k] = 1.0 / u.range_spacing[k];
     J.first_line_time[k] = u.first_line_time[k];
     J.slr_time[k] = u.slr_time[k];
     J.range_spacing[k] = u.range_spacing[k];
@@ -252,7 +284,7 @@ int fill_geo_job(const tops_geo_job &u, GeoJob &J) {
   }
   J.cpm = u.cpm_dev;
   J.status = u.status_dev;
-  J.blocks = gc_blocks_for((long)u.dem_lines * u.dem_pixels);
+  J.blocks = gc_blocks_for(u.dem_lines, u.dem_pixels);
   return TOPS_OK;
 }
 

@@ -481,6 +481,56 @@ int tops_pair_run(tops_pair *P, void *stream) {
   return TOPS_OK;
 }
 
+// Stage timing: the launches of tops_pair_run with CUDA events between the
+// stages, then a synchronisation; ms[5] = geocoreg, ReSlave resample, ESD,
+// ReSlaveESD resample, coherence.
+int tops_pair_stage_times(tops_pair *P, void *stream, float *ms) {
+  if (!P || !P->dem_set || !ms) return TOPS_E_INVALID;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int nb = P->nb;
+  cudaEvent_t ev[6];
+  for (int i = 0; i < 6; i++) P_CUDA(cudaEventCreate(&ev[i]));
+  int r = TOPS_OK;
+  std::vector<tops_resample_job> jobs;
+  std::vector<tops_esd_overlap> ovs;
+  std::vector<tops_coh_job> cj;
+  do {
+    if (cudaEventRecord(ev[0], st) != cudaSuccess) { r = TOPS_E_CUDA; break; }
+    if ((r = tops_geocoreg(P->geo.data(), nb, P->d_geo_scratch, P->geo_scratch, stream)) != TOPS_OK)
+      break;
+    cudaEventRecord(ev[1], st);
+    pair_rs1_jobs(P, jobs);
+    if (!jobs.empty() &&
+        (r = tops_resample_ex(P->lut, jobs.data(), (int)jobs.size(), P->o.precision, stream)) !=
+            TOPS_OK)
+      break;
+    cudaEventRecord(ev[2], st);
+    if (nb > 1) {
+      pair_esd_overlaps(P, ovs);
+      if ((r = tops_esd(ovs.data(), nb - 1, P->o.win_az, P->o.win_rg, P->o.esd_threshold,
+                        P->d_shift, P->d_sums, P->d_esd_scratch, P->esd_scratch, stream)) !=
+          TOPS_OK)
+        break;
+    }
+    cudaEventRecord(ev[3], st);
+    jobs.clear();
+    pair_rs2_jobs(P, P->d_shift, jobs);
+    if ((r = tops_resample_ex(P->lut, jobs.data(), nb, P->o.precision, stream)) != TOPS_OK) break;
+    cudaEventRecord(ev[4], st);
+    pair_coh_jobs(P, cj);
+    if ((r = tops_coherence(cj.data(), nb, P->o.win_rg, P->o.win_az, stream)) != TOPS_OK) break;
+    if (cudaEventRecord(ev[5], st) != cudaSuccess || cudaEventSynchronize(ev[5]) != cudaSuccess) {
+      r = TOPS_E_CUDA;
+      break;
+    }
+    for (int i = 0; i < 5; i++)
+      if (cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]) != cudaSuccess) r = TOPS_E_CUDA;
+  } while (0);
+  if (r != TOPS_OK) cudaStreamSynchronize(st);
+  for (int i = 0; i < 6; i++) cudaEventDestroy(ev[i]);
+  return r;
+}
+
 // The per-burst launch loop: every stage launched once per burst (or
 // overlap), as the reference's drivers call their stages; the comparison form
 // for the batched plans.

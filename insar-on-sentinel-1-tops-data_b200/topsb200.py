@@ -561,6 +561,7 @@ class Tune(C.Structure):
 
 _proto("tops_pair_run_per_burst", C.c_int, [_vp, _vp])
 _proto("tops_stream_synchronize", C.c_int, [_vp])
+_proto("tops_pair_stage_times", C.c_int, [_vp, _vp, _fp])
 _proto("tops_pair_process", C.c_int, [_vp, _vp, _vp, _vp, _vp, _fp, _dp, _dp, _vp])
 _proto("tops_batch_create", C.c_int, [C.POINTER(_vp), C.c_int, C.POINTER(_vp)])
 _proto("tops_batch_destroy", C.c_int, [_vp])
@@ -664,6 +665,14 @@ class Pair:
             check(lib.tops_stream_synchronize(C.c_void_p(stream)), "tops_stream_synchronize")
             out["shifts"] = out["shifts"][:self.nb - 1]
         return out
+
+    def stage_times(self, stream=0):
+        """ms of geocoreg, ReSlave resample, ESD, ReSlaveESD resample, coherence."""
+        ms = np.zeros(5, np.float32)
+        check(lib.tops_pair_stage_times(self._h, C.c_void_p(stream), ptr(ms, C.c_float)),
+              "tops_pair_stage_times")
+        return dict(zip(("geocoreg", "resample", "esd", "resample_esd", "coherence"),
+                        map(float, ms)))
 
     def buffers(self) -> PairBuffers:
         b = PairBuffers()
