@@ -55,11 +55,11 @@ __device__ __forceinline__ float4 coh_product(short2 m, float2 s) {
                      mi * s.x - mr * s.y, s.x * s.x + s.y * s.y, mr * mr + mi * mi);
 }
 
+// a += b with packed FP32x2 adds
 __device__ __forceinline__ void add4(float4 &a, const float4 &b) {
-  a.x += b.x;
-  a.y += b.y;
-  a.z += b.z;
-  a.w += b.w;
+  const float2 c = __fadd2_rn(make_float2(a.x, a.y), make_float2(b.x, b.y));
+  const float2 p = __fadd2_rn(make_float2(a.z, a.w), make_float2(b.z, b.w));
+  a = make_float4(c.x, c.y, p.x, p.y);
 }
 
 // Horizontal pass of one group: CO_CPI consecutive outputs per item.  The
@@ -94,13 +94,19 @@ __device__ __forceinline__ void coh_horizontal(const CoShared &S, const CohJob &
       if (u > 0) {
         const float4 a = V[pad8(u - 1 + win_rg)];
         const float4 b = V[pad8(u - 1)];
-        w.x += a.x - b.x;
-        w.y += a.y - b.y;
-        w.z += a.z - b.z;
-        w.w += a.w - b.w;
+        const float2 m1 = make_float2(-1.f, -1.f);
+        const float2 wc = __fadd2_rn(make_float2(w.x, w.y),
+                                     __ffma2_rn(make_float2(b.x, b.y), m1, make_float2(a.x, a.y)));
+        const float2 wp = __fadd2_rn(make_float2(w.z, w.w),
+                                     __ffma2_rn(make_float2(b.z, b.w), m1, make_float2(a.z, a.w)));
+        w = make_float4(wc.x, wc.y, wp.x, wp.y);
       }
+      // |sum m s*| / sqrt(sum |s|^2 sum |m|^2) as num rsqrt(num) rsqrt(p):
+      // two MUFU reciprocal square roots instead of an IEEE square root
+      // (relative error a few 1e-7)
       const float p = w.z * w.w;
-      float g = (p > 0.f) ? sqrtf(w.x * w.x + w.y * w.y) * rsqrtf(p) : 0.f;
+      const float num = fmaf(w.x, w.x, w.y * w.y);
+      float g = (p > 0.f && num > 0.f) ? num * rsqrtf(num) * rsqrtf(p) : 0.f;
       if (Jd[pad8(u + dx)] < 1e-6f) g = 0.f;
       out[u] = g;
     }
