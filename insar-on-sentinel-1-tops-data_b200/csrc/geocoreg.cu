@@ -76,8 +76,25 @@ __device__ __forceinline__ void orbit_pos(const double (*c)[8], int n, double t,
 }
 
 // Zero-Doppler (line, pixel) of target T for image k of job J.
-__device__ void ell2lp(const GeoJob &J, int k, const double T[3], double &line, double &pixel) {
-  double az = J.azi_init[k];
+// 1/x: the hardware's approximate FP64 reciprocal refined by two
+// Newton-Raphson steps r <- r + r (1 - x r) (each doubles the correct bits;
+// a Newton step of the zero-Doppler solve needs no correctly rounded
+// quotient, only its root does not move)
+__device__ __forceinline__ double rcp_nr(double x) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+  double e = fma(-x, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-x, r, 1.0);
+  return fma(r, e, r);
+}
+
+// az: the Newton start on entry (the reference starts every pixel at the
+// burst-centre time; here a thread starts from the solution of the pixel
+// above in its column, which converges to the same root in fewer steps),
+// the zero-Doppler azimuth time on return.
+__device__ void ell2lp(const GeoJob &J, int k, const double T[3], double &az, double &line,
+                       double &pixel) {
   const double (*c)[8] = J.coef[k];
   const int n = J.ncoef[k];
   double P[3], V[3], A[3];
@@ -86,9 +103,9 @@ __device__ void ell2lp(const GeoJob &J, int k, const double T[3], double &line, 
     orbit_eval(c, n, t, P, V, A);
     const double dx = T[0] - P[0], dy = T[1] - P[1], dz = T[2] - P[2];
     // -(V/10 . d) / ((A/100 . d) - |V/10|^2) (SolveNewtonEq, :101-112)
-    const double sol = -10.0 * (V[0] * dx + V[1] * dy + V[2] * dz) /
-                       ((A[0] * dx + A[1] * dy + A[2] * dz) - V[0] * V[0] - V[1] * V[1] -
-                        V[2] * V[2]);
+    const double sol = -10.0 * (V[0] * dx + V[1] * dy + V[2] * dz) *
+                       rcp_nr((A[0] * dx + A[1] * dy + A[2] * dz) - V[0] * V[0] - V[1] * V[1] -
+                              V[2] * V[2]);
     az += sol;
     if (fabs(sol) < 1e-010) break;
   }
@@ -137,6 +154,7 @@ __global__ void __launch_bounds__(GC_NT) geocoreg_kernel(const __grid_constant__
     double slam, clam;
     sincos((J.lon0 + J.dlon * col) * d2r, &slam, &clam);
     const int nr = min(GC_TR, J.lines - row0);
+    double azm = J.azi_init[0], azs = J.azi_init[1];   // Newton starts down the column
     for (int rr = 0; rr < nr; rr++) {
       const long off = (long)(row0 + rr) * J.dem_pitch + col;
       float h;
@@ -149,9 +167,9 @@ __global__ void __launch_bounds__(GC_NT) geocoreg_kernel(const __grid_constant__
       const double nph = row_n[rr] + h;
       const double T[3] = {nph * cphi * clam, nph * cphi * slam, (nph - e2 * (nph - h)) * sphi};
       double ml, mp, sl, sp;
-      ell2lp(J, 0, T, ml, mp);
+      ell2lp(J, 0, T, azm, ml, mp);
       if (!(ml >= J.ymin && ml <= J.ymax && mp >= J.xmin && mp <= J.xmax)) continue;
-      ell2lp(J, 1, T, sl, sp);
+      ell2lp(J, 1, T, azs, sl, sp);
       const double L = (ml - ymid) * J.inv_yq;
       const double P = (mp - xmid) * J.inv_xq;
       const double a[6] = {1.0, L, P, L * L, L * P, P * P};
