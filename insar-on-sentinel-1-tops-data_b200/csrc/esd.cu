@@ -57,13 +57,20 @@ __device__ __forceinline__ float4 prod4(short2 m, float2 s) {
                      mr * mr + mi * mi);
 }
 
+// |sum m s*| / sqrt(sum |s|^2 sum |m|^2) as num rsqrt(num) rsqrt(p): two
+// MUFU reciprocal square roots instead of two IEEE square roots and a
+// division (relative error a few 1e-7)
 __device__ __forceinline__ float gamma_of(float4 w) {
   const float p = w.z * w.w;
-  return (p > 0.f) ? sqrtf(w.x * w.x + w.y * w.y) / sqrtf(p) : 0.f;
+  const float num = fmaf(w.x, w.x, w.y * w.y);
+  return (p > 0.f && num > 0.f) ? num * rsqrtf(num) * rsqrtf(p) : 0.f;
 }
 
-__global__ void __launch_bounds__(ES_NT) esd_kernel(const __grid_constant__ EsBatch B,
-                                                     double2 *partials) {
+// WAZ > 0: the azimuth window height at compile time, so the input rows of a
+// group are loaded together (their latencies overlap); 0: any height.
+template <int WAZ>
+__global__ void __launch_bounds__(ES_NT, 2) esd_kernel(const __grid_constant__ EsBatch B,
+                                                        double2 *partials) {
   extern __shared__ __align__(16) unsigned char es_smem[];
   EsShared &S = *reinterpret_cast<EsShared *>(es_smem);
   const int tid = threadIdx.x;
@@ -74,7 +81,7 @@ __global__ void __launch_bounds__(ES_NT) esd_kernel(const __grid_constant__ EsBa
   const EsdOverlap &O = B.ov[ob];
   const int local = item - O.item_begin;
   const int strip = local % O.strips, seg = local / O.strips;
-  const int win_rg = B.win_rg, win_az = B.win_az;
+  const int win_rg = B.win_rg, win_az = WAZ > 0 ? WAZ : B.win_az;
   const int dw = (win_rg - 1) / 2, dh = (win_az - 1) / 2;
   const int c0 = strip * ES_TW;
   const int cN = min(ES_TW, O.pixels - c0);
@@ -94,8 +101,12 @@ __global__ void __launch_bounds__(ES_NT) esd_kernel(const __grid_constant__ EsBa
       aF[k] = aB[k] = make_float4(0.f, 0.f, 0.f, 0.f);
       cF[k] = cB[k] = make_float2(0.f, 0.f);
     }
-    const int nin = gr + win_az - 1;
-    for (int q = 0; q < nin; q++) {
+    // input rows rg - dh .. rg - dh + nin - 1 (all of them for a full group:
+    // rows past the overlap's end load as zero)
+    const int nin = WAZ > 0 ? ES_GR + WAZ - 1 : gr + win_az - 1;
+#pragma unroll
+    for (int q = 0; q < (WAZ > 0 ? ES_GR + WAZ - 1 : 1 << 20); q++) {
+      if (WAZ == 0 && q >= nin) break;
       const int y = rg - dh + q;
       float4 pF = make_float4(0.f, 0.f, 0.f, 0.f), pB = pF;
       if (xin && y >= 0 && y < O.lines) {
@@ -257,8 +268,9 @@ int launch_esd(const EsdOverlap *ovs, int n_ov, int win_az, int win_rg, float th
   TOPS_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDevices) return TOPS_E_INVALID;
   if (!attr_done[dev]) {
-    TOPS_CUDA_TRY(cudaFuncSetAttribute(esd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)sizeof(EsShared)));
+    for (auto fn : {esd_kernel<3>, esd_kernel<6>, esd_kernel<0>})
+      TOPS_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sizeof(EsShared)));
     attr_done[dev] = true;
   }
   double2 *part = static_cast<double2 *>(scratch);
@@ -276,7 +288,12 @@ int launch_esd(const EsdOverlap *ovs, int n_ov, int win_az, int win_rg, float th
       B.n_ov++;
     }
     B.total_items = items;
-    esd_kernel<<<items, ES_NT, sizeof(EsShared), st>>>(B, part);
+    if (win_az == 3)
+      esd_kernel<3><<<items, ES_NT, sizeof(EsShared), st>>>(B, part);
+    else if (win_az == 6)
+      esd_kernel<6><<<items, ES_NT, sizeof(EsShared), st>>>(B, part);
+    else
+      esd_kernel<0><<<items, ES_NT, sizeof(EsShared), st>>>(B, part);
     TOPS_CUDA_TRY(cudaGetLastError());
     esd_finalize_kernel<<<B.n_ov, 256, 0, st>>>(B, part, shifts, sums, o0);
     TOPS_CUDA_TRY(cudaGetLastError());
