@@ -298,6 +298,25 @@ typedef struct {
   double sv_t[32], sv_x[32], sv_y[32], sv_z[32];
 } tops_swath_info;
 
+/* =========================================================== stitching */
+
+/* Debursting of one sub-swath (Stitch_OneSubswath / getLineIdxInMetaData,
+ * Func.cpp:2766-2933): for every output line, from the first valid line of
+ * burst burst0 to the last valid line of burst burstN at the azimuth
+ * interval, the row of the burst stack (bursts burst0..burstN, lines_per_burst
+ * rows each) it is taken from.  first_valid / last_valid: per-burst valid
+ * line indices (the annotation's firstValidLine / lastValidLine).  line_map
+ * NULL: only *height is returned.  TOPS_E_INVALID where the reference would
+ * stop (a line no burst covers) or a line falls outside the stacked bursts. */
+int tops_stitch_line_map(const tops_swath_info *m, const int *first_valid, const int *last_valid,
+                         int burst0, int burstN, int *line_map, int capacity, int *height);
+
+/* Row gather on the device: dst row i = src row line_map_dev[i] (device
+ * int array), row_bytes per row (a multiple of 4: CInt16, float or complex64
+ * rows), pitches in bytes.  Asynchronous on `stream`. */
+int tops_stitch(const void *src, size_t src_pitch, void *dst, size_t dst_pitch,
+                const int *line_map_dev, int height, size_t row_bytes, void *stream);
+
 /* ============================================================ config */
 
 /* config.txt (reference ReadInput, Func.cpp:7-130): key=value lines.

@@ -561,6 +561,24 @@ class Tune(C.Structure):
 
 _proto("tops_pair_run_per_burst", C.c_int, [_vp, _vp])
 _proto("tops_stream_synchronize", C.c_int, [_vp])
+_proto("tops_stitch_line_map", C.c_int, [C.POINTER(SwathInfo), _ip, _ip, C.c_int, C.c_int, _ip,
+                                         C.c_int, _ip])
+_proto("tops_stitch", C.c_int, [_vp, C.c_size_t, _vp, C.c_size_t, _vp, C.c_int, C.c_size_t, _vp])
+
+
+def stitch_line_map(info: "SwathInfo", first_valid, last_valid, burst0: int, burstN: int):
+    """Rows of the burst stack burst0..burstN that the debursted output lines
+    copy (tops_stitch_line_map); raises TopsError where the reference stops."""
+    fv = np.ascontiguousarray(first_valid, np.int32)
+    lv = np.ascontiguousarray(last_valid, np.int32)
+    h = C.c_int()
+    check(lib.tops_stitch_line_map(C.byref(info), ptr(fv, C.c_int), ptr(lv, C.c_int), burst0,
+                                   burstN, None, 0, C.byref(h)), "tops_stitch_line_map")
+    out = np.zeros(h.value, np.int32)
+    check(lib.tops_stitch_line_map(C.byref(info), ptr(fv, C.c_int), ptr(lv, C.c_int), burst0,
+                                   burstN, ptr(out, C.c_int), h.value, C.byref(h)),
+          "tops_stitch_line_map")
+    return out
 _proto("tops_pair_stage_times", C.c_int, [_vp, _vp, _fp])
 _proto("tops_pair_process", C.c_int, [_vp, _vp, _vp, _vp, _vp, _fp, _dp, _dp, _vp])
 _proto("tops_batch_create", C.c_int, [C.POINTER(_vp), C.c_int, C.POINTER(_vp)])

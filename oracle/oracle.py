@@ -244,6 +244,30 @@ def resample(slave, cpm_az, cpm_rg, az_shift, kaz, krg, s_burst_idx, mbox, sbox,
     return out, cnt
 
 
+_proto("orc_stitch_line_map", C.c_int, [C.c_int, C.c_int, _dp, _dp, C.c_double, C.c_double, _ip,
+                                        _ip, C.c_int, C.c_int, _ip, C.c_int])
+
+
+def stitch_line_map(first_time, last_time, lines_per_burst, dt, first_line_time, first_valid,
+                    last_valid, burst0, burstN):
+    """Rows of the burst stack burst0..burstN copied by each output line
+    (Stitch_OneSubswath, Func.cpp:2822-2933); None where the reference stops."""
+    ft = np.ascontiguousarray(first_time, np.float64)
+    lt = np.ascontiguousarray(last_time, np.float64)
+    fv = np.ascontiguousarray(first_valid, np.int32)
+    lv = np.ascontiguousarray(last_valid, np.int32)
+    nb = len(ft)
+    args = (nb, lines_per_burst, _p(ft, C.c_double), _p(lt, C.c_double), dt, first_line_time,
+            _p(fv, C.c_int), _p(lv, C.c_int), burst0, burstN)
+    h = lib.orc_stitch_line_map(*args, None, 0)
+    if h <= 0:
+        return None
+    out = np.zeros(h, np.int32)
+    if lib.orc_stitch_line_map(*args, _p(out, C.c_int), h) != h:
+        return None
+    return out
+
+
 def coherence(master, slave, win_rg, win_az):
     master = np.ascontiguousarray(master, np.int16)
     slave = np.ascontiguousarray(slave, np.float32)

@@ -9,6 +9,7 @@
 //   func_fns.inc        matTxmat, choles, solvechol, invertchol, Polyfit_Orbit
 //                       (Func.cpp:940-1126), getVelocity (1284-1314),
 //                       computeDC (1828-1865), InKernelInit (2105-2158),
+//                       getLineIdxInMetaData (2766-2820),
 //                       EstOverlapSize, GetSpectralSep (2935-2976)
 //   func_deramp_dc.inc  ComputeDerampPara, per-burst DC polynomials and the
 //                       Doppler centroid rows (Func.cpp:1938-1971)
@@ -56,7 +57,7 @@ struct SubSwathInfo {
   double wavelength = 0;
   double azimuthSteeringRate = 0;
   int firstValidPixel = 0;
-  int numOfBursts = 0, linesPerBurst = 0, samplesPerBurst = 0;
+  int numOfBursts = 0, linesPerBurst = 0, samplesPerBurst = 0, numOfLines = 0;
   double burstFirstLineTime[16] = {};
   double burstLastLineTime[16] = {};
   double *rangeDependDopplerRate = nullptr;
@@ -189,6 +190,22 @@ double ref_spectral_sep(int n_bursts, int samples_per_burst, int lines_per_burst
   sw.azimuthTimeInterval = dt;
   sw.dopplerRate = kt;
   return GetSpectralSep(sw);
+}
+
+// getLineIdxInMetaData of a sub-swath with these burst times
+int ref_line_idx(int n_bursts, int lines_per_burst, const double *first, const double *last,
+                 double dt, int num_lines, double t, int burst0, int burstN) {
+  if (n_bursts < 1 || n_bursts > 16) return -2;
+  SubSwathInfo sw;
+  sw.numOfBursts = n_bursts;
+  sw.linesPerBurst = lines_per_burst;
+  sw.numOfLines = num_lines;
+  sw.azimuthTimeInterval = dt;
+  for (int b = 0; b < n_bursts; b++) {
+    sw.burstFirstLineTime[b] = first[b];
+    sw.burstLastLineTime[b] = last[b];
+  }
+  return getLineIdxInMetaData(sw, t, burst0, burstN);
 }
 
 }  // extern "C"

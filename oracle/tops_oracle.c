@@ -271,6 +271,61 @@ double orc_spectral_sep(int n_bursts, int W, int L, double dt, const double *kt)
 }
 
 /* --------------------------------------------------------------- geocoreg */
+/* ----------------------------------------------------------- stitching */
+/* getLineIdxInMetaData (Func.cpp:2766-2820), line for line */
+static int orc_line_idx(int nb, int L, const double *first, const double *last, double dt,
+                        int num_lines, double target, int b0, int bN) {
+  int sy0 = -1, sy1 = -1, burst_num0 = -1, burst_num1 = -1, k = 0;
+  for (int i = 0; i < nb; i++) {
+    if (target >= first[i] && target < last[i]) {
+      int sy = i * L + (int)(((target - first[i]) / dt) + 0.5);
+      if (k == 0) {
+        sy0 = sy;
+        burst_num0 = i;
+      } else {
+        sy1 = sy;
+        burst_num1 = i;
+        break;
+      }
+      ++k;
+    }
+  }
+  if (sy0 != -1 && sy1 != -1) {
+    if (burst_num1 == b0) return sy1;
+    if (burst_num1 == bN + 1) return sy0;
+    double mid = (last[burst_num0] + first[burst_num1]) / 2.0;
+    if (target > mid) return sy1;
+  }
+  if (target < last[nb - 1] + dt && target >= last[nb - 1]) sy0 = num_lines - 1;
+  return sy0;
+}
+
+/* Stitch_OneSubswath (Func.cpp:2822-2933): the output lines and the gapped-
+ * image row each one reads */
+int orc_stitch_line_map(int n_bursts, int lines_per_burst, const double *first_time,
+                        const double *last_time, double dt, double first_line_time,
+                        const int *first_valid, const int *last_valid, int burst0, int burstN,
+                        int *map, int capacity) {
+  double t_first = first_time[burst0] + first_valid[burst0] * dt;   /* Func.cpp:401 */
+  double t_last = first_time[burstN] + last_valid[burstN] * dt;      /* Func.cpp:403 */
+  int y_min = (int)((t_first - first_line_time) / dt);
+  int y_max = (int)((t_last - first_line_time) / dt);
+  int height = y_max - y_min + 1;
+  if (!map) return height;
+  if (height > capacity) return -1;
+  for (int y = y_min; y <= y_max; y++) {
+    int yy = y - y_min;
+    double line_time = t_first + yy * dt;
+    int idx = orc_line_idx(n_bursts, lines_per_burst, first_time, last_time, dt,
+                           n_bursts * lines_per_burst, line_time, burst0, burstN);
+    if (idx == -1) return -1;
+    idx -= burst0 * lines_per_burst;
+    if (idx < 0 || idx >= (burstN - burst0 + 1) * lines_per_burst) return -1;
+    map[yy] = idx;
+  }
+  return height;
+}
+
 /* cuConstants.cuh:53-56 */
 double orc_normalize_warp(double v, double lo, double hi) {
   return (v - (0.5 * (lo + hi))) / (0.25 * (hi - lo));

@@ -70,6 +70,15 @@ void orc_overlap_size(int n_bursts, const double *first_time, const double *last
 /* Func.cpp:2962-2976 (GetSpectralSep); kt is [n_bursts][W]. */
 double orc_spectral_sep(int n_bursts, int W, int L, double dt, const double *kt);
 
+/* Stitch_OneSubswath + getLineIdxInMetaData (Func.cpp:2766-2933): for each
+ * output line, the row of the burst stack burst0..burstN it copies; returns
+ * the line count, or -1 where the reference stops (no burst covers a line)
+ * or a row falls outside the stack; map may be NULL (count only). */
+int orc_stitch_line_map(int n_bursts, int lines_per_burst, const double *first_time,
+                        const double *last_time, double dt, double first_line_time,
+                        const int *first_valid, const int *last_valid, int burst0, int burstN,
+                        int *map, int capacity);
+
 /* Geometric coregistration of one burst: Geocoreg_cuda.cu:87-323 (llh2xyz,
  * SolveNewtonEq, getPos/getVelo/getAcc, ell2lpGeo), 548-605 (WeighthSet,
  * AMatrixSet), 822-851 (normal equations + Cholesky solve, restated with

@@ -7,6 +7,7 @@ stages, built from the reference sources into oracle/_ref/ by
 stores every input they saw and what they returned:
 
     python tests/golden/make_golden.py host            -> tests/golden/ref_host.npz
+    python tests/golden/make_golden.py stitch          -> tests/golden/ref_stitch.npz
     python tests/golden/make_golden.py stages [--out D] -> D/ref_stages.npz (needs a GPU)
 
 The scene comes from the product's seeded generator (tops_synth_*), but the
@@ -226,6 +227,60 @@ def host(out_path):
     print(f"wrote {out_path}: {len(keep)} arrays")
 
 
+# ---------------------------------------------------------- stitch part
+# Burst timings of the debursting cases: S1 IW-like (2.055 ms lines, 1500
+# lines per burst, a 2.7585 s burst cycle, about 157 overlap lines), with
+# per-burst valid-line margins and sub-ranges of bursts.
+STITCH_CASES = [
+    # n_bursts, dt, cycle, first valid, last valid, burst0, burstN, seed
+    (9, 0.002055, 2.7585, 25, 1474, 0, 8, 1),
+    (9, 0.002055, 2.7585, 25, 1474, 2, 5, 2),
+    (9, 0.002055, 2.7585, 3, 1496, 0, 0, 3),
+    (9, 0.002055, 2.7585, 60, 1440, 8, 8, 4),
+    (4, 0.00205556, 2.7581, 40, 1460, 1, 3, 5),
+    (3, 0.002055, 3.0824, 10, 1489, 0, 2, 6),   # bursts that just touch
+]
+
+
+def stitch(out_path):
+    """Stitch_OneSubswath's line selection (Func.cpp:2822-2873) over the
+    reference's own getLineIdxInMetaData (Func.cpp:2766-2820): yMin, yMax and
+    the line times follow the reference's arithmetic (C int truncation of
+    doubles); each line's row is getLineIdxInMetaData - burst0 * L."""
+    H = _lib("libref_host.so")
+    H.ref_line_idx.restype = C.c_int
+    H.ref_line_idx.argtypes = [C.c_int, C.c_int, _dp, _dp, C.c_double, C.c_int, C.c_double,
+                               C.c_int, C.c_int]
+    out = {}
+    L = 1500
+    for ci, (nb, dt, cycle, fv, lv, b0, bN, seed) in enumerate(STITCH_CASES):
+        rng = np.random.default_rng(seed)
+        t0 = 51234.5 + rng.uniform(0, 1)
+        first = t0 + cycle * np.arange(nb) + rng.uniform(-2e-4, 2e-4, nb)
+        last = first + (L - 1) * dt
+        fvs = np.full(nb, fv, np.int32) + rng.integers(0, 3, nb).astype(np.int32)
+        lvs = np.full(nb, lv, np.int32) - rng.integers(0, 3, nb).astype(np.int32)
+        first_line_time = first[0]
+        t_first = first[b0] + int(fvs[b0]) * dt          # burstFirstValidLineTime (Func.cpp:401)
+        t_last = first[bN] + int(lvs[bN]) * dt           # burstLastValidLineTime (Func.cpp:403)
+        y_min = int((t_first - first_line_time) / dt)    # C truncation (Func.cpp:2834-2835)
+        y_max = int((t_last - first_line_time) / dt)
+        rows = []
+        for y in range(y_min, y_max + 1):
+            t = t_first + (y - y_min) * dt
+            idx = H.ref_line_idx(nb, L, _ptr(first, C.c_double), _ptr(last, C.c_double), dt,
+                                 nb * L, t, b0, bN)
+            rows.append(idx - b0 * L if idx != -1 else -1)
+        out[f"case{ci}_first"] = first
+        out[f"case{ci}_last"] = last
+        out[f"case{ci}_params"] = np.array([nb, L, b0, bN], np.int32)
+        out[f"case{ci}_dt"] = np.array([dt, first_line_time])
+        out[f"case{ci}_valid"] = np.stack([fvs, lvs])
+        out[f"case{ci}_map"] = np.array(rows, np.int32)
+    np.savez_compressed(out_path, **out)
+    print(f"wrote {out_path}: {len(STITCH_CASES)} cases")
+
+
 # ---------------------------------------------------------- stage part
 def _stage_libs():
     R = _lib("libref_resample.so")
@@ -384,12 +439,14 @@ def stages(out_path, host_path):
 
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
-    ap.add_argument("part", choices=("host", "stages"))
+    ap.add_argument("part", choices=("host", "stitch", "stages"))
     ap.add_argument("--out", default=HERE)
     a = ap.parse_args()
     os.makedirs(a.out, exist_ok=True)
     if a.part == "host":
         host(os.path.join(a.out, "ref_host.npz"))
+    elif a.part == "stitch":
+        stitch(os.path.join(a.out, "ref_stitch.npz"))
     else:
         stages(os.path.join(a.out, "ref_stages.npz"), os.path.join(HERE, "ref_host.npz"))
 
