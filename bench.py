@@ -644,6 +644,7 @@ def main():
     # ---- per-stage timing (CUDA events between the stages of one eager run,
     # on the launch stream), averaged over `steps` runs
     stages = stage_report(T, P, S, windows, sp, args.steps)
+    stages.update(stitch_report(T, P, S, torch, stream, args.steps))
     rs_ms = stages["resample_esd"]["ms"]
 
     # ---- end-to-end through the C ABI with pinned host buffers: the
@@ -743,6 +744,44 @@ def main():
     P.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+STITCH_MARGIN = 20   # invalid lines at each burst edge of the synthetic bursts
+
+
+def stitch_report(T, P, S, torch, stream, steps):
+    """Debursting of the pair's coherence and ReSlaveESD (tops_stitch over
+    the line map of bursts 0..n-1, STITCH_MARGIN invalid lines at each burst
+    edge): device time per gather with CUDA events, bytes read + written."""
+    import ctypes as C
+    nb, L, W = S.cfg.n_bursts, S.cfg.lines_per_burst, S.cfg.samples_per_burst
+    fv = np.full(nb, STITCH_MARGIN, np.int32)
+    lv = np.full(nb, L - 1 - STITCH_MARGIN, np.int32)
+    m = T.stitch_line_map(S.swath[0], fv, lv, 0, nb - 1)
+    m_dev = torch.from_numpy(m).cuda()
+    B = P.buffers()
+    peak, _ = peaks()
+    out = {}
+    for name, src, pitch, eb in (("stitch_coh", B.coh, B.coh_pitch, 4),
+                                 ("stitch_reslave_esd", B.reslave_esd, B.cplx_pitch, 8)):
+        dst = torch.empty((len(m), W * eb // 4), dtype=torch.int32, device="cuda")
+        run = lambda: T.check(T.lib.tops_stitch(
+            C.c_void_p(src), pitch, C.c_void_p(dst.data_ptr()), W * eb, C.c_void_p(m_dev.data_ptr()),
+            len(m), W * eb, C.c_void_p(stream.cuda_stream)), "tops_stitch")
+        for _ in range(3):
+            run()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(max(steps, 1)):
+            run()
+        e1.record(stream)
+        stream.synchronize()
+        ms = e0.elapsed_time(e1) / max(steps, 1)
+        nbytes = 2.0 * len(m) * W * eb
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        out[name] = {"ms": ms, "bytes": nbytes, "gbs": gbs, "frac_hbm": gbs / peak,
+                     "lines": int(len(m))}
+    return out
 
 
 def stage_report(T, P, S, windows, sp, steps):
