@@ -50,7 +50,10 @@ def test_stitch_pipeline_outputs(T, scene_esd):
     out = P.download()
     fv, lv = np.full(nb, 7, np.int32), np.full(nb, L - 9, np.int32)
     m = T.stitch_line_map(S.swath[0], fv, lv, 0, nb - 1)
-    assert np.all(np.diff(m) > 0) and m[0] == fv[0] and m[-1] == (nb - 1) * L + lv[-1]
+    # the reference truncates the first and last output line indices
+    # separately (Func.cpp:2834-2835), so the last line may stop one short
+    assert np.all(np.diff(m) > 0) and m[0] == fv[0]
+    assert (nb - 1) * L + lv[-1] - 1 <= m[-1] <= (nb - 1) * L + lv[-1]
     m_dev = torch.from_numpy(m).cuda()
     B = P.buffers()
     for src_ptr, pitch, row_bytes, ref, dtype in (
