@@ -317,6 +317,26 @@ int tops_stitch_line_map(const tops_swath_info *m, const int *first_valid, const
 int tops_stitch(const void *src, size_t src_pitch, void *dst, size_t dst_pitch,
                 const int *line_map_dev, int height, size_t row_bytes, void *stream);
 
+/* ======================================================= TIFF raster I/O */
+
+/* Pixel types of the reference's GeoTIFF files (GDAL GDT_CInt16,
+ * GDT_Float32, GDT_CFloat32: SLCs, coherence, resampled slaves). */
+enum { TOPS_TIFF_CINT16 = 1, TOPS_TIFF_FLOAT32 = 2, TOPS_TIFF_CFLOAT32 = 3 };
+
+/* Writes a single-band, uncompressed, little-endian baseline TIFF
+ * (strips, SampleFormat complex int / IEEE float / complex IEEE float), the
+ * raster layout of the reference's TiffWrite (DataTypes.cpp:545-666) without
+ * GDAL.  rows of `pitch` bytes.  Classic TIFF: the file must stay below
+ * 4 GiB (TOPS_E_INVALID otherwise). */
+int tops_tiff_write(const char *path, int type, int width, int height, const void *data,
+                    size_t pitch);
+
+/* Reads a single-band, uncompressed, strip-organised TIFF of one of the
+ * three pixel types (little- or big-endian file); data NULL: only the type
+ * and size are returned.  Rows are packed (width * pixel bytes). */
+int tops_tiff_read(const char *path, int *type, int *width, int *height, void *data,
+                   size_t capacity);
+
 /* ============================================================ config */
 
 /* config.txt (reference ReadInput, Func.cpp:7-130): key=value lines.
@@ -336,6 +356,9 @@ typedef struct {
   /* serving */
   double hbm_budget_gb, arrival_rate;
   int n_jobs;
+  /* 1: tops_run_config also writes the debursted coherence (the reference's
+   * disabled stitching step, Main.cpp:123-131) */
+  int stitch;
 } tops_config;
 
 /* Parse a config file.  Unknown keys are ignored (as in the reference);

@@ -354,6 +354,7 @@ int tops_config_read(const char *path, tops_config *cfg, int *err_line) {
     else if (key == "hbm_budget_gb") ok = set_dbl(&cfg->hbm_budget_gb);
     else if (key == "arrival_rate") ok = set_dbl(&cfg->arrival_rate);
     else if (key == "n_jobs") ok = set_int(&cfg->n_jobs);
+    else if (key == "stitch") ok = set_int(&cfg->stitch);
     // unknown keys are ignored, as in the reference
     if (!ok) {
       status = TOPS_E_CONFIG;

@@ -175,6 +175,7 @@ class Config(C.Structure):
         ("coh_win_rg", C.c_int), ("coh_win_az", C.c_int), ("npoints", C.c_int),
         ("esd_coh_threshold", C.c_double),
         ("hbm_budget_gb", C.c_double), ("arrival_rate", C.c_double), ("n_jobs", C.c_int),
+        ("stitch", C.c_int),
     ]
 
 
@@ -561,6 +562,35 @@ class Tune(C.Structure):
 
 _proto("tops_pair_run_per_burst", C.c_int, [_vp, _vp])
 _proto("tops_stream_synchronize", C.c_int, [_vp])
+_proto("tops_tiff_write", C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, _vp, C.c_size_t])
+_proto("tops_tiff_read", C.c_int, [C.c_char_p, _ip, _ip, _ip, _vp, C.c_size_t])
+TIFF_TYPES = {1: (np.int16, 2), 2: (np.float32, 1), 3: (np.complex64, 1)}
+
+
+def tiff_write(path: str, a: np.ndarray) -> None:
+    """CInt16 ([h][w][2] int16), float32 or complex64 [h][w] raster."""
+    if a.dtype == np.int16:
+        t = 1
+    elif a.dtype == np.float32:
+        t = 2
+    elif a.dtype == np.complex64:
+        t = 3
+    else:
+        raise TypeError(a.dtype)
+    a = np.ascontiguousarray(a)
+    check(lib.tops_tiff_write(str(path).encode(), t, a.shape[1], a.shape[0],
+                              C.c_void_p(a.ctypes.data), a.strides[0]), "tops_tiff_write")
+
+
+def tiff_read(path: str) -> np.ndarray:
+    t, w, h = C.c_int(), C.c_int(), C.c_int()
+    check(lib.tops_tiff_read(str(path).encode(), C.byref(t), C.byref(w), C.byref(h), None, 0),
+          "tops_tiff_read")
+    dt, comps = TIFF_TYPES[t.value]
+    out = np.zeros((h.value, w.value, comps) if comps > 1 else (h.value, w.value), dt)
+    check(lib.tops_tiff_read(str(path).encode(), C.byref(t), C.byref(w), C.byref(h),
+                             C.c_void_p(out.ctypes.data), out.nbytes), "tops_tiff_read")
+    return out
 _proto("tops_stitch_line_map", C.c_int, [C.POINTER(SwathInfo), _ip, _ip, C.c_int, C.c_int, _ip,
                                          C.c_int, _ip])
 _proto("tops_stitch", C.c_int, [_vp, C.c_size_t, _vp, C.c_size_t, _vp, C.c_int, C.c_size_t, _vp])
