@@ -124,6 +124,26 @@ int tops_plain_pair(const tops_swath_info *master, const tops_swath_info *slave,
  * tops_pair_run. */
 int tops_pair_run_per_burst(tops_pair *p, void *stream);
 
+/* ================================================= config.txt-driven run
+ * The reference's main program (Main.cpp:11-150) on this library: reads
+ * config.txt (tops_config_read: the reference's keys plus the synthetic-scene
+ * keys), and for each sub-swath firstsubswath..lastsubswath processes bursts
+ * burst0..burstN (1-based) with the device-resident plan and writes
+ * <process_dir>/ReSlave-N.tif, ReSlaveESD-N.tif and Coh-N.tif (TIFF rasters,
+ * CFloat32 / Float32) -- plus CohStitch-N.tif, the debursted coherence, when
+ * the config sets stitch=1 (the reference's stitching step is disabled).
+ * Product, orbit and DEM readers are outside this library: each sub-swath's
+ * inputs come from the seeded synthetic generator (sub-swath N: seed +
+ * 1000 (N - 1)).  Returns TOPS_E_CONFIG for a malformed or unsupported
+ * config (npoints other than 12, empty ranges). */
+typedef struct {
+  int subswaths, burst_pairs;   /* processed */
+  double seconds;               /* processing and writing, without scene generation */
+  double shifts[TOPS_MAX_BURSTS];   /* ESD shifts of the last sub-swath */
+} tops_run_stats;
+
+int tops_run_config(const char *config_path, tops_run_stats *stats);
+
 /* ============================================== batched sub-swath pairs
  * Several plans -- e.g. the 3 sub-swaths of a product, whose bursts differ in
  * lines and samples -- processed together: one launch per stage for all

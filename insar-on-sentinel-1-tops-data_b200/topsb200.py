@@ -314,6 +314,21 @@ def swath_deramp_params(info: SwathInfo, orbit_coefs, ncoef: int):
     return {"dc": dc, "fmrate": fm, "tref": tref, "kt": kt}
 
 
+class RunStats(C.Structure):
+    _fields_ = [("subswaths", C.c_int), ("burst_pairs", C.c_int), ("seconds", C.c_double),
+                ("shifts", C.c_double * MAX_BURSTS)]
+
+
+_proto("tops_run_config", C.c_int, [C.c_char_p, C.POINTER(RunStats)])
+
+
+def run_config(path: str) -> RunStats:
+    """The config.txt-driven run (tops_run_config)."""
+    st = RunStats()
+    check(lib.tops_run_config(str(path).encode(), C.byref(st)), f"tops_run_config({path})")
+    return st
+
+
 def read_config(path: str) -> Config:
     cfg = Config()
     check(lib.tops_config_defaults(C.byref(cfg)), "tops_config_defaults")
