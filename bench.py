@@ -109,10 +109,30 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
-def build_scene(T, cfg, rank):
+def rank_config(cfg, rank):
+    """The scene of one rank: replicas only -- every rank processes its own
+    sub-swath pair (same sizes, seed + 1000 rank); nothing is exchanged."""
     c = dict(cfg)
     c["seed"] = c["seed"] + 1000 * rank
-    return T.Scene(**c)
+    return c
+
+
+def build_scene(T, cfg, rank):
+    return T.Scene(**rank_config(cfg, rank))
+
+
+def max_over_ranks(v, dist, world, device):
+    """The slowest rank's value (all ranks take this collective step)."""
+    import torch
+    t = torch.tensor([float(v)], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_value(world, pairs_per_rank, ms_max):
+    """Burst pairs of all ranks per second of the slowest rank."""
+    return world * pairs_per_rank * 1e3 / ms_max
 
 
 class CpuPath:
@@ -635,11 +655,8 @@ def main():
         dist.barrier()
     ms = e0.elapsed_time(e1) / args.steps
     launches_per_step = P.buffers().n_launches   # counted by the runs above
-    ms_t = torch.tensor([ms], device="cuda")
-    if world > 1:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
-    value = world * nb * 1e3 / ms_max
+    ms_max = max_over_ranks(ms, dist, world, "cuda")
+    value = whole_job_value(world, nb, ms_max)
 
     # ---- per-stage timing (CUDA events between the stages of one eager run,
     # on the launch stream), averaged over `steps` runs
@@ -669,10 +686,7 @@ def main():
     e2e_ms = timed(process, args.e2e_steps)
     serial_ms = timed(serial, max(1, args.e2e_steps // 2))
     e2e_step_ms = float(np.mean(e2e_ms))
-    e2e_t = torch.tensor([e2e_step_ms], device="cuda")
-    if world > 1:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-    e2e_value = world * nb * 1e3 / float(e2e_t.item())
+    e2e_value = whole_job_value(world, nb, max_over_ranks(e2e_step_ms, dist, world, "cuda"))
     h2d = 2 * n * W * 4
     d2h = 2 * n * W * 8 + n * W * 4 + 8 * 12 * nb + 8 * (nb - 1)
 
