@@ -6,9 +6,10 @@ stages, built from the reference sources into oracle/_ref/ by
 ``make -C oracle/ref``, run on a small seeded synthetic scene; this script
 stores every input they saw and what they returned:
 
-    python tests/golden/make_golden.py host            -> tests/golden/ref_host.npz
+    python tests/golden/make_golden.py host [--scene 2]   -> tests/golden/ref_host[2].npz
     python tests/golden/make_golden.py stitch          -> tests/golden/ref_stitch.npz
-    python tests/golden/make_golden.py stages [--out D] -> D/ref_stages.npz (needs a GPU)
+    python tests/golden/make_golden.py stages [--scene 2] [--out D]
+                                                   -> D/ref_stages[2].npz (needs a GPU)
 
 The scene comes from the product's seeded generator (tops_synth_*), but the
 fixtures hold the generated arrays themselves, so the tests replay them
@@ -43,12 +44,23 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 REF_DIR = os.path.join(ROOT, "oracle", "_ref")
 sys.path.insert(0, os.path.join(ROOT, "insar-on-sentinel-1-tops-data_b200"))
 
-# 3 bursts of 128 x 256 with 24-line overlaps.  W is a multiple of 16 (the
-# reference's deramp kernel reads its per-column rows in blocks of 16) and
-# W * 8 bytes is a multiple of 256 (its prefix-sum kernels need a pitch of a
-# multiple of 32 complex samples, EstCoh.cu:505-517, EstESD.cu:1027-1031).
-SCENE = dict(n_bursts=3, lines_per_burst=128, samples_per_burst=256, overlap_lines=24,
-             dem_lines=128, dem_pixels=128, seed=23, az_shift_true=0.03)
+# Scene 1: 3 bursts of 128 x 256 with 24-line overlaps.  Scene 2: 4 bursts of
+# 160 x 300 with 30-line overlaps, the opposite misregistration, and a width
+# that is no multiple of 16, 32 or the product's 112-column strips.  Widths
+# like 300 stay inside the reference's buffers: its deramp kernel reads the
+# per-column rows up to the next multiple of 16 (DerampAndResample.cu:138-140)
+# and its prefix sums run over the whole row pitch (EstCoh.cu:502-521,
+# EstESD.cu:1045-1056), both within the padded rows cudaMallocPitch returns,
+# whose pitch the ESD driver checks to be a multiple of 32 complex samples
+# (it returns no shifts otherwise; scene 2 got them).  The overlap line count
+# is rounded up to a multiple of 8 before allocation (EstESD.cu:590, 950).
+SCENES = {
+    "1": dict(n_bursts=3, lines_per_burst=128, samples_per_burst=256, overlap_lines=24,
+              dem_lines=128, dem_pixels=128, seed=23, az_shift_true=0.03),
+    "2": dict(n_bursts=4, lines_per_burst=160, samples_per_burst=300, overlap_lines=30,
+              dem_lines=160, dem_pixels=160, seed=29, az_shift_true=-0.04),
+}
+SCENE = SCENES["1"]
 DEM_MARGIN = 24
 NODATA = -32768
 ESD_THRESHOLD = 0.3
@@ -441,14 +453,18 @@ def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("part", choices=("host", "stitch", "stages"))
     ap.add_argument("--out", default=HERE)
+    ap.add_argument("--scene", default="1", choices=sorted(SCENES))
     a = ap.parse_args()
+    global SCENE
+    SCENE = SCENES[a.scene]
+    sfx = "" if a.scene == "1" else a.scene
     os.makedirs(a.out, exist_ok=True)
     if a.part == "host":
-        host(os.path.join(a.out, "ref_host.npz"))
+        host(os.path.join(a.out, f"ref_host{sfx}.npz"))
     elif a.part == "stitch":
         stitch(os.path.join(a.out, "ref_stitch.npz"))
     else:
-        stages(os.path.join(a.out, "ref_stages.npz"), os.path.join(HERE, "ref_host.npz"))
+        stages(os.path.join(a.out, f"ref_stages{sfx}.npz"), os.path.join(HERE, f"ref_host{sfx}.npz"))
 
 
 if __name__ == "__main__":

@@ -1,7 +1,8 @@
 """Oracle and product host code against the reference's own host precomputes.
 
-tests/golden/ref_host.npz was written by tests/golden/make_golden.py from the
-reference's Func.cpp functions (built into oracle/_ref/ by oracle/ref/):
+tests/golden/ref_host{,2}.npz were written by tests/golden/make_golden.py
+for two seeded scenes from the reference's Func.cpp functions (built into
+oracle/_ref/ by oracle/ref/):
 Polyfit_Orbit (Func.cpp:1050-1126), ComputeDerampPara (1868-2099),
 InKernelInit (2105-2158), EstOverlapSize and GetSpectralSep (2935-2976).
 Both the product's host code and the oracle reproduce every value bit for bit.
@@ -11,9 +12,9 @@ import hashlib
 import numpy as np
 import pytest
 
-from golden_io import load, swath_info
+from golden_io import SCENES, load, swath_info
 
-H = load("ref_host.npz")
+HS = {sfx: load(f"ref_host{sfx}.npz") for sfx in SCENES}
 TAGS = ("m", "s")
 
 
@@ -25,8 +26,10 @@ def _sha(a):
     return hashlib.sha256(np.ascontiguousarray(a, np.float32).tobytes()).hexdigest()
 
 
-@pytest.mark.parametrize("case", range(len(H["lut_params"])))
-def test_lut_bit_identical_to_reference(T, O, case):
+@pytest.mark.parametrize("sfx", SCENES)
+@pytest.mark.parametrize("case", range(len(HS[""]["lut_params"])))
+def test_lut_bit_identical_to_reference(T, O, sfx, case):
+    H = HS[sfx]
     prf, abw, rsr2x = (float(v) for v in H["lut_params"][case])
     want_az, want_rg = H["lut_sha256"][case]
     kaz, krg = T.lut(prf, abw, rsr2x)
@@ -37,8 +40,10 @@ def test_lut_bit_identical_to_reference(T, O, case):
         assert np.array_equal(kaz, H["lut_kaz"]) and np.array_equal(krg, H["lut_krg"])
 
 
+@pytest.mark.parametrize("sfx", SCENES)
 @pytest.mark.parametrize("tag", TAGS)
-def test_polyfit_orbit_matches_reference(T, O, tag):
+def test_polyfit_orbit_matches_reference(T, O, sfx, tag):
+    H = HS[sfx]
     t, x, y, z = H[f"{tag}_sv"]
     want = [H[f"{tag}_c{a}"] for a in "xyz"]
     for got in (T.polyfit_orbit(t, x, y, z), O.polyfit_orbit(t, x, y, z)):
@@ -46,12 +51,14 @@ def test_polyfit_orbit_matches_reference(T, O, tag):
             assert np.array_equal(g, w), (g, w)
 
 
+@pytest.mark.parametrize("sfx", SCENES)
 @pytest.mark.parametrize("tag", TAGS)
 @pytest.mark.parametrize("dc", ["", "_interp"])
-def test_deramp_params_match_reference(T, O, tag, dc):
+def test_deramp_params_match_reference(T, O, sfx, tag, dc):
     """Per-burst DC (copied per burst when the annotation has more estimates
     than bursts, interpolated by computeDC otherwise), FM rate, reference
     time and kt (Func.cpp:1938-2093)."""
+    H = HS[sfx]
     info = swath_info(T, H, tag, "dc_list" + dc)
     coefs = [H[f"{tag}_c{a}"] for a in "xyz"]
     got_p = T.swath_deramp_params(info, coefs, len(coefs[0]))
@@ -62,8 +69,10 @@ def test_deramp_params_match_reference(T, O, tag, dc):
             assert np.array_equal(got[k], want), (k, _rel(got[k], want))
 
 
+@pytest.mark.parametrize("sfx", SCENES)
 @pytest.mark.parametrize("tag", TAGS)
-def test_overlap_and_spectral_sep_match_reference(T, O, tag):
+def test_overlap_and_spectral_sep_match_reference(T, O, sfx, tag):
+    H = HS[sfx]
     first, last = H[f"{tag}_burst_first"], H[f"{tag}_burst_last"]
     dt = float(H[f"{tag}_reals"][0])
     L = int(H[f"{tag}_ints"][1])
