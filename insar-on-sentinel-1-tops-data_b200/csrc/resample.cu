@@ -119,16 +119,17 @@ struct __align__(16) RsShared {
   int nx_lo, nx_hi;                   // rows the next group brings
 };
 
-// Asynchronous global -> shared copies of 4 or 8 bytes; src_bytes 0 fills
-// the destination with zeros without reading.
-__device__ __forceinline__ void cp_async_8(void *dst, const void *src, int src_bytes) {
-  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+// Asynchronous global -> shared copies of 4 or 8 bytes to a shared-window
+// address; src_bytes 0 fills the destination with zeros without reading.
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void cp_async_8s(unsigned d, const void *src, int src_bytes) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src),
                "r"(src_bytes)
                : "memory");
 }
-__device__ __forceinline__ void cp_async_4(void *dst, const void *src, int src_bytes) {
-  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+__device__ __forceinline__ void cp_async_4s(unsigned d, const void *src, int src_bytes) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src),
                "r"(src_bytes)
                : "memory");
@@ -469,6 +470,7 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
   const int xa0 = S.xw + xr0;                // absolute slave columns xa0, xa0 + 1
   const bool xin0 = xa0 >= J.sx0 && xa0 <= J.sx1;
   const bool xin1 = xa0 + 1 >= J.sx0 && xa0 + 1 <= J.sx1;
+  const bool pair8 = xin0 && xin1 && J.slave_al8;   // one 8-byte copy per staged row
   const DerampQuad refq = {S.ref_a0, S.ref_a1, S.ref_a2};
   const double tm = S.tm;
   DerampQuad cq0 = refq, cq1 = refq;
@@ -616,22 +618,34 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
     }
     // Raw slave rows [lo, hi] (at most RS_FR) into the staging rows: this
     // thread copies its column pair of rows lo + rp + 4u to stage[4u + rp];
-    // zeros outside the slave box.
+    // zeros outside the slave box.  The job fields are read once per call;
+    // the source offset and the destination step by 4 rows per copy.
     const int rp = tid >> 6;   // row phase
     auto stage_rows = [&](int lo, int hi) {
-      const int xo = xa0 - J.sx0;
+      hi = min(hi, lo + RS_FR - 1);
+      int y = lo + rp;
+      if (y <= hi) {
+        const short2 *const sl = J.slave;
+        const long pitch = J.slave_pitch;
+        const int sy0 = J.sy0;
+        const unsigned rows_in = (unsigned)(J.sy1 - J.sy0);
+        long off = (long)(y - sy0) * pitch + (xa0 - J.sx0);
+        unsigned dst = smem_u32(&S.stage[rp][xr0]);
+        constexpr unsigned kStep = 4u * RS_FW * sizeof(short2);
+        if (pair8) {
 #pragma unroll 1
-      for (int u = 0; u < RS_FR / 4; u++) {
-        const int y = lo + rp + 4 * u;
-        if (y > hi) break;
-        short2 *dst = &S.stage[4 * u + rp][xr0];
-        const bool yin = y >= J.sy0 && y <= J.sy1;
-        const short2 *row = J.slave + (long)(yin ? y - J.sy0 : 0) * J.slave_pitch;
-        if (yin && xin0 && xin1 && J.slave_al8) {
-          cp_async_8(dst, row + xo, 8);
+          for (; y <= hi; y += 4, off += 4 * pitch, dst += kStep) {
+            const bool yin = (unsigned)(y - sy0) <= rows_in;
+            cp_async_8s(dst, sl + (yin ? off : 0), yin ? 8 : 0);
+          }
         } else {
-          cp_async_4(dst, (yin && xin0) ? row + xo : J.slave, (yin && xin0) ? 4 : 0);
-          cp_async_4(dst + 1, (yin && xin1) ? row + xo + 1 : J.slave, (yin && xin1) ? 4 : 0);
+#pragma unroll 1
+          for (; y <= hi; y += 4, off += 4 * pitch, dst += kStep) {
+            const bool yin = (unsigned)(y - sy0) <= rows_in;
+            const bool i0 = yin && xin0, i1 = yin && xin1;
+            cp_async_4s(dst, sl + (i0 ? off : 0), i0 ? 4 : 0);
+            cp_async_4s(dst + 4, sl + (i1 ? off + 1 : 0), i1 ? 4 : 0);
+          }
         }
       }
       cp_async_commit();
@@ -648,15 +662,17 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
         cp_async_wait_all();
       }
       // deramp of the new rows (column pair of this thread) into the ring
+      const int sy0 = J.sy0;
+      const unsigned rows_in = (unsigned)(J.sy1 - J.sy0);
+      const int last = min(need_hi, new_lo + RS_FR - 1);
 #pragma unroll 1
-      for (int u = 0; u < RS_FR / 4; u++) {
-        const int y = new_lo + rp + 4 * u;
-        if (y > need_hi) break;
+      for (int y = new_lo + rp, u4 = rp; y <= last; y += 4, u4 += 4) {
         const int slot = y & (RS_FR - 1);
-        const short2 a = S.stage[4 * u + rp][xr0], b = S.stage[4 * u + rp][xr0 + 1];
+        const short4 ab = *reinterpret_cast<const short4 *>(&S.stage[u4][xr0]);
+        const short2 a = make_short2(ab.x, ab.y), b = make_short2(ab.z, ab.w);
         float2 d0 = make_float2(0.f, 0.f), d1 = d0;
         float G0 = 0.f, G1 = 0.f;
-        if (y >= J.sy0 && y <= J.sy1) {
+        if ((unsigned)(y - sy0) <= rows_in) {
           float r0, r1;
           if (kSplit) {
             const float tc = S.ring_tc[slot], rho = S.ring_rho[slot];
