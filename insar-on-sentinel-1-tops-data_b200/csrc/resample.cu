@@ -20,7 +20,9 @@
 //       from the two ends and the vertex.  A row whose whole strip maps to one
 //       (azimuth line, LUT bin) key -- in a TOPS pair nearly every row -- gets
 //       one shared azimuth pass.  The same bounds give the slave lines the
-//       group needs.
+//       group needs.  Warp 7, idle in the range pass [D], prepares the next
+//       group's keys, ring-row table and azimuth taps during [D], into the
+//       second of two per-row tables; the other warps never wait for it.
 //   [B] New slave rows are deramped once into a ring of RS_FR rows x RS_FW
 //       columns in shared memory: d (complex) and the FP32 residual
 //       G = phi - phi_ref of the deramp phase against a reference column.
@@ -66,7 +68,7 @@ constexpr int RS_SEG = 256;  // output rows per work item
 constexpr int RS_MAXJOBS = 32;
 constexpr int RS_DP = RS_TW / 2;   // column pairs of the range pass
 constexpr int RS_DT = RS_DP * 4;   // range-pass threads (4 row quarters of 4 rows)
-static_assert(RS_DT <= RS_NT, "range pass needs RS_DT threads");
+static_assert(RS_DT == RS_NT - 32, "warp 7 prepares the next group during the range pass");
 static_assert(RS_GR == 16 && RS_FW == 128 && RS_NT == 256 && RS_FR == 32,
               "the thread mappings assume these sizes");
 
@@ -79,6 +81,12 @@ struct RsBatch {
   int total_items;
   int *counter;            // persistent launch: work-item queue (else null)
   ResampleJob jobs[RS_MAXJOBS];
+};
+
+struct RsRows {
+  int v[RS_GR];                       // 1: shared azimuth pass valid for the row
+  int L0[RS_GR], bL[RS_GR];           // its azimuth line and LUT bin
+  float rho[RS_GR], psif[RS_GR];      // row phase Psi reduced mod 2 pi, and as float
 };
 
 struct __align__(16) RsShared {
@@ -97,10 +105,10 @@ struct __align__(16) RsShared {
   alignas(16) double col_phat[RS_TW];
   alignas(16) double col_qaz[RS_TW];
   alignas(16) double col_qrg[RS_TW];
-  int row_v[RS_GR];                   // 1: shared azimuth pass valid for the row
-  int row_L0[RS_GR], row_bL[RS_GR];
+  // per-row tables of a group; the range pass of one group reads one copy
+  // while warp 7 prepares the other for the next group
+  RsRows rows[2];
   float row_M0[RS_GR], row_P1[RS_GR], row_P2[RS_GR];
-  float row_rho[RS_GR], row_psif[RS_GR];
   int g_lmin, g_lmax;                 // slave lines the group's interior pixels use
   double caz[6], crg[6], shift;
   int xw;                             // absolute slave column of ring column 0
@@ -241,8 +249,8 @@ __device__ float2 interior_from_global(const ResampleJob &J, const RsLut &lut, i
 }
 
 // ---------------------------------------------------- ring per-pixel path
-__device__ float2 interior_from_ring(const RsShared &S, const RsLut &lut, int L0, int bL, int P0,
-                                     int bP) {
+__device__ float2 interior_from_ring(const RsShared &S, const RsLut &lut, const ResampleJob &J,
+                                     const DerampQuad &refq, int L0, int bL, int P0, int bP) {
   const float *kl = lut.kaz + bL * kTaps;
   const float *kp = lut.krg + bP * kTaps;
   float kpr[kTaps];
@@ -266,7 +274,9 @@ __device__ float2 interior_from_ring(const RsShared &S, const RsLut &lut, int L0
     sre = fmaf(w, tre, sre);
     sim = fmaf(w, tim, sim);
     sg = fmaf(w, tg, sg);
-    psi = fma((double)w, S.ring_phiref[slot], psi);
+    // the reference-column phase of the line, as the ring-row table holds it
+    const double phref = quad_eval(refq, (double)(L0 - 5 + j - J.s_first_line) * J.dt);
+    psi = fma((double)w, phref, psi);
   }
   float phi = reduce_2pi(psi) + __ldg(lut.sp1 + bP) * (float)psi + sg;
   return cmul_conj_phase(make_float2(sre, sim), phi);
@@ -296,7 +306,8 @@ __device__ __forceinline__ float2 wtap(const ColW &cw, int i) {
 
 // One interior pixel of a row with a shared azimuth pass: 12-tap range pass
 // over vd / vg of the row (single column).
-__device__ __forceinline__ float2 range_pixel(const RsShared &S, const ColW &cw, int r, int xb) {
+__device__ __forceinline__ float2 range_pixel(const RsShared &S, const RsRows &R, const ColW &cw,
+                                              int r, int xb) {
   float2 acc = make_float2(0.f, 0.f);
   float sg = 0.f;
   const float *vgrow = reinterpret_cast<const float *>(&S.vgp[r >> 1][0]) + (r & 1);
@@ -306,7 +317,7 @@ __device__ __forceinline__ float2 range_pixel(const RsShared &S, const ColW &cw,
     acc = __ffma2_rn(w, S.vd[r][xb + i], acc);
     sg = fmaf(w.x, vgrow[2 * (xb + i)], sg);
   }
-  const float phi = S.row_rho[r] + cw.sp1 * S.row_psif[r] + sg;
+  const float phi = R.rho[r] + cw.sp1 * R.psif[r] + sg;
   return cmul_conj_phase(acc, phi);
 }
 
@@ -500,16 +511,17 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
   const bool out16 = J.out_al16 != 0;
 
   int loaded_lo = INT32_MIN, loaded_hi = INT32_MIN;  // valid ring rows (uniform)
-  __syncthreads();
-
-  for (int rg = r_begin; rg < r_end; rg += RS_GR) {
-    const int gr = min(RS_GR, r_end - rg);
-    // ---- [A] (warp 0) the group's row keys and ring rows; lanes 0..15 take
-    // the rows of this group, lanes 16..31 those of the next group, whose
-    // ring rows are staged during this one
-    if (tid < 32) {
+  // ---- [A] + row setup of the group starting at row rgp into row table nb,
+  // run by warp 7 (idle in the range pass) one group ahead: the group's row
+  // keys, the ring-row table of the slave lines it brings, the rows the group
+  // after it brings (staged while it computes), and per row the azimuth taps,
+  // their moments and the row phase.  Lanes 0..15 take the rows of group
+  // rgp, lanes 16..31 those of the group after it.
+  auto prep_group = [&](int rgp, int nb) {
+    RsRows &Q = S.rows[nb];
+    {
       const int half = lane >> 4, r = lane & 15;
-      const int rgx = rg + half * RS_GR;
+      const int rgx = rgp + half * RS_GR;
       int v = 0, lmin = INT32_MAX, lmax = INT32_MIN, L0 = 0, bL = 0;
       if (rgx + r < r_end) {
         const int ri = rgx - r_begin + r;
@@ -530,11 +542,11 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
       const int nmin = __shfl_sync(0xffffffffu, gmin, 16);
       const int nmax = __shfl_sync(0xffffffffu, gmax, 16);
       const bool cok = cmin <= cmax && (cmax - cmin + 12 <= RS_FR);
-      const bool nok = rg + RS_GR < r_end && nmin <= nmax && (nmax - nmin + 12 <= RS_FR);
+      const bool nok = rgp + RS_GR < r_end && nmin <= nmax && (nmax - nmin + 12 <= RS_FR);
       if (half == 0) {
-        S.row_v[r] = v && cok;
-        S.row_L0[r] = L0;
-        S.row_bL[r] = max(bL, 0);
+        Q.v[r] = v && cok;
+        Q.L0[r] = L0;
+        Q.bL[r] = max(bL, 0);
       }
       if (lane == 0) {
         S.g_lmin = cok ? cmin : 1;
@@ -575,22 +587,19 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
         S.nx_hi = hi;
       }
     }
-    __syncthreads();
-
-    // ---- [B] per-row azimuth setup (threads 0..127: 8 lanes per row) and
-    // ring loads of the new slave rows (2 columns per thread)
-    const int glmin = S.g_lmin, glmax = S.g_lmax;
-    const bool ring_ok = glmin <= glmax;
-    if (tid < 8 * RS_GR) {
-      // azimuth taps (w, w) pairs, their moments M0..M2 and the row phase
-      // Psi = sum_j kAz[j] phi_ref(L0 - 5 + j): lane j < 6 takes taps 2j, 2j+1
-      const int r = tid >> 3, j = tid & 7;
-      const bool rv = S.row_v[r] != 0;
+    __syncwarp();
+    // azimuth taps (w, w) pairs, their moments M0..M2 and the row phase
+    // Psi = sum_j kAz[j] phi_ref(L0 - 5 + j): 8 lanes per row, 4 rows per
+    // pass; lane j < 6 takes taps 2j, 2j+1
+#pragma unroll 1
+    for (int r = lane >> 3; r < RS_GR; r += 4) {
+      const int j = lane & 7;
+      const bool rv = Q.v[r] != 0;
       float m0 = 0.f, m1 = 0.f, m2 = 0.f;
       double psi = 0.0;
       if (rv && j < kTaps / 2) {
-        const int L0 = S.row_L0[r];
-        const float *kl = lut.kaz + S.row_bL[r] * kTaps + 2 * j;
+        const int L0 = Q.L0[r];
+        const float *kl = lut.kaz + Q.bL[r] * kTaps + 2 * j;
         const float w0 = __ldg(kl), w1 = __ldg(kl + 1);
         S.wpair[r][j] = make_float4(w0, w0, w1, w1);
         const float u0 = (float)(2 * j - 5), u1 = (float)(2 * j - 4);
@@ -608,14 +617,26 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
         psi += __shfl_xor_sync(0xffffffffu, psi, o);
       }
       if (rv && j == 0) {
-        const double tc = (double)(S.row_L0[r] - J.s_first_line) * J.dt - tm;
+        const double tc = (double)(Q.L0[r] - J.s_first_line) * J.dt - tm;
         S.row_M0[r] = m0;
         S.row_P1[r] = (float)(2.0 * tc * J.dt * m1 + J.dt * J.dt * m2);
         S.row_P2[r] = (float)(J.dt * m1);
-        S.row_rho[r] = reduce_2pi(psi);
-        S.row_psif[r] = (float)psi;
+        Q.rho[r] = reduce_2pi(psi);
+        Q.psif[r] = (float)psi;
       }
     }
+  };
+  __syncthreads();
+  if (tid >= RS_DT) prep_group(r_begin, 0);
+  __syncthreads();
+
+  int buf = 0;   // row table of the current group
+  for (int rg = r_begin; rg < r_end; rg += RS_GR, buf ^= 1) {
+    const int gr = min(RS_GR, r_end - rg);
+    const RsRows &R = S.rows[buf];
+    // ---- [B] ring loads of the new slave rows (2 columns per thread)
+    const int glmin = S.g_lmin, glmax = S.g_lmax;
+    const bool ring_ok = glmin <= glmax;
     // Raw slave rows [lo, hi] (at most RS_FR) into the staging rows: this
     // thread copies its column pair of rows lo + rp + 4u to stage[4u + rp];
     // zeros outside the slave box.  The job fields are read once per call;
@@ -721,12 +742,12 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
       const int q = tid >> 6;      // rows 4q .. 4q+3
       const int r0 = 4 * q;
       if (r0 < gr) {
-        const int L00 = S.row_L0[r0];
+        const int L00 = R.L0[r0];
         bool blk = r0 + 4 <= gr;
 #pragma unroll
         for (int k = 0; k < 4; k++) {
           const int r = min(r0 + k, RS_GR - 1);
-          blk = blk && S.row_v[r] && S.row_L0[r] == L00 + k;
+          blk = blk && R.v[r] && R.L0[r] == L00 + k;
         }
         if (blk) {
           float2 a0[4], a1[4];
@@ -768,8 +789,8 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
 #pragma unroll 1
           for (int k = 0; k < 4 && r0 + k < gr; k++) {
             const int r = r0 + k;
-            if (!S.row_v[r]) continue;
-            const int L0 = S.row_L0[r];
+            if (!R.v[r]) continue;
+            const int L0 = R.L0[r];
             float2 a0 = make_float2(0.f, 0.f), a1 = a0;
 #pragma unroll
             for (int j = 0; j < kTaps; j++) {
@@ -817,7 +838,7 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
         // window.  A column's range key may change between the two rows
         // (about once per 100 rows); its weights are then reloaded for the
         // second row and its phase residual is interpolated per row.
-        bool fast = two && dval1 && out16 && S.row_v[ra] && S.row_v[ra + 1];
+        bool fast = two && dval1 && out16 && R.v[ra] && R.v[ra + 1];
 #pragma unroll
         for (int k = 0; k < 2; k++) {
           const int xbk = p0v[k][0] - 5 - S.xw;
@@ -862,7 +883,7 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
 #pragma unroll
           for (int k = 0; k < 2; k++) {
             const int r = ra + k;
-            const float rho = S.row_rho[r], psif = S.row_psif[r];
+            const float rho = R.rho[r], psif = R.psif[r];
             // sp1 of the column's row-k bin (cw holds row 1's weights now)
             const float sp0 = (k == 0 && !same) ? __ldg(lut.sp1 + bpv[0][0]) : cw0.sp1;
             const float sp1 = (k == 0 && !same) ? __ldg(lut.sp1 + bpv[0][1]) : cw1.sp1;
@@ -878,15 +899,15 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
             const int r = ra + k;
             if (r >= gr) break;
             const int ri = rg - r_begin + r;
-            const bool rv = S.row_v[r];
+            const bool rv = R.v[r];
 #pragma unroll 1
             for (int c = 0; c < 2; c++) {
               if (!(c ? dval1 : dval0)) continue;
               const int col = dc + c;
               int l0, bl;
               if (rv) {
-                l0 = S.row_L0[r];
-                bl = S.row_bL[r];
+                l0 = R.L0[r];
+                bl = R.bL[r];
               } else {
                 const double y =
                     fma(S.rowB_az[ri], S.col_phat[col], S.rowA_az[ri] + S.col_qaz[col]);
@@ -906,13 +927,13 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
                 if (rv && in_win) {
                   if (c) {
                     colw_load(cw1, lut, (p0 << 12) | bp);
-                    res = range_pixel(S, cw1, r, xbp);
+                    res = range_pixel(S, R, cw1, r, xbp);
                   } else {
                     colw_load(cw0, lut, (p0 << 12) | bp);
-                    res = range_pixel(S, cw0, r, xbp);
+                    res = range_pixel(S, R, cw0, r, xbp);
                   }
                 } else if (ring_ok && in_win && l0 - 5 >= loaded_lo && l0 + 6 <= loaded_hi) {
-                  res = interior_from_ring(S, lut, l0, bl, p0, bp);
+                  res = interior_from_ring(S, lut, J, refq, l0, bl, p0, bp);
                 } else {
                   res = interior_from_global(J, lut, l0, bl, p0, bp);
                 }
@@ -922,6 +943,8 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
           }
         }
       }
+    } else if (rg + RS_GR < r_end) {
+      prep_group(rg + RS_GR, buf ^ 1);
     }
     __syncthreads();
   }
