@@ -654,7 +654,7 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
         unsigned dst = smem_u32(&S.stage[rp][xr0]);
         constexpr unsigned kStep = 4u * RS_FW * sizeof(short2);
         if (pair8) {
-#pragma unroll 1
+#pragma unroll 4
           for (; y <= hi; y += 4, off += 4 * pitch, dst += kStep) {
             const bool yin = (unsigned)(y - sy0) <= rows_in;
             cp_async_8s(dst, sl + (yin ? off : 0), yin ? 8 : 0);
@@ -686,7 +686,7 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
       const int sy0 = J.sy0;
       const unsigned rows_in = (unsigned)(J.sy1 - J.sy0);
       const int last = min(need_hi, new_lo + RS_FR - 1);
-#pragma unroll 1
+#pragma unroll 2
       for (int y = new_lo + rp, u4 = rp; y <= last; y += 4, u4 += 4) {
         const int slot = y & (RS_FR - 1);
         const short4 ab = *reinterpret_cast<const short4 *>(&S.stage[u4][xr0]);
@@ -816,7 +816,7 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
 
     // ---- [D] range pass, reramp, store: 2 columns x 4 rows per thread
     if (dthread) {
-#pragma unroll 1
+#pragma unroll 2
       for (int h = 0; h < 2; h++) {
         const int ra = 4 * drq + 2 * h;     // rows ra, ra + 1 (ra even)
         if (ra >= gr) break;
