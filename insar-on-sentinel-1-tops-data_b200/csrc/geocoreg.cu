@@ -90,9 +90,9 @@ __device__ __forceinline__ double rcp_nr(double x) {
 }
 
 // az: the Newton start on entry (the reference starts every pixel at the
-// burst-centre time; here a thread starts from the solution of the pixel
-// above in its column, which converges to the same root in fewer steps),
-// the zero-Doppler azimuth time on return.
+// burst-centre time; here a thread starts from the solutions of the pixels
+// above in its column, extrapolated linearly, which converges to the same
+// root in fewer steps), the zero-Doppler azimuth time on return.
 __device__ void ell2lp(const GeoJob &J, int k, const double T[3], double &az, double &line,
                        double &pixel) {
   const double (*c)[8] = J.coef[k];
@@ -155,6 +155,12 @@ __global__ void __launch_bounds__(GC_NT) geocoreg_kernel(const __grid_constant__
     sincos((J.lon0 + J.dlon * col) * d2r, &slam, &clam);
     const int nr = min(GC_TR, J.lines - row0);
     double azm = J.azi_init[0], azs = J.azi_init[1];   // Newton starts down the column
+    // per-row change of each solution between the last two solved rows (0
+    // unless they are adjacent): the next row's start is extrapolated by it,
+    // which leaves a first Newton step near 1e-9 s instead of the per-row
+    // change of the azimuth time, one iteration less per solve
+    double dm = 0.0, ds = 0.0;
+    int lm = -2, ls = -2;   // last row solved for master / slave
     for (int rr = 0; rr < nr; rr++) {
       const long off = (long)(row0 + rr) * J.dem_pitch + col;
       float h;
@@ -167,9 +173,21 @@ __global__ void __launch_bounds__(GC_NT) geocoreg_kernel(const __grid_constant__
       const double nph = row_n[rr] + h;
       const double T[3] = {nph * cphi * clam, nph * cphi * slam, (nph - e2 * (nph - h)) * sphi};
       double ml, mp, sl, sp;
-      ell2lp(J, 0, T, azm, ml, mp);
+      {
+        double a = azm + (lm == rr - 1 ? dm : 0.0);
+        ell2lp(J, 0, T, a, ml, mp);
+        dm = (lm == rr - 1) ? a - azm : 0.0;
+        azm = a;
+        lm = rr;
+      }
       if (!(ml >= J.ymin && ml <= J.ymax && mp >= J.xmin && mp <= J.xmax)) continue;
-      ell2lp(J, 1, T, azs, sl, sp);
+      {
+        double a = azs + (ls == rr - 1 ? ds : 0.0);
+        ell2lp(J, 1, T, a, sl, sp);
+        ds = (ls == rr - 1) ? a - azs : 0.0;
+        azs = a;
+        ls = rr;
+      }
       const double L = (ml - ymid) * J.inv_yq;
       const double P = (mp - xmid) * J.inv_xq;
       const double a[6] = {1.0, L, P, L * L, L * P, P * P};
