@@ -98,18 +98,26 @@ __device__ void ell2lp(const GeoJob &J, int k, const double T[3], double &az, do
   const double (*c)[8] = J.coef[k];
   const int n = J.ncoef[k];
   double P[3], V[3], A[3];
+  double sol = 0.0;
   for (int it = 0; it <= 10; it++) {
     const double t = (az - J.mid_time[k]) * 0.1;
     orbit_eval(c, n, t, P, V, A);
     const double dx = T[0] - P[0], dy = T[1] - P[1], dz = T[2] - P[2];
     // -(V/10 . d) / ((A/100 . d) - |V/10|^2) (SolveNewtonEq, :101-112)
-    const double sol = -10.0 * (V[0] * dx + V[1] * dy + V[2] * dz) *
-                       rcp_nr((A[0] * dx + A[1] * dy + A[2] * dz) - V[0] * V[0] - V[1] * V[1] -
-                              V[2] * V[2]);
+    sol = -10.0 * (V[0] * dx + V[1] * dy + V[2] * dz) *
+          rcp_nr((A[0] * dx + A[1] * dy + A[2] * dz) - V[0] * V[0] - V[1] * V[1] - V[2] * V[2]);
     az += sol;
     if (fabs(sol) < 1e-010) break;
   }
-  orbit_pos(c, n, (az - J.mid_time[k]) * 0.1, P);
+  // position at the final az: from the last evaluation and one Taylor term
+  // when the last step was below the stopping bound (dP/daz = V / 10; the
+  // next term is below 1e-19 m), else evaluated afresh
+  if (fabs(sol) < 1e-010) {
+#pragma unroll
+    for (int q = 0; q < 3; q++) P[q] = fma(0.1 * sol, V[q], P[q]);
+  } else {
+    orbit_pos(c, n, (az - J.mid_time[k]) * 0.1, P);
+  }
   line = J.line_offset[k] + (az - J.first_line_time[k]) * J.inv_dt[k];
   const double r = sqrt((T[0] - P[0]) * (T[0] - P[0]) + (T[1] - P[1]) * (T[1] - P[1]) +
                         (T[2] - P[2]) * (T[2] - P[2]));
