@@ -25,7 +25,11 @@
 // two derivatives are evaluated with Horner's rule instead of pow(), and
 // the Newton step folds the reference's velocity / 10 and acceleration / 100
 // scalings into one division; the root and the stopping rule are the
-// reference's, the rounding of the iterates differs in the last bits.
+// reference's, the rounding of the iterates differs in the last bits.  Down
+// a column, each solve starts from the previous solutions extrapolated
+// linearly, and its first Newton step takes the orbit state there from a
+// Taylor shift of the previous solve's position, velocity and acceleration
+// (kept in shared memory), so most solves need one polynomial evaluation.
 #include <cuda_runtime.h>
 
 #include <vector>
@@ -92,14 +96,38 @@ __device__ __forceinline__ double rcp_nr(double x) {
 // az: the Newton start on entry (the reference starts every pixel at the
 // burst-centre time; here a thread starts from the solutions of the pixels
 // above in its column, extrapolated linearly, which converges to the same
-// root in fewer steps), the zero-Doppler azimuth time on return.
-__device__ void ell2lp(const GeoJob &J, int k, const double T[3], double &az, double &line,
-                       double &pixel) {
+// root in fewer steps), the zero-Doppler azimuth time on return.  st: the
+// orbit position, velocity and acceleration at the last solution of this
+// column (9 doubles at a stride of GC_NT in shared memory), valid when have
+// is set, and delta = start - that solution.  The first Newton step then
+// takes the orbit state at the start from a Taylor shift of st (a few FMAs)
+// instead of a polynomial evaluation; on return st holds this solve's state.
+__device__ void ell2lp(const GeoJob &J, int k, const double T[3], double &az, double delta,
+                       double &line, double &pixel, double *st, bool &have) {
   const double (*c)[8] = J.coef[k];
   const int n = J.ncoef[k];
   double P[3], V[3], A[3];
   double sol = 0.0;
-  for (int it = 0; it <= 10; it++) {
+  int it0 = 0;
+  if (have) {
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      // shift by dt = delta / 10 in normalised time (third-order term: below
+      // 1e-9 m for the millisecond steps between DEM rows)
+      const double dt = 0.1 * delta;
+      const double a = st[(6 + q) * GC_NT], v = st[(3 + q) * GC_NT];
+      P[q] = fma(dt, fma(0.5 * dt, a, v), st[q * GC_NT]);
+      V[q] = fma(dt, a, v);
+      A[q] = a;
+    }
+    const double dx = T[0] - P[0], dy = T[1] - P[1], dz = T[2] - P[2];
+    sol = -10.0 * (V[0] * dx + V[1] * dy + V[2] * dz) *
+          rcp_nr((A[0] * dx + A[1] * dy + A[2] * dz) - V[0] * V[0] - V[1] * V[1] - V[2] * V[2]);
+    az += sol;
+    it0 = 1;   // that step is the solve's first iteration
+  }
+  const bool done = it0 == 1 && fabs(sol) < 1e-010;
+  for (int it = it0; it <= 10 && !done; it++) {
     const double t = (az - J.mid_time[k]) * 0.1;
     orbit_eval(c, n, t, P, V, A);
     const double dx = T[0] - P[0], dy = T[1] - P[1], dz = T[2] - P[2];
@@ -122,12 +150,20 @@ __device__ void ell2lp(const GeoJob &J, int k, const double T[3], double &az, do
   const double r = sqrt((T[0] - P[0]) * (T[0] - P[0]) + (T[1] - P[1]) * (T[1] - P[1]) +
                         (T[2] - P[2]) * (T[2] - P[2]));
   pixel = (r - J.slr_time[k] * kSol) * J.inv_range_spacing[k];
+#pragma unroll
+  for (int q = 0; q < 3; q++) {
+    st[q * GC_NT] = P[q];
+    st[(3 + q) * GC_NT] = V[q];
+    st[(6 + q) * GC_NT] = A[q];
+  }
+  have = true;
 }
 
-__global__ void __launch_bounds__(GC_NT) geocoreg_kernel(const __grid_constant__ GcBatch B,
+__global__ void __launch_bounds__(GC_NT, 2) geocoreg_kernel(const __grid_constant__ GcBatch B,
                                                          double *partials) {
   __shared__ double red[GC_NT / 32][GC_NSUM];
   __shared__ double row_s[GC_TR], row_c[GC_TR], row_n[GC_TR];
+  __shared__ double ostate[2][9][GC_NT];   // last solve's orbit state per thread and image
   const int blk = blockIdx.x;
   if (blk >= B.total_blocks) return;
   int jb = 0;
@@ -163,10 +199,9 @@ __global__ void __launch_bounds__(GC_NT) geocoreg_kernel(const __grid_constant__
     sincos((J.lon0 + J.dlon * col) * d2r, &slam, &clam);
     const int nr = min(GC_TR, J.lines - row0);
     double azm = J.azi_init[0], azs = J.azi_init[1];   // Newton starts down the column
+    bool hm = false, hs = false;   // orbit state of a solve above held (master / slave)
     // per-row change of each solution between the last two solved rows (0
-    // unless they are adjacent): the next row's start is extrapolated by it,
-    // which leaves a first Newton step near 1e-9 s instead of the per-row
-    // change of the azimuth time, one iteration less per solve
+    // unless they are adjacent): the next row's start is extrapolated by it
     double dm = 0.0, ds = 0.0;
     int lm = -2, ls = -2;   // last row solved for master / slave
     for (int rr = 0; rr < nr; rr++) {
@@ -182,16 +217,18 @@ __global__ void __launch_bounds__(GC_NT) geocoreg_kernel(const __grid_constant__
       const double T[3] = {nph * cphi * clam, nph * cphi * slam, (nph - e2 * (nph - h)) * sphi};
       double ml, mp, sl, sp;
       {
-        double a = azm + (lm == rr - 1 ? dm : 0.0);
-        ell2lp(J, 0, T, a, ml, mp);
+        const double d = lm == rr - 1 ? dm : 0.0;
+        double a = azm + d;
+        ell2lp(J, 0, T, a, d, ml, mp, &ostate[0][0][threadIdx.x], hm);
         dm = (lm == rr - 1) ? a - azm : 0.0;
         azm = a;
         lm = rr;
       }
       if (!(ml >= J.ymin && ml <= J.ymax && mp >= J.xmin && mp <= J.xmax)) continue;
       {
-        double a = azs + (ls == rr - 1 ? ds : 0.0);
-        ell2lp(J, 1, T, a, sl, sp);
+        const double d = ls == rr - 1 ? ds : 0.0;
+        double a = azs + d;
+        ell2lp(J, 1, T, a, d, sl, sp, &ostate[1][0][threadIdx.x], hs);
         ds = (ls == rr - 1) ? a - azs : 0.0;
         azs = a;
         ls = rr;
