@@ -39,7 +39,7 @@
 namespace tops {
 
 constexpr int GC_NT = 256;
-constexpr int GC_TR = 16;   // DEM rows per tile
+constexpr int GC_TR = 32;   // DEM rows per tile (each starts its columns' Newton chains afresh)
 constexpr int GC_MAXJOBS = 16;
 constexpr int GC_NSUM = 33;
 constexpr double kEllA = 6378137.0;                              // cuConstants.cuh:5
