@@ -126,8 +126,10 @@ __device__ void ell2lp(const GeoJob &J, int k, const double T[3], double &az, do
     az += sol;
     it0 = 1;   // that step is the solve's first iteration
   }
-  const bool done = it0 == 1 && fabs(sol) < 1e-010;
-  for (int it = it0; it <= 10 && !done; it++) {
+  // at least one step from an exact orbit evaluation, also when the shifted
+  // step is already below the bound: the zero-Doppler root is sensitive to
+  // the velocity's direction, which the shift only approximates
+  for (int it = it0; it <= 10 && !(it > it0 && fabs(sol) < 1e-010); it++) {
     const double t = (az - J.mid_time[k]) * 0.1;
     orbit_eval(c, n, t, P, V, A);
     const double dx = T[0] - P[0], dy = T[1] - P[1], dz = T[2] - P[2];
