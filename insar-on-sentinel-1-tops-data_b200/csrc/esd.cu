@@ -92,49 +92,9 @@ __global__ void __launch_bounds__(ES_NT, 2) esd_kernel(const __grid_constant__ E
   const bool xin = tid < nload && x >= 0 && x < O.pixels;
   float accr = 0.f, acci = 0.f;
 
-  for (int rg = r_begin; rg < r_end; rg += ES_GR) {
-    const int gr = min(ES_GR, r_end - rg);
-    float4 aF[ES_GR], aB[ES_GR];
-    float2 cF[ES_GR], cB[ES_GR];
-#pragma unroll
-    for (int k = 0; k < ES_GR; k++) {
-      aF[k] = aB[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-      cF[k] = cB[k] = make_float2(0.f, 0.f);
-    }
-    // input rows rg - dh .. rg - dh + nin - 1 (all of them for a full group:
-    // rows past the overlap's end load as zero)
-    const int nin = WAZ > 0 ? ES_GR + WAZ - 1 : gr + win_az - 1;
-#pragma unroll
-    for (int q = 0; q < (WAZ > 0 ? ES_GR + WAZ - 1 : 1 << 20); q++) {
-      if (WAZ == 0 && q >= nin) break;
-      const int y = rg - dh + q;
-      float4 pF = make_float4(0.f, 0.f, 0.f, 0.f), pB = pF;
-      if (xin && y >= 0 && y < O.lines) {
-        const long mo = (long)y * O.m_pitch + x, so = (long)y * O.s_pitch + x;
-        pF = prod4(O.mF[mo], O.sF[so]);
-        pB = prod4(O.mB[mo], O.sB[so]);
-      }
-#pragma unroll
-      for (int k = 0; k < ES_GR; k++) {
-        const int j = q - k;
-        if (j >= 0 && j < win_az) {
-          aF[k].x += pF.x; aF[k].y += pF.y; aF[k].z += pF.z; aF[k].w += pF.w;
-          aB[k].x += pB.x; aB[k].y += pB.y; aB[k].z += pB.z; aB[k].w += pB.w;
-        }
-        if (q == k + dh) {
-          cF[k] = make_float2(pF.x, pF.y);
-          cB[k] = make_float2(pB.x, pB.y);
-        }
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < ES_GR; k++) {
-      S.VF[k][tid] = aF[k];
-      S.VB[k][tid] = aB[k];
-      S.IF[k][tid] = cF[k];
-      S.IB[k][tid] = cB[k];
-    }
-    __syncthreads();
+  // horizontal box, mask and unit phasor of the group's rows (shared-memory
+  // vertical sums and centre interferograms), accumulated into accr / acci
+  auto horizontal = [&](int gr) {
     const int ngrp = (cN + 3) >> 2;
     for (int it = tid; it < gr * ngrp; it += ES_NT) {
       const int k = it / ngrp;
@@ -178,7 +138,127 @@ __global__ void __launch_bounds__(ES_NT, 2) esd_kernel(const __grid_constant__ E
         }
       }
     }
+  };
+
+  if constexpr (WAZ > 0 && WAZ <= 4) {
+    // Short windows: the products of the last WAZ - 1 input rows stay in
+    // registers from one group to the next, so every input row is read
+    // once, and the next group's rows are loaded before the current group's
+    // horizontal pass, so their latency overlaps it.
+    constexpr int NQ = WAZ - 1 > 0 ? WAZ - 1 : 1;
+    auto load = [&](int y, short2 &mf, float2 &sf, short2 &mb, float2 &sb) {
+      mf = mb = make_short2(0, 0);
+      sf = sb = make_float2(0.f, 0.f);
+      if (xin && y >= 0 && y < O.lines) {
+        const long mo = (long)y * O.m_pitch + x, so = (long)y * O.s_pitch + x;
+        mf = O.mF[mo];
+        sf = O.sF[so];
+        mb = O.mB[mo];
+        sb = O.sB[so];
+      }
+    };
+    float4 qF[NQ], qB[NQ];
+#pragma unroll
+    for (int j = 0; j < WAZ - 1; j++) {
+      short2 mf, mb;
+      float2 sf, sb;
+      load(r_begin - dh + j, mf, sf, mb, sb);
+      qF[j] = prod4(mf, sf);
+      qB[j] = prod4(mb, sb);
+    }
+    short2 vmf[ES_GR], vmb[ES_GR];
+    float2 vsf[ES_GR], vsb[ES_GR];
+#pragma unroll
+    for (int k = 0; k < ES_GR; k++)
+      load(r_begin - dh + WAZ - 1 + k, vmf[k], vsf[k], vmb[k], vsb[k]);
+    for (int rg = r_begin; rg < r_end; rg += ES_GR) {
+      const int gr = min(ES_GR, r_end - rg);
+      float4 pF[WAZ - 1 + ES_GR], pB[WAZ - 1 + ES_GR];
+#pragma unroll
+      for (int j = 0; j < WAZ - 1; j++) {
+        pF[j] = qF[j];
+        pB[j] = qB[j];
+      }
+#pragma unroll
+      for (int k = 0; k < ES_GR; k++) {
+        pF[WAZ - 1 + k] = prod4(vmf[k], vsf[k]);
+        pB[WAZ - 1 + k] = prod4(vmb[k], vsb[k]);
+      }
+      const int rn = rg + ES_GR;
+      if (rn < r_end) {
+#pragma unroll
+        for (int k = 0; k < ES_GR; k++)
+          load(rn - dh + WAZ - 1 + k, vmf[k], vsf[k], vmb[k], vsb[k]);
+      }
+#pragma unroll
+      for (int k = 0; k < ES_GR; k++) {
+        float4 aF = pF[k], aB = pB[k];
+#pragma unroll
+        for (int j = 1; j < WAZ; j++) {
+          aF.x += pF[k + j].x; aF.y += pF[k + j].y; aF.z += pF[k + j].z; aF.w += pF[k + j].w;
+          aB.x += pB[k + j].x; aB.y += pB[k + j].y; aB.z += pB[k + j].z; aB.w += pB[k + j].w;
+        }
+        S.VF[k][tid] = aF;
+        S.VB[k][tid] = aB;
+        S.IF[k][tid] = make_float2(pF[k + dh].x, pF[k + dh].y);
+        S.IB[k][tid] = make_float2(pB[k + dh].x, pB[k + dh].y);
+      }
+#pragma unroll
+      for (int j = 0; j < WAZ - 1; j++) {
+        qF[j] = pF[ES_GR + j];
+        qB[j] = pB[ES_GR + j];
+      }
+      __syncthreads();
+      horizontal(gr);
+      __syncthreads();
+    }
+  } else {
+  for (int rg = r_begin; rg < r_end; rg += ES_GR) {
+    const int gr = min(ES_GR, r_end - rg);
+    float4 aF[ES_GR], aB[ES_GR];
+    float2 cF[ES_GR], cB[ES_GR];
+#pragma unroll
+    for (int k = 0; k < ES_GR; k++) {
+      aF[k] = aB[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+      cF[k] = cB[k] = make_float2(0.f, 0.f);
+    }
+    // input rows rg - dh .. rg - dh + nin - 1 (all of them for a full group:
+    // rows past the overlap's end load as zero)
+    const int nin = WAZ > 0 ? ES_GR + WAZ - 1 : gr + win_az - 1;
+#pragma unroll
+    for (int q = 0; q < (WAZ > 0 ? ES_GR + WAZ - 1 : 1 << 20); q++) {
+      if (WAZ == 0 && q >= nin) break;
+      const int y = rg - dh + q;
+      float4 pF = make_float4(0.f, 0.f, 0.f, 0.f), pB = pF;
+      if (xin && y >= 0 && y < O.lines) {
+        const long mo = (long)y * O.m_pitch + x, so = (long)y * O.s_pitch + x;
+        pF = prod4(O.mF[mo], O.sF[so]);
+        pB = prod4(O.mB[mo], O.sB[so]);
+      }
+#pragma unroll
+      for (int k = 0; k < ES_GR; k++) {
+        const int j = q - k;
+        if (j >= 0 && j < win_az) {
+          aF[k].x += pF.x; aF[k].y += pF.y; aF[k].z += pF.z; aF[k].w += pF.w;
+          aB[k].x += pB.x; aB[k].y += pB.y; aB[k].z += pB.z; aB[k].w += pB.w;
+        }
+        if (q == k + dh) {
+          cF[k] = make_float2(pF.x, pF.y);
+          cB[k] = make_float2(pB.x, pB.y);
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < ES_GR; k++) {
+      S.VF[k][tid] = aF[k];
+      S.VB[k][tid] = aB[k];
+      S.IF[k][tid] = cF[k];
+      S.IB[k][tid] = cB[k];
+    }
     __syncthreads();
+    horizontal(gr);
+    __syncthreads();
+  }
   }
   // ---- block reduction (fixed order)
   for (int o = 16; o > 0; o >>= 1) {
