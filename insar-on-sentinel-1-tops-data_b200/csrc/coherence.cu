@@ -45,7 +45,7 @@ struct CoBatch {
 
 struct CoShared {
   float4 V[CO_GR][pad8(CO_NT)];      // vertical sums (re, im, |s|^2, |m|^2), pad8(x)
-  float judge[CO_GR][pad8(CO_NT)];   // |s|^2 of the centre pixel, pad8(x)
+  float spow[CO_GR][pad8(CO_NT)];   // |s|^2 of the centre pixel, pad8(x)
   int next_item;                     // persistent launch: the item just taken
 };
 
@@ -80,7 +80,7 @@ __device__ __forceinline__ void coh_horizontal(const CoShared &S, const CohJob &
     const int cg = (it - k * NG) * CO_CPI;
     if (cg >= cN) continue;
     const float4 *V = &S.V[k][pad8(cg)];
-    const float *Jd = &S.judge[k][pad8(cg)];
+    const float *Jd = &S.spow[k][pad8(cg)];
     float4 w = make_float4(0.f, 0.f, 0.f, 0.f);
     if (WRG > 0) {
 #pragma unroll
@@ -191,7 +191,7 @@ __device__ __forceinline__ void coherence_item(CoShared &S, const CoBatch &B, in
 #pragma unroll
         for (int j = 1; j < WAZ; j++) add4(a, p[k + j]);
         S.V[k][pad8(tid)] = a;
-        S.judge[k][pad8(tid)] = p[k + dy].z;
+        S.spow[k][pad8(tid)] = p[k + dy].z;
       }
 #pragma unroll
       for (int j = 0; j < NQ; j++) q[j] = p[CO_GR + j];
@@ -204,11 +204,11 @@ __device__ __forceinline__ void coherence_item(CoShared &S, const CoBatch &B, in
       const int gr = min(CO_GR, r_end - rg);
       // vertical pass: input rows rg-dy .. rg-dy+gr+win_az-2
       float4 acc[CO_GR];
-      float judge[CO_GR];
+      float spow[CO_GR];
 #pragma unroll
       for (int k = 0; k < CO_GR; k++) {
         acc[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-        judge[k] = 0.f;
+        spow[k] = 0.f;
       }
       const int nin = gr + win_az - 1;
       for (int qi = 0; qi < nin; qi++) {
@@ -220,13 +220,13 @@ __device__ __forceinline__ void coherence_item(CoShared &S, const CoBatch &B, in
         for (int k = 0; k < CO_GR; k++) {
           const int j = qi - k;
           if (j >= 0 && j < win_az) add4(acc[k], pr);
-          if (qi == k + dy) judge[k] = pr.z;
+          if (qi == k + dy) spow[k] = pr.z;
         }
       }
 #pragma unroll
       for (int k = 0; k < CO_GR; k++) {
         S.V[k][pad8(tid)] = acc[k];
-        S.judge[k][pad8(tid)] = judge[k];
+        S.spow[k][pad8(tid)] = spow[k];
       }
       __syncthreads();
       coh_horizontal<WRG>(S, J, tid, rg, gr, c0, cN, win_rg, dx);

@@ -649,9 +649,9 @@ void orc_coherence(const int16_t *master, const float *slave, int lines, int pix
         }
       }
       size_t k = (size_t)r * pixels + c;
-      double judge = hypot((double)slave[2 * k], (double)slave[2 * k + 1]);
+      double amp = hypot((double)slave[2 * k], (double)slave[2 * k + 1]);
       double p = ps * pm;
-      if (judge < 0.001)
+      if (amp < 0.001)
         coh[k] = 0.0;
       else
         coh[k] = (p > 0.0) ? sqrt(sre * sre + sim * sim) / sqrt(p) : 0.0;
