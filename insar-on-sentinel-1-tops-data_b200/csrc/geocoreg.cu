@@ -54,8 +54,33 @@ struct GcBatch {
 // Position and the first two derivatives with respect to the normalised time
 // t of an orbit polynomial (getPos/getVelo/getAcc, Geocoreg_cuda.cu:123-205,
 // return the derivatives divided by 10 and 100).
+// The same with the coefficient count N known at compile time (fully
+// unrolled; the orbit fit returns 6 coefficients for more than 6 state
+// vectors, Func.cpp:1050-1126).
+template <int N>
+__device__ __forceinline__ void orbit_eval_n(const double (*c)[8], double t, double p[3],
+                                             double v[3], double a[3]) {
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    double pp = c[k][N - 1], vv = 0.0, aa = 0.0;
+#pragma unroll
+    for (int i = N - 2; i >= 0; --i) {
+      aa = fma(aa, t, 2.0 * vv);
+      vv = fma(vv, t, pp);
+      pp = fma(pp, t, c[k][i]);
+    }
+    p[k] = pp;
+    v[k] = vv;
+    a[k] = aa;
+  }
+}
+
 __device__ __forceinline__ void orbit_eval(const double (*c)[8], int n, double t, double p[3],
                                            double v[3], double a[3]) {
+  if (n == 6) {
+    orbit_eval_n<6>(c, t, p, v, a);
+    return;
+  }
 #pragma unroll
   for (int k = 0; k < 3; k++) {
     double pp = c[k][n - 1], vv = 0.0, aa = 0.0;
