@@ -624,6 +624,93 @@ def stitch_line_map(info: "SwathInfo", first_valid, last_valid, burst0: int, bur
                                    burstN, ptr(out, C.c_int), h.value, C.byref(h)),
           "tops_stitch_line_map")
     return out
+# ------------------------------------------------ Sentinel-1 front end (tops_s1.h)
+class S1Annotation(C.Structure):
+    _fields_ = [
+        ("polarisation", C.c_char * 8), ("first_line_utc", C.c_char * 40),
+        ("last_line_utc", C.c_char * 40), ("dc_method", C.c_char * 40),
+        ("number_of_lines", C.c_int), ("number_of_samples", C.c_int),
+        ("last_valid_pixel", C.c_int),
+        ("azimuth_pixel_spacing", C.c_double), ("radar_frequency", C.c_double),
+        ("heading", C.c_double), ("range_bandwidth", C.c_double),
+        ("ascending_node_time", C.c_double), ("slr_time_last_pixel", C.c_double),
+        ("first_valid_line", C.c_int * MAX_BURSTS), ("last_valid_line", C.c_int * MAX_BURSTS),
+        ("burst_first_valid_time", C.c_double * MAX_BURSTS),
+        ("burst_last_valid_time", C.c_double * MAX_BURSTS),
+        ("burst_lat_min", C.c_double * MAX_BURSTS), ("burst_lat_max", C.c_double * MAX_BURSTS),
+        ("burst_lon_min", C.c_double * MAX_BURSTS), ("burst_lon_max", C.c_double * MAX_BURSTS),
+        ("geo_lines", C.c_int), ("geo_points_per_line", C.c_int),
+    ]
+
+
+class S1Geogrid(C.Structure):
+    _fields_ = [("lines", C.c_int), ("points", C.c_int), ("az_time", _dp), ("slr_time", _dp),
+                ("lat", _dp), ("lon", _dp)]
+
+
+_proto("tops_s1_annotation_read", C.c_int, [C.c_char_p, C.POINTER(SwathInfo),
+                                            C.POINTER(S1Annotation)])
+_proto("tops_s1_geogrid_read", C.c_int, [C.c_char_p, C.c_int, _dp, _dp, _dp, _dp, _dp, _ip, _ip])
+_proto("tops_s1_orbit_read", C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.POINTER(SwathInfo),
+                                       _dp])
+_proto("tops_s1_burst_overlap", C.c_int, [C.c_int, C.c_int, C.POINTER(SwathInfo),
+                                          C.POINTER(S1Geogrid), C.POINTER(SwathInfo),
+                                          C.POINTER(S1Geogrid), _ip, _ip, _ip, _ip])
+
+
+def s1_annotation_read(path: str, info: "SwathInfo" = None):
+    """(SwathInfo, S1Annotation) of one annotation file (tops_s1_annotation_read);
+    the state vectors of a given info are kept."""
+    info = info if info is not None else SwathInfo()
+    ex = S1Annotation()
+    check(lib.tops_s1_annotation_read(str(path).encode(), C.byref(info), C.byref(ex)),
+          "tops_s1_annotation_read")
+    return info, ex
+
+
+def s1_geogrid_read(path: str) -> dict:
+    """Geolocation grid arrays [lines][points] of an annotation file."""
+    nl, npl = C.c_int(), C.c_int()
+    check(lib.tops_s1_geogrid_read(str(path).encode(), 0, None, None, None, None, None,
+                                   C.byref(nl), C.byref(npl)), "tops_s1_geogrid_read")
+    n = nl.value * npl.value
+    g = {k: np.zeros(n) for k in ("az_time", "slr_time", "lat", "lon", "incidence")}
+    check(lib.tops_s1_geogrid_read(str(path).encode(), n, *(ptr(g[k], C.c_double) for k in
+                                   ("az_time", "slr_time", "lat", "lon", "incidence")),
+                                   C.byref(nl), C.byref(npl)), "tops_s1_geogrid_read")
+    g = {k: v.reshape(nl.value, npl.value) for k, v in g.items()}
+    return g
+
+
+def s1_orbit_read(path: str, first_line_utc: str, last_line_utc: str, info: "SwathInfo"):
+    """Fills info's state vectors from an EOF file (tops_s1_orbit_read);
+    returns the [n][3] velocities."""
+    vel = np.zeros((32, 3))
+    check(lib.tops_s1_orbit_read(str(path).encode(), first_line_utc.encode(),
+                                 last_line_utc.encode(), C.byref(info), ptr(vel, C.c_double)),
+          "tops_s1_orbit_read")
+    return vel[:info.n_sv].copy()
+
+
+def _grid_struct(g: dict):
+    keep = [np.ascontiguousarray(g[k], np.float64) for k in ("az_time", "slr_time", "lat", "lon")]
+    lines, points = keep[0].shape
+    return S1Geogrid(lines, points, *(ptr(a, C.c_double) for a in keep)), keep
+
+
+def s1_burst_overlap(burst0: int, burstN: int, master: "SwathInfo", master_grid: dict,
+                     slave: "SwathInfo", slave_grid: dict):
+    """(m_burst0, m_burstN, s_burst0, s_burstN), 0-based (tops_s1_burst_overlap);
+    burst0 / burstN are 1-based as in config.txt."""
+    mg, k1 = _grid_struct(master_grid)
+    sg, k2 = _grid_struct(slave_grid)
+    out = [C.c_int(-1) for _ in range(4)]
+    check(lib.tops_s1_burst_overlap(burst0, burstN, C.byref(master), C.byref(mg),
+                                    C.byref(slave), C.byref(sg), *(C.byref(o) for o in out)),
+          "tops_s1_burst_overlap")
+    return tuple(o.value for o in out)
+
+
 _proto("tops_pair_stage_times", C.c_int, [_vp, _vp, _fp])
 _proto("tops_pair_process", C.c_int, [_vp, _vp, _vp, _vp, _vp, _fp, _dp, _dp, _vp])
 _proto("tops_batch_create", C.c_int, [C.POINTER(_vp), C.c_int, C.POINTER(_vp)])

@@ -8,6 +8,7 @@ stores every input they saw and what they returned:
 
     python tests/golden/make_golden.py host [--scene 2]   -> tests/golden/ref_host[2].npz
     python tests/golden/make_golden.py stitch          -> tests/golden/ref_stitch.npz
+    python tests/golden/make_golden.py front           -> tests/golden/ref_front.npz
     python tests/golden/make_golden.py stages [--scene 2] [--out D]
                                                    -> D/ref_stages[2].npz (needs a GPU)
 
@@ -239,6 +240,100 @@ def host(out_path):
     print(f"wrote {out_path}: {len(keep)} arrays")
 
 
+# ------------------------------------------------------------ front part
+# Burst matching (ComputerBurstOverlap, Func.cpp:1610-1746) on sub-ranges of
+# one synthetic 6-burst pair: (burst0, burstN) 1-based as in config.txt, and
+# the scene bursts the master and the slave start at.  A slave that starts
+# later than the master's burst0 takes the reference's second branch
+# (Func.cpp:1685-1741).
+FRONT_SCENE = dict(n_bursts=6, lines_per_burst=200, samples_per_burst=400, overlap_lines=20,
+                   dem_lines=160, dem_pixels=160, seed=31)
+FRONT_CASES = [(1, 6, 0, 0), (2, 5, 0, 0), (4, 6, 0, 0), (6, 6, 0, 0), (3, 6, 0, 2),
+               (1, 4, 0, 2), (1, 6, 2, 0), (2, 3, 1, 3), (1, 6, 0, 3)]
+
+
+class RefImage(C.Structure):
+    _fields_ = [("n_bursts", C.c_int), ("lines_per_burst", C.c_int),
+                ("samples_per_burst", C.c_int), ("dt", C.c_double), ("prf", C.c_double),
+                ("rsr", C.c_double), ("slr_first", C.c_double), ("slr_last", C.c_double),
+                ("first_line_time", C.c_double), ("last_line_time", C.c_double),
+                ("burst_first_line_time", _dp), ("geo_lines", C.c_int), ("geo_points", C.c_int),
+                ("az_time", _dp), ("slr_time", _dp), ("lat", _dp), ("lon", _dp),
+                ("n_points", C.c_int), ("n_coef", C.c_int), ("orbit_t", _dp), ("cx", _dp),
+                ("cy", _dp), ("cz", _dp)]
+
+
+def sub_swath_info(info, k):
+    """The sub-swath's bursts from k on (a copy; the state vectors stay)."""
+    import topsb200 as T
+    out = T.SwathInfo()
+    C.memmove(C.byref(out), C.byref(info), C.sizeof(info))
+    nb = info.n_bursts - k
+    out.n_bursts = nb
+    for b in range(nb):
+        out.burst_first_line_time[b] = info.burst_first_line_time[b + k]
+        out.burst_last_line_time[b] = info.burst_last_line_time[b + k]
+    out.first_line_time = out.burst_first_line_time[0]
+    out.last_line_time = out.burst_last_line_time[nb - 1]
+    return out
+
+
+def front(out_path):
+    import topsb200 as T
+    sys.path.insert(0, os.path.dirname(HERE))
+    import s1_files
+    H = _lib("libref_host.so")
+    Fr = _lib("libref_front.so")
+    H.ref_polyfit_orbit.restype = C.c_int
+    H.ref_polyfit_orbit.argtypes = [C.c_int] + [_dp] * 7
+    Fr.ref_burst_overlap.restype = None
+    Fr.ref_burst_overlap.argtypes = [C.c_int, C.c_int, C.POINTER(RefImage), C.POINTER(RefImage),
+                                     _ip]
+    S = T.Scene(**FRONT_SCENE)
+    out = {"cases": np.array(FRONT_CASES, np.int32)}
+    keep = []
+
+    def ref_image(info, grid):
+        t, x, y, z = (np.ascontiguousarray(info_arr) for info_arr in
+                      (info.sv_t[:info.n_sv], info.sv_x[:info.n_sv], info.sv_y[:info.n_sv],
+                       info.sv_z[:info.n_sv]))
+        cx, cy, cz = (np.zeros(8) for _ in range(3))
+        n = H.ref_polyfit_orbit(len(t), _ptr(t, C.c_double), _ptr(x, C.c_double),
+                                _ptr(y, C.c_double), _ptr(z, C.c_double), _ptr(cx, C.c_double),
+                                _ptr(cy, C.c_double), _ptr(cz, C.c_double))
+        bft = np.ascontiguousarray(info.burst_first_line_time[:info.n_bursts])
+        g = {k: np.ascontiguousarray(grid[k], np.float64) for k in
+             ("az_time", "slr_time", "lat", "lon")}
+        keep.extend([t, cx, cy, cz, bft, *g.values()])
+        slr_last = info.slr_time + (info.samples_per_burst - 1) * info.range_spacing / 299792458.0
+        return RefImage(info.n_bursts, info.lines_per_burst, info.samples_per_burst, info.dt,
+                        info.prf, info.rsr, info.slr_time, slr_last, info.first_line_time,
+                        info.last_line_time, _ptr(bft, C.c_double), g["az_time"].shape[0],
+                        g["az_time"].shape[1], _ptr(g["az_time"], C.c_double),
+                        _ptr(g["slr_time"], C.c_double), _ptr(g["lat"], C.c_double),
+                        _ptr(g["lon"], C.c_double), len(t), n, _ptr(t, C.c_double),
+                        _ptr(cx, C.c_double), _ptr(cy, C.c_double), _ptr(cz, C.c_double))
+
+    for i, (b0, bN, km, ks) in enumerate(FRONT_CASES):
+        m = sub_swath_info(S.swath[0], km)
+        sl = sub_swath_info(S.swath[1], ks)
+        gm = s1_files.grid_from_scene(S, m, first_burst=km)
+        gs = s1_files.grid_from_scene(S, sl, first_burst=ks)
+        rm, rs = ref_image(m, gm), ref_image(sl, gs)
+        res = np.full(4, -1, np.int32)
+        Fr.ref_burst_overlap(b0, bN, C.byref(rm), C.byref(rs), _ptr(res, C.c_int))
+        for tag, info, g in (("m", m, gm), ("s", sl, gs)):
+            for k, v in swath_fields(info).items():
+                out[f"c{i}_{tag}_{k}"] = v
+            for k in ("az_time", "slr_time", "lat", "lon"):
+                out[f"c{i}_{tag}_grid_{k}"] = g[k]
+        out[f"c{i}_out"] = res
+        print(f"case {i} burst {b0}..{bN} master from {km} slave from {ks}: {res.tolist()}")
+    S.close()
+    np.savez_compressed(out_path, **out)
+    print(f"wrote {out_path}: {len(out)} arrays")
+
+
 # ---------------------------------------------------------- stitch part
 # Burst timings of the debursting cases: S1 IW-like (2.055 ms lines, 1500
 # lines per burst, a 2.7585 s burst cycle, about 157 overlap lines), with
@@ -451,7 +546,7 @@ def stages(out_path, host_path):
 
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
-    ap.add_argument("part", choices=("host", "stitch", "stages"))
+    ap.add_argument("part", choices=("host", "stitch", "stages", "front"))
     ap.add_argument("--out", default=HERE)
     ap.add_argument("--scene", default="1", choices=sorted(SCENES))
     a = ap.parse_args()
@@ -463,6 +558,8 @@ def main():
         host(os.path.join(a.out, f"ref_host{sfx}.npz"))
     elif a.part == "stitch":
         stitch(os.path.join(a.out, "ref_stitch.npz"))
+    elif a.part == "front":
+        front(os.path.join(a.out, "ref_front.npz"))
     else:
         stages(os.path.join(a.out, f"ref_stages{sfx}.npz"), os.path.join(HERE, f"ref_host{sfx}.npz"))
 
