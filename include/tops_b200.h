@@ -320,8 +320,9 @@ int tops_stitch(const void *src, size_t src_pitch, void *dst, size_t dst_pitch,
 /* ======================================================= TIFF raster I/O */
 
 /* Pixel types of the reference's GeoTIFF files (GDAL GDT_CInt16,
- * GDT_Float32, GDT_CFloat32: SLCs, coherence, resampled slaves). */
-enum { TOPS_TIFF_CINT16 = 1, TOPS_TIFF_FLOAT32 = 2, TOPS_TIFF_CFLOAT32 = 3 };
+ * GDT_Float32, GDT_CFloat32: SLCs, coherence, resampled slaves; GDT_Int16:
+ * the DEM it reads, DataTypes.cpp:230-290). */
+enum { TOPS_TIFF_CINT16 = 1, TOPS_TIFF_FLOAT32 = 2, TOPS_TIFF_CFLOAT32 = 3, TOPS_TIFF_INT16 = 4 };
 
 /* Writes a single-band, uncompressed, little-endian baseline TIFF
  * (strips, SampleFormat complex int / IEEE float / complex IEEE float), the
@@ -332,10 +333,24 @@ int tops_tiff_write(const char *path, int type, int width, int height, const voi
                     size_t pitch);
 
 /* Reads a single-band, uncompressed, strip-organised TIFF of one of the
- * three pixel types (little- or big-endian file); data NULL: only the type
+ * pixel types (little- or big-endian file; 16-bit unsigned samples are read
+ * as TOPS_TIFF_INT16, as GDAL's Int16 reads them); data NULL: only the type
  * and size are returned.  Rows are packed (width * pixel bytes). */
 int tops_tiff_read(const char *path, int *type, int *width, int *height, void *data,
                    size_t capacity);
+
+/* The geotransform GDAL gives a north-up GeoTIFF (the reference's RefDem::Init,
+ * DataTypes.cpp:200-222, reads the DEM's through GDALGetGeoTransform):
+ * gt[0] / gt[3] x / y of the upper-left corner, gt[1] pixel width, gt[5]
+ * pixel height (negative), gt[2] = gt[4] = 0; from ModelPixelScale and
+ * ModelTiepoint, the origin moved half a pixel for PixelIsPoint rasters.
+ * TOPS_E_INVALID without those tags. */
+int tops_tiff_georef(const char *path, double gt[6]);
+
+/* tops_tiff_write with that georeferencing (north-up, geographic WGS 84,
+ * pixel is area), e.g. for a DEM; gt as tops_tiff_georef returns it. */
+int tops_tiff_write_georef(const char *path, int type, int width, int height, const void *data,
+                           size_t pitch, const double gt[6]);
 
 /* ============================================================ config */
 

@@ -132,10 +132,18 @@ int tops_pair_run_per_burst(tops_pair *p, void *stream);
  * <process_dir>/ReSlave-N.tif, ReSlaveESD-N.tif and Coh-N.tif (TIFF rasters,
  * CFloat32 / Float32) -- plus CohStitch-N.tif, the debursted coherence, when
  * the config sets stitch=1 (the reference's stitching step is disabled).
- * Product, orbit and DEM readers are outside this library: each sub-swath's
- * inputs come from the seeded synthetic generator (sub-swath N: seed +
+ * With masterpath / slavepath naming SAFE directories, each sub-swath's
+ * inputs are read from them (the annotation file whose name holds
+ * "-iwN-" and "-slc-<polarisation>", and the measurement raster of the same
+ * name), from preciseOrbitMaster /
+ * preciseOrbitSlave (the state vectors around the product's first
+ * sub-swath) and from SpecificDemPath (an int16 or float32 GeoTIFF); the
+ * master's bursts burst0..burstN are matched on the slave
+ * (tops_s1_burst_overlap) and each burst's DEM window is its lat/lon box
+ * plus 24 DEM pixels.  With masterpath empty or "(synthetic)", the inputs
+ * come from the seeded synthetic generator (sub-swath N: seed +
  * 1000 (N - 1)).  Returns TOPS_E_CONFIG for a malformed or unsupported
- * config (npoints other than 12, empty ranges). */
+ * config (npoints other than 12, empty ranges) or missing product files. */
 typedef struct {
   int subswaths, burst_pairs;   /* processed */
   double seconds;               /* processing and writing, without scene generation */

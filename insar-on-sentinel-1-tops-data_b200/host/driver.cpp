@@ -6,12 +6,19 @@
 // firstsubswath to lastsubswath runs geometric coregistration, deramp and
 // resampling, ESD and coherence over the bursts burst0..burstN (1-based),
 // writing ReSlave-N.tif, ReSlaveESD-N.tif and Coh-N.tif into process_dir
-// (and, in its disabled stitching step, CohStitch-N.tif).  Product readers
-// are outside this library, so the inputs of each sub-swath come from the
-// seeded synthetic generator, configured by the synthetic keys of the same
-// file (seed, n_bursts, lines_per_burst, ...; sub-swath N uses seed +
-// 1000 (N - 1)).  The processing is the device-resident burst-pair plan; the
-// outputs are written as TIFF rasters of the reference's pixel types.
+// (and, in its disabled stitching step, CohStitch-N.tif).
+//
+// With masterpath set (and not "(synthetic)"), the inputs are the products
+// the reference reads: the SAFE directories' annotation files and
+// measurement rasters of the configured polarisation, the precise-orbit
+// files and the GeoTIFF DEM (tops_s1.h readers, tops_tiff_read /
+// tops_tiff_georef), with the master's bursts burst0..burstN matched on the
+// slave (ComputerBurstOverlap).  Otherwise each sub-swath comes from the
+// seeded synthetic generator,
+// configured by the synthetic keys of the same file (seed, n_bursts,
+// lines_per_burst, ...; sub-swath N uses seed + 1000 (N - 1)).  The
+// processing is the device-resident burst-pair plan; the outputs are
+// written as TIFF rasters of the reference's pixel types.
 #include <cuda_runtime.h>
 #include <errno.h>
 #include <stdio.h>
@@ -22,7 +29,13 @@
 #include <string>
 #include <vector>
 
+#include <dirent.h>
+#include <math.h>
+
+#include <algorithm>
+
 #include "tops_pipeline.h"
+#include "tops_s1.h"
 #include "tops_synth.h"
 
 namespace {
@@ -71,6 +84,22 @@ int make_dir(const std::string &d) {
     if (_s != TOPS_OK) return _s;       \
   } while (0)
 
+// The inputs of one sub-swath pair for the plan: k bursts each, the DEM with
+// its geotransform and one window per burst, the burst-stacked SLC rows and
+// the valid lines of each master burst (for debursting).
+struct PairInputs {
+  tops_swath_info m, s;
+  int k = 0;
+  const float *dem = nullptr;
+  int dem_lines = 0, dem_pixels = 0;
+  double lat0 = 0, lon0 = 0, dlat = 0, dlon = 0;
+  std::vector<tops_dem_window> win;
+  const int16_t *ms = nullptr, *ss = nullptr;
+  std::vector<int> first_valid, last_valid;
+};
+
+int process_pair(const tops_config &c, int nsub, tops_run_stats *st, const PairInputs &in);
+
 int run_subswath(const tops_config &c, int nsub, tops_run_stats *st) {
   tops_synth_cfg sc;
   D_TRY(tops_synth_defaults(&sc));
@@ -90,18 +119,192 @@ int run_subswath(const tops_config &c, int nsub, tops_run_stats *st) {
   tops_swath_info mi, si;
   D_TRY(tops_synth_swath(scene.s, 0, &mi));
   D_TRY(tops_synth_swath(scene.s, 1, &si));
-  const tops_swath_info m = sub_swath(mi, b0, k), s = sub_swath(si, b0, k);
-  const int L = m.lines_per_burst, W = m.samples_per_burst;
+  PairInputs in;
+  in.m = sub_swath(mi, b0, k);
+  in.s = sub_swath(si, b0, k);
+  in.k = k;
+  const int L = in.m.lines_per_burst, W = in.m.samples_per_burst;
   tops_dem_info di;
-  const float *dem = tops_synth_dem(scene.s, &di);
-  std::vector<tops_dem_window> win(k);
+  in.dem = tops_synth_dem(scene.s, &di);
+  in.dem_lines = di.lines;
+  in.dem_pixels = di.pixels;
+  in.lat0 = di.lat0;
+  in.lon0 = di.lon0;
+  in.dlat = di.dlat;
+  in.dlon = di.dlon;
+  in.win.resize(k);
   for (int i = 0; i < k; i++)
-    D_TRY(tops_synth_burst_dem_window(scene.s, b0 + i, 24, &win[i].row0, &win[i].col0,
-                                      &win[i].rows, &win[i].cols));
+    D_TRY(tops_synth_burst_dem_window(scene.s, b0 + i, 24, &in.win[i].row0, &in.win[i].col0,
+                                      &in.win[i].rows, &in.win[i].cols));
   const size_t burst_elems = (size_t)L * W * 2;   // int16 per burst
-  const int16_t *ms = tops_synth_slc(scene.s, 0) + (size_t)b0 * burst_elems;
-  const int16_t *ss = tops_synth_slc(scene.s, 1) + (size_t)b0 * burst_elems;
+  in.ms = tops_synth_slc(scene.s, 0) + (size_t)b0 * burst_elems;
+  in.ss = tops_synth_slc(scene.s, 1) + (size_t)b0 * burst_elems;
+  // every line of the synthetic bursts is valid
+  in.first_valid.assign(k, 0);
+  in.last_valid.assign(k, L - 1);
+  return process_pair(c, nsub, st, in);
+}
 
+// ------------------------------------------------------------ products
+// Names in dir that contain `needle` and end in one of the extensions,
+// sorted (the reference lists a SAFE directory's files the same way,
+// GetFiles, Func.cpp:579-628).
+std::vector<std::string> list_files(const std::string &dir, const std::string &needle,
+                                    std::initializer_list<const char *> exts) {
+  std::vector<std::string> out;
+  DIR *d = opendir(dir.c_str());
+  if (!d) return out;
+  while (struct dirent *e = readdir(d)) {
+    const std::string n = e->d_name;
+    if (n.find(needle) == std::string::npos) continue;
+    for (const char *x : exts) {
+      const size_t lx = strlen(x);
+      if (n.size() > lx && n.compare(n.size() - lx, lx, x) == 0) {
+        out.push_back(n);
+        break;
+      }
+    }
+  }
+  closedir(d);
+  std::sort(out.begin(), out.end());
+  return out;
+}
+
+// One sub-swath of one product: annotation, geolocation grid, state
+// vectors and the measurement raster.
+struct Product {
+  tops_swath_info info;
+  tops_s1_annotation ann;
+  std::vector<double> az, rg, lat, lon;
+  int geo_lines = 0, geo_points = 0;
+  std::vector<int16_t> slc;   // [lines][samples][2]
+  int slc_lines = 0, slc_samples = 0;
+};
+
+int load_product(const std::string &safe, int nsub, const std::string &pol,
+                 const std::string &orbit, Product &P) {
+  const std::string adir = safe + "/annotation", mdir = safe + "/measurement";
+  const std::string flag = "-slc-" + pol;
+  const std::vector<std::string> xmls = list_files(adir, flag, {".xml"});
+  const std::string iw = "-iw" + std::to_string(nsub) + "-";
+  std::string xml;
+  for (const std::string &n : xmls)
+    if (n.find(iw) != std::string::npos) xml = n;
+  if (xml.empty()) return TOPS_E_CONFIG;
+  memset(&P.info, 0, sizeof P.info);
+  D_TRY(tops_s1_annotation_read((adir + "/" + xml).c_str(), &P.info, &P.ann));
+  // the state vectors around the product's first sub-swath's lines, as the
+  // reference reads them once per product (Main.cpp:33-36)
+  tops_s1_annotation first;
+  tops_swath_info tmp;
+  memset(&tmp, 0, sizeof tmp);
+  D_TRY(tops_s1_annotation_read((adir + "/" + xmls[0]).c_str(), &tmp, &first));
+  D_TRY(tops_s1_orbit_read(orbit.c_str(), first.first_line_utc, first.last_line_utc, &P.info,
+                           nullptr));
+  int gl = 0, gp = 0;
+  D_TRY(tops_s1_geogrid_read((adir + "/" + xml).c_str(), 0, nullptr, nullptr, nullptr, nullptr,
+                             nullptr, &gl, &gp));
+  const size_t ng = (size_t)gl * gp;
+  P.az.resize(ng);
+  P.rg.resize(ng);
+  P.lat.resize(ng);
+  P.lon.resize(ng);
+  D_TRY(tops_s1_geogrid_read((adir + "/" + xml).c_str(), (int)ng, P.az.data(), P.rg.data(),
+                             P.lat.data(), P.lon.data(), nullptr, &gl, &gp));
+  P.geo_lines = gl;
+  P.geo_points = gp;
+  // the measurement raster of the same name
+  const std::string stem = xml.substr(0, xml.size() - 4);
+  std::string tif;
+  for (const std::string &n : list_files(mdir, stem, {".tiff", ".tif"})) tif = n;
+  if (tif.empty()) return TOPS_E_CONFIG;
+  const std::string tpath = mdir + "/" + tif;
+  int type = 0, w = 0, h = 0;
+  D_TRY(tops_tiff_read(tpath.c_str(), &type, &w, &h, nullptr, 0));
+  if (type != TOPS_TIFF_CINT16 || w != P.info.samples_per_burst ||
+      h < P.info.n_bursts * P.info.lines_per_burst)
+    return TOPS_E_CONFIG;
+  P.slc.resize((size_t)w * h * 2);
+  D_TRY(tops_tiff_read(tpath.c_str(), &type, &w, &h, P.slc.data(), P.slc.size() * 2));
+  P.slc_lines = h;
+  P.slc_samples = w;
+  return TOPS_OK;
+}
+
+// The DEM window of one burst: its lat/lon box extended by 24 DEM pixels,
+// as the reference's GeometricCoreg asks RefDem::getData for it
+// (Func.cpp:2240-2255, DataTypes.cpp:236-262).
+tops_dem_window dem_window(const tops_s1_annotation &a, int b, double lat_max, double lon_min,
+                           double dlat, double dlon) {
+  const double la0 = a.burst_lat_min[b] - 24 * dlat, la1 = a.burst_lat_max[b] + 24 * dlat;
+  const double lo0 = a.burst_lon_min[b] - 24 * dlon, lo1 = a.burst_lon_max[b] + 24 * dlon;
+  const double ul0 = floor((lat_max - la1) / dlat), ul1 = floor((lo0 - lon_min) / dlon);
+  const double lr0 = ceil((lat_max - la0) / dlat), lr1 = ceil((lo1 - lon_min) / dlon);
+  tops_dem_window w;
+  w.row0 = (int)ul0;
+  w.col0 = (int)ul1;
+  w.rows = (int)(lr0 - ul0 + 1);
+  w.cols = (int)(lr1 - ul1 + 1);
+  return w;
+}
+
+int run_subswath_product(const tops_config &c, int nsub, tops_run_stats *st) {
+  Product M, S;
+  D_TRY(load_product(c.masterpath, nsub, c.polarisation, c.preciseOrbitMaster, M));
+  D_TRY(load_product(c.slavepath, nsub, c.polarisation, c.preciseOrbitSlave, S));
+  const tops_s1_geogrid mg = {M.geo_lines, M.geo_points, M.az.data(), M.rg.data(), M.lat.data(),
+                              M.lon.data()};
+  const tops_s1_geogrid sg = {S.geo_lines, S.geo_points, S.az.data(), S.rg.data(), S.lat.data(),
+                              S.lon.data()};
+  int mb0 = 0, mbN = 0, sb0 = 0, sbN = 0;
+  D_TRY(tops_s1_burst_overlap(c.burst0, c.burstN, &M.info, &mg, &S.info, &sg, &mb0, &mbN, &sb0,
+                              &sbN));
+  const int k = mbN - mb0 + 1;
+  if (k < 1 || mbN >= M.info.n_bursts || sbN >= S.info.n_bursts || sbN - sb0 + 1 != k ||
+      M.info.lines_per_burst != S.info.lines_per_burst ||
+      M.info.samples_per_burst != S.info.samples_per_burst)
+    return TOPS_E_CONFIG;
+  // the DEM (int16 or float32 heights) and its geotransform
+  int type = 0, w = 0, h = 0;
+  D_TRY(tops_tiff_read(c.SpecificDemPath, &type, &w, &h, nullptr, 0));
+  if (type != TOPS_TIFF_INT16 && type != TOPS_TIFF_FLOAT32) return TOPS_E_CONFIG;
+  double gt[6];
+  D_TRY(tops_tiff_georef(c.SpecificDemPath, gt));
+  std::vector<float> dem((size_t)w * h);
+  if (type == TOPS_TIFF_INT16) {
+    std::vector<int16_t> raw((size_t)w * h);
+    D_TRY(tops_tiff_read(c.SpecificDemPath, &type, &w, &h, raw.data(), raw.size() * 2));
+    for (size_t i = 0; i < raw.size(); i++) dem[i] = raw[i];
+  } else {
+    D_TRY(tops_tiff_read(c.SpecificDemPath, &type, &w, &h, dem.data(), dem.size() * 4));
+  }
+  // RefDem::Init (DataTypes.cpp:200-222): upper-left corner and spacings
+  const double lat_max = gt[3], lon_min = gt[0], dlat = fabs(gt[5]), dlon = fabs(gt[1]);
+  PairInputs in;
+  in.m = sub_swath(M.info, mb0, k);
+  in.s = sub_swath(S.info, sb0, k);
+  in.k = k;
+  in.dem = dem.data();
+  in.dem_lines = h;
+  in.dem_pixels = w;
+  in.lat0 = lat_max;
+  in.lon0 = lon_min;
+  in.dlat = dlat;
+  in.dlon = dlon;
+  const int L = M.info.lines_per_burst, W = M.info.samples_per_burst;
+  for (int i = 0; i < k; i++) {
+    in.win.push_back(dem_window(M.ann, mb0 + i, lat_max, lon_min, dlat, dlon));
+    in.first_valid.push_back(M.ann.first_valid_line[mb0 + i]);
+    in.last_valid.push_back(M.ann.last_valid_line[mb0 + i]);
+  }
+  in.ms = M.slc.data() + (size_t)mb0 * L * W * 2;
+  in.ss = S.slc.data() + (size_t)sb0 * L * W * 2;
+  return process_pair(c, nsub, st, in);
+}
+
+int process_pair(const tops_config &c, int nsub, tops_run_stats *st, const PairInputs &in) {
+  const tops_swath_info &m = in.m, &s = in.s;
+  const int k = in.k, L = m.lines_per_burst, W = m.samples_per_burst;
   auto t0 = std::chrono::steady_clock::now();
   tops_pair_opts o;
   D_TRY(tops_pair_opts_default(&o));
@@ -110,9 +313,10 @@ int run_subswath(const tops_config &c, int nsub, tops_run_stats *st) {
   o.esd_threshold = (float)c.esd_coh_threshold;
   o.reslave_full = 1;
   Plan plan;
-  D_TRY(tops_pair_create(&m, &s, &o, di.lines, di.pixels, &plan.p));
-  D_TRY(tops_pair_set_dem(plan.p, dem, di.lat0, di.lon0, di.dlat, di.dlon, win.data(), nullptr));
-  D_TRY(tops_pair_upload(plan.p, ms, ss, nullptr));
+  D_TRY(tops_pair_create(&m, &s, &o, in.dem_lines, in.dem_pixels, &plan.p));
+  D_TRY(tops_pair_set_dem(plan.p, in.dem, in.lat0, in.lon0, in.dlat, in.dlon, in.win.data(),
+                          nullptr));
+  D_TRY(tops_pair_upload(plan.p, in.ms, in.ss, nullptr));
   D_TRY(tops_pair_run(plan.p, nullptr));
   const size_t n = (size_t)k * L * W;
   std::vector<float> reslave(2 * n), reslave_esd(2 * n), coh(n);
@@ -130,12 +334,11 @@ int run_subswath(const tops_config &c, int nsub, tops_run_stats *st) {
   D_TRY(tops_tiff_write((dir + "/Coh" + tag).c_str(), TOPS_TIFF_FLOAT32, W, k * L, coh.data(),
                         (size_t)W * 4));
   if (c.stitch) {
-    // every line of the synthetic bursts is valid
-    std::vector<int> fv(k, 0), lv(k, L - 1);
+    const int *fv = in.first_valid.data(), *lv = in.last_valid.data();
     int h = 0;
-    D_TRY(tops_stitch_line_map(&m, fv.data(), lv.data(), 0, k - 1, nullptr, 0, &h));
+    D_TRY(tops_stitch_line_map(&m, fv, lv, 0, k - 1, nullptr, 0, &h));
     std::vector<int> map(h);
-    D_TRY(tops_stitch_line_map(&m, fv.data(), lv.data(), 0, k - 1, map.data(), h, &h));
+    D_TRY(tops_stitch_line_map(&m, fv, lv, 0, k - 1, map.data(), h, &h));
     tops_pair_buffers b;
     D_TRY(tops_pair_buffers_get(plan.p, &b));
     int *d_map = nullptr;
@@ -179,7 +382,9 @@ extern "C" int tops_run_config(const char *config_path, tops_run_stats *stats) {
       c.n_bursts < 1 || c.n_bursts > TOPS_MAX_BURSTS)
     return TOPS_E_CONFIG;
   D_TRY(make_dir(c.process_dir));   // CheckDir (Main.cpp:26)
+  // products unless masterpath is empty or "(synthetic)"
+  const bool products = c.masterpath[0] != '\0' && strcmp(c.masterpath, "(synthetic)") != 0;
   for (int nsub = c.firstsubswath; nsub <= c.lastsubswath; nsub++)
-    D_TRY(run_subswath(c, nsub, stats));
+    D_TRY(products ? run_subswath_product(c, nsub, stats) : run_subswath(c, nsub, stats));
   return TOPS_OK;
 }

@@ -579,13 +579,42 @@ _proto("tops_pair_run_per_burst", C.c_int, [_vp, _vp])
 _proto("tops_stream_synchronize", C.c_int, [_vp])
 _proto("tops_tiff_write", C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, _vp, C.c_size_t])
 _proto("tops_tiff_read", C.c_int, [C.c_char_p, _ip, _ip, _ip, _vp, C.c_size_t])
-TIFF_TYPES = {1: (np.int16, 2), 2: (np.float32, 1), 3: (np.complex64, 1)}
+_proto("tops_tiff_georef", C.c_int, [C.c_char_p, _dp])
+_proto("tops_tiff_write_georef", C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, _vp,
+                                           C.c_size_t, _dp])
+TIFF_TYPES = {1: (np.int16, 2), 2: (np.float32, 1), 3: (np.complex64, 1), 4: (np.int16, 1)}
+
+
+def _tiff_type(a: np.ndarray) -> int:
+    if a.dtype == np.int16:
+        return 1 if a.ndim == 3 else 4
+    if a.dtype == np.float32:
+        return 2
+    if a.dtype == np.complex64:
+        return 3
+    raise TypeError(a.dtype)
+
+
+def tiff_georef(path: str) -> np.ndarray:
+    """GDAL-style geotransform of a GeoTIFF (tops_tiff_georef)."""
+    gt = np.zeros(6)
+    check(lib.tops_tiff_georef(str(path).encode(), ptr(gt, C.c_double)), "tops_tiff_georef")
+    return gt
+
+
+def tiff_write_georef(path: str, a: np.ndarray, gt) -> None:
+    """tiff_write with a north-up geotransform (e.g. a DEM)."""
+    a = np.ascontiguousarray(a)
+    g = np.ascontiguousarray(gt, np.float64)
+    check(lib.tops_tiff_write_georef(str(path).encode(), _tiff_type(a), a.shape[1], a.shape[0],
+                                     C.c_void_p(a.ctypes.data), a.strides[0], ptr(g, C.c_double)),
+          "tops_tiff_write_georef")
 
 
 def tiff_write(path: str, a: np.ndarray) -> None:
-    """CInt16 ([h][w][2] int16), float32 or complex64 [h][w] raster."""
+    """CInt16 ([h][w][2] int16), int16, float32 or complex64 [h][w] raster."""
     if a.dtype == np.int16:
-        t = 1
+        t = 1 if a.ndim == 3 else 4
     elif a.dtype == np.float32:
         t = 2
     elif a.dtype == np.complex64:

@@ -27,24 +27,28 @@ def g17(x: float) -> str:
 def grid_from_scene(scene, info, points: int = 11, first_burst: int = 0) -> dict:
     """A geolocation grid with one row per burst start and one after the
     last burst: azimuth times of the burst first lines (and the last burst's
-    last line), slant-range times across the swath, and the centre of each
-    burst's DEM window as latitude / longitude (the reference uses the grid
-    only to seed its range-Doppler solution, Func.cpp:1627-1640).  info may
-    hold the scene's bursts from first_burst on."""
+    last line), slant-range times across the swath, and latitude / longitude
+    running across each burst's DEM-window box from its north-west to its
+    south-east corner, so the per-burst boxes the reader derives cover the
+    bursts (the reference uses the grid for those boxes and to seed its
+    range-Doppler solution, Func.cpp:494-537, 1627-1640).  info may hold the
+    scene's bursts from first_burst on."""
     nb = info.n_bursts
     di = scene.dem_info
-    centres = []
+    boxes = []
     for b in range(nb):
         r0, c0, nr, nc = scene.dem_window(min(first_burst + b, scene.cfg.n_bursts - 1), 0)
-        centres.append((di.lat0 - (r0 + 0.5 * nr) * di.dlat, di.lon0 + (c0 + 0.5 * nc) * di.dlon))
-    centres.append(centres[-1])
+        boxes.append((di.lat0 - r0 * di.dlat, di.lat0 - (r0 + nr - 1) * di.dlat,
+                      di.lon0 + c0 * di.dlon, di.lon0 + (c0 + nc - 1) * di.dlon))
+    boxes.append(boxes[-1])
     az = [info.burst_first_line_time[b] for b in range(nb)] + [info.burst_last_line_time[nb - 1]]
     rg = info.slr_time + np.linspace(0.0, (info.samples_per_burst - 1) / (2.0 * info.rsr), points)
     lines = nb + 1
+    u = np.linspace(0.0, 1.0, points)
     g = {"az_time": np.repeat(np.array(az)[:, None], points, axis=1),
          "slr_time": np.repeat(rg[None, :], lines, axis=0),
-         "lat": np.repeat(np.array([c[0] for c in centres])[:, None], points, axis=1),
-         "lon": np.repeat(np.array([c[1] for c in centres])[:, None], points, axis=1),
+         "lat": np.array([b[0] + (b[1] - b[0]) * u for b in boxes]),
+         "lon": np.array([b[2] + (b[3] - b[2]) * u for b in boxes]),
          "incidence": np.repeat(np.linspace(30.0, 46.0, points)[None, :], lines, axis=0),
          "line": np.repeat(np.arange(lines)[:, None] * info.lines_per_burst, points, axis=1)}
     return g

@@ -97,3 +97,41 @@ def test_refuses_compressed_and_unknown(T, tmp_path):
         T.tiff_read(tmp_path / "missing.tif")
     with pytest.raises(TypeError):
         T.tiff_write(tmp_path / "x.tif", np.zeros((2, 2), np.float64))
+
+
+def test_int16_and_georef_round_trip(T, tmp_path):
+    """An int16 raster with a north-up geotransform (a DEM) reads back with
+    the geotransform GDAL would give it."""
+    a = (np.arange(30 * 41).reshape(30, 41) - 700).astype(np.int16)
+    gt = [10.5, 1 / 3600, 0.0, 45.25, 0.0, -1 / 3600]
+    p = tmp_path / "dem.tif"
+    T.tiff_write_georef(p, a, gt)
+    assert np.array_equal(T.tiff_read(p), a)
+    assert np.array_equal(T.tiff_georef(p), np.array(gt))
+    f = np.random.default_rng(1).normal(0, 300, (17, 23)).astype(np.float32)
+    T.tiff_write_georef(tmp_path / "f.tif", f, gt)
+    assert np.array_equal(T.tiff_read(tmp_path / "f.tif"), f)
+
+
+def test_georef_pixel_is_point(T, tmp_path):
+    """A PixelIsPoint raster's origin moves half a pixel up and left, as
+    GDAL reports it (GTRasterTypeGeoKey 1025 = 2)."""
+    a = np.zeros((8, 8), np.int16)
+    gt = [10.0, 0.5, 0.0, 40.0, 0.0, -0.25]
+    p = tmp_path / "pt.tif"
+    T.tiff_write_georef(p, a, gt)
+    raw = bytearray(p.read_bytes())
+    key = np.array([1025, 0, 1, 1], "<u2").tobytes()
+    i = raw.index(key)
+    raw[i:i + 8] = np.array([1025, 0, 1, 2], "<u2").tobytes()
+    p.write_bytes(bytes(raw))
+    assert np.allclose(T.tiff_georef(p), [10.0 - 0.25, 0.5, 0.0, 40.0 + 0.125, 0.0, -0.25])
+
+
+def test_georef_refusals(T, tmp_path):
+    a = np.zeros((4, 4), np.float32)
+    T.tiff_write(tmp_path / "plain.tif", a)
+    with pytest.raises(T.TopsError):
+        T.tiff_georef(tmp_path / "plain.tif")
+    with pytest.raises(T.TopsError):   # south-up or rotated transforms are not written
+        T.tiff_write_georef(tmp_path / "x.tif", a, [0, 1, 0, 0, 0, 1])
