@@ -316,10 +316,9 @@ extern "C" int tops_tiff_georef(const char *path, double gt[6]) {
       else if (tag == kTagTiepoint) ok = doubles(p, tie);
       else if (tag == kTagGeoKeys && in.val(p + 2, 2) == kShort) {
         const uint32_t cnt = in.val(p + 4, 4);
-        if (cnt < 4 || cnt > 4096) continue;
+        if (cnt < 4 || cnt > 4096) continue;   // 4 or more shorts: stored at an offset
         std::vector<uint8_t> raw((size_t)cnt * 2);
-        const uint32_t off = cnt * 2 <= 4 ? 0 : in.val(p + 8, 4);
-        if (!in.read(off, raw.data(), raw.size())) continue;
+        if (!in.read(in.val(p + 8, 4), raw.data(), raw.size())) continue;
         const uint32_t nkeys = in.val(raw.data() + 6, 2);
         for (uint32_t k = 0; k < nkeys && 4 + 4 * k + 3 < cnt; k++) {
           const uint8_t *q = raw.data() + 8 * (k + 1);
