@@ -82,12 +82,17 @@ int batch_resample(tops_batch *B, bool esd_pass, int *counters, cudaStream_t st)
   for (size_t p = 0; p < B->pairs.size(); p++) {
     const tops_pair *P = B->pairs[p];
     const size_t n0 = jobs.size();
-    if (esd_pass)
+    if (esd_pass) {
       pair_rs2_jobs(P, B->d_shift + B->ov_begin[p], jobs);
-    else
+      // the first burst's ReSlaveESD copied from its ReSlave (or resampled
+      // as it, without the full ReSlave)
+      const int skip = pair_first_burst_copy(P, st);
+      if (skip < 0) return TOPS_E_CUDA;
+      if (skip) jobs.erase(jobs.begin() + (long)n0);
+    } else {
       pair_rs1_jobs(P, jobs);
+    }
     luts.resize(jobs.size(), P->lut);
-    (void)n0;
   }
   if (jobs.empty()) return TOPS_OK;
   return tops::resample_launch_multi(luts.data(), jobs.data(), (int)jobs.size(), B->o.precision,

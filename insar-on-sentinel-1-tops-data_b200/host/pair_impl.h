@@ -101,6 +101,7 @@ int pair_bind_dem(tops_pair *P, const float *d_dem, size_t dem_pitch, int dem_li
 // shifts, one per overlap.
 void pair_rs1_jobs(const tops_pair *P, std::vector<tops_resample_job> &jobs);
 void pair_esd_overlaps(const tops_pair *P, std::vector<tops_esd_overlap> &ovs);
+int pair_first_burst_copy(const tops_pair *P, cudaStream_t st);
 void pair_rs2_jobs(const tops_pair *P, const double *shifts,
                    std::vector<tops_resample_job> &jobs);
 void pair_coh_jobs(const tops_pair *P, std::vector<tops_coh_job> &cj);

@@ -410,7 +410,13 @@ void pair_esd_overlaps(const tops_pair *P, std::vector<tops_esd_overlap> &ovs) {
   }
 }
 
-// shifts: the device ESD shifts of this pair's overlaps
+// shifts: the device ESD shifts of this pair's overlaps.  One job per burst.
+// The first burst's ReSlaveESD is its ReSlave (the reference copies it,
+// ResampleFirstBurst, Func.cpp:2653-2674): its job is the ReSlave job (slave
+// interval, no shift), so its output equals that burst's ReSlave bit for
+// bit; pair_first_burst_copy replaces it by a copy when the full ReSlave is
+// computed.  Later bursts: the ESD shift of the overlap before them and the
+// master's interval, as DerampDemodResample_ESD gets it (Func.cpp:2704).
 void pair_rs2_jobs(const tops_pair *P, const double *shifts,
                    std::vector<tops_resample_job> &jobs) {
   const int nb = P->nb, L = P->L;
@@ -418,10 +424,28 @@ void pair_rs2_jobs(const tops_pair *P, const double *shifts,
     tops_resample_job j = base_job(P, b);
     j.out = P->d_res_esd + (size_t)b * L * P->cplx_pitch;
     j.out_rows = -1;
-    if (b > 0) j.az_shift_dev = shifts + (b - 1);
-    j.dt = P->m.dt;   // DerampDemodResample_ESD gets the master's interval (Func.cpp:2704)
+    if (b > 0) {
+      j.az_shift_dev = shifts + (b - 1);
+      j.dt = P->m.dt;
+    }
     jobs.push_back(j);
   }
+}
+
+// With the full ReSlave computed: the first burst's ReSlaveESD copied from
+// it (device to device, on the stream after the ReSlave resample); returns
+// 1 when the copy is enqueued (the caller then skips the first rs2 job), 0
+// when that job must run, or a negative CUDA error.
+int pair_first_burst_copy(const tops_pair *P, cudaStream_t st) {
+  if (!P->o.reslave_full) return 0;
+  const cudaError_t e =
+      cudaMemcpy2DAsync(P->d_res_esd, P->cplx_pitch, P->d_reslave, P->cplx_pitch,
+                        (size_t)P->W * 8, P->L, cudaMemcpyDeviceToDevice, st);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    return -1;
+  }
+  return 1;
 }
 
 void pair_coh_jobs(const tops_pair *P, std::vector<tops_coh_job> &cj) {
@@ -470,8 +494,14 @@ int tops_pair_run(tops_pair *P, void *stream) {
   //    uncorrected, Func.cpp:2653-2702)
   jobs.clear();
   pair_rs2_jobs(P, P->d_shift, jobs);
-  P_TRY(tops_resample_ex(P->lut, jobs.data(), nb, P->o.precision, stream));
-  launches += 1;
+  {
+    const int skip = pair_first_burst_copy(P, static_cast<cudaStream_t>(stream));
+    if (skip < 0) return TOPS_E_CUDA;
+    if (nb - skip > 0) {
+      P_TRY(tops_resample_ex(P->lut, jobs.data() + skip, nb - skip, P->o.precision, stream));
+      launches += 1;
+    }
+  }
   // 5. coherence of master vs ReSlaveESD
   std::vector<tops_coh_job> cj;
   pair_coh_jobs(P, cj);
@@ -515,7 +545,15 @@ int tops_pair_stage_times(tops_pair *P, void *stream, float *ms) {
     cudaEventRecord(ev[3], st);
     jobs.clear();
     pair_rs2_jobs(P, P->d_shift, jobs);
-    if ((r = tops_resample_ex(P->lut, jobs.data(), nb, P->o.precision, stream)) != TOPS_OK) break;
+    const int skip = pair_first_burst_copy(P, st);
+    if (skip < 0) {
+      r = TOPS_E_CUDA;
+      break;
+    }
+    if (nb - skip > 0 &&
+        (r = tops_resample_ex(P->lut, jobs.data() + skip, nb - skip, P->o.precision, stream)) !=
+            TOPS_OK)
+      break;
     cudaEventRecord(ev[4], st);
     pair_coh_jobs(P, cj);
     if ((r = tops_coherence(cj.data(), nb, P->o.win_rg, P->o.win_az, stream)) != TOPS_OK) break;
