@@ -30,5 +30,19 @@ int resample_launch_multi(const tops_lut_dev *const *luts, const tops_resample_j
                           int njobs, int precision, const TileCfg &cfg, cudaStream_t st);
 int coherence_launch(const tops_coh_job *jobs, int njobs, int win_rg, int win_az,
                      const TileCfg &cfg, cudaStream_t st);
+// Same-device 2-D copies (dst row i = src row i) with the debursting gather
+// kernel, several in one launch (blockIdx.y picks the copy): HBM speed,
+// where the copy engine reaches about a third of it.  Pitches and row_bytes
+// as tops_stitch takes them.
+struct RowCopy {
+  const void *src;
+  size_t src_pitch;
+  void *dst;
+  size_t dst_pitch;
+  size_t row_bytes;
+  int height;
+};
+// One launch per 16 copies; *launches (if non-null) counts them.
+int row_copy(const RowCopy *copies, int n, cudaStream_t st, int *launches);
 
 }  // namespace tops

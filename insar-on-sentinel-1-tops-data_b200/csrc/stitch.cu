@@ -4,11 +4,13 @@
 //
 // HBM-bound copy: one CTA per few output rows; threads move 16-byte vectors
 // when both images' bases and pitches allow it, else 4-byte words.  The map
-// comes from tops_stitch_line_map.
+// comes from tops_stitch_line_map.  tops::row_copy runs the same loop
+// without a map (row i copies row i) over several images in one launch.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include "common.cuh"
+#include "launch.h"
 
 namespace tops {
 
@@ -26,6 +28,55 @@ __global__ void __launch_bounds__(ST_NT) stitch_kernel(const char *__restrict__ 
     V *d = reinterpret_cast<V *>(dst + (size_t)r * dp);
     for (int i = threadIdx.x; i < nvec; i += ST_NT) d[i] = __ldg(s + i);
   }
+}
+
+constexpr int RC_MAX = 16;   // copies per row_copy launch
+struct RowCopies {
+  RowCopy c[RC_MAX];
+};
+
+template <typename V>
+__global__ void __launch_bounds__(ST_NT) row_copy_kernel(const RowCopies cs) {
+  const RowCopy &c = cs.c[blockIdx.y];
+  const int nvec = (int)(c.row_bytes / sizeof(V));
+  const int r0 = blockIdx.x * ST_ROWS;
+  for (int r = r0; r < r0 + ST_ROWS && r < c.height; r++) {
+    const V *s = reinterpret_cast<const V *>(static_cast<const char *>(c.src) + (size_t)r * c.src_pitch);
+    V *d = reinterpret_cast<V *>(static_cast<char *>(c.dst) + (size_t)r * c.dst_pitch);
+    for (int i = threadIdx.x; i < nvec; i += ST_NT) d[i] = __ldg(s + i);
+  }
+}
+
+int row_copy(const RowCopy *copies, int n, cudaStream_t st, int *launches) {
+  if (n < 0 || (n > 0 && !copies)) return TOPS_E_INVALID;
+  for (int k = 0; k < n; k++) {
+    const RowCopy &c = copies[k];
+    if (!c.src || !c.dst || c.height < 0 || c.row_bytes == 0 || (c.row_bytes & 3) ||
+        c.src_pitch < c.row_bytes || c.dst_pitch < c.row_bytes || ((c.src_pitch | c.dst_pitch) & 3))
+      return TOPS_E_INVALID;
+  }
+  for (int k0 = 0; k0 < n; k0 += RC_MAX) {
+    RowCopies cs = {};
+    int rows = 0, m = 0;
+    uintptr_t bits = 0;
+    for (int k = k0; k < n && k < k0 + RC_MAX; k++) {
+      const RowCopy &c = copies[k];
+      if (c.height == 0) continue;
+      cs.c[m++] = c;
+      rows = c.height > rows ? c.height : rows;
+      bits |= reinterpret_cast<uintptr_t>(c.src) | reinterpret_cast<uintptr_t>(c.dst) |
+              c.src_pitch | c.dst_pitch | c.row_bytes;
+    }
+    if (m == 0) continue;
+    const dim3 grid((rows + ST_ROWS - 1) / ST_ROWS, m);
+    if (!(bits & 15))
+      row_copy_kernel<int4><<<grid, ST_NT, 0, st>>>(cs);
+    else
+      row_copy_kernel<int><<<grid, ST_NT, 0, st>>>(cs);
+    TOPS_CUDA_TRY(cudaGetLastError());
+    if (launches) *launches += 1;
+  }
+  return TOPS_OK;
 }
 
 }  // namespace tops

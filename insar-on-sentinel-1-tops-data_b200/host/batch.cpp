@@ -75,25 +75,35 @@ tops::TileCfg tile(int seg_rows, int persistent, int *counters) {
   return c;
 }
 
+int chunks(size_t n, int per) { return (int)((n + per - 1) / per); }
+
 // The resample stage of all pairs as one launch (chunked per 32 jobs).
-int batch_resample(tops_batch *B, bool esd_pass, int *counters, cudaStream_t st) {
+int batch_resample(tops_batch *B, bool esd_pass, int *counters, cudaStream_t st, int *launches) {
   std::vector<tops_resample_job> jobs;
   std::vector<const tops_lut_dev *> luts;
+  std::vector<tops::RowCopy> copies;
   for (size_t p = 0; p < B->pairs.size(); p++) {
     const tops_pair *P = B->pairs[p];
     const size_t n0 = jobs.size();
     if (esd_pass) {
       pair_rs2_jobs(P, B->d_shift + B->ov_begin[p], jobs);
       // the first burst's ReSlaveESD copied from its ReSlave (or resampled
-      // as it, without the full ReSlave)
-      const int skip = pair_first_burst_copy(P, st);
-      if (skip < 0) return TOPS_E_CUDA;
-      if (skip) jobs.erase(jobs.begin() + (long)n0);
+      // as it, without the full ReSlave): one copy launch for all pairs
+      tops::RowCopy c;
+      if (pair_first_burst_copy(P, &c)) {
+        copies.push_back(c);
+        jobs.erase(jobs.begin() + (long)n0);
+      }
     } else {
       pair_rs1_jobs(P, jobs);
     }
     luts.resize(jobs.size(), P->lut);
   }
+  if (!copies.empty()) {
+    const int r = tops::row_copy(copies.data(), (int)copies.size(), st, launches);
+    if (r != TOPS_OK) return r;
+  }
+  *launches += chunks(jobs.size(), 32);
   if (jobs.empty()) return TOPS_OK;
   return tops::resample_launch_multi(luts.data(), jobs.data(), (int)jobs.size(), B->o.precision,
                                      tile(B->tune.rs_seg_rows, B->tune.rs_persistent, counters),
@@ -107,7 +117,6 @@ int batch_coherence(tops_batch *B, int *counters, cudaStream_t st) {
                                 tile(B->tune.coh_seg_rows, B->tune.coh_persistent, counters), st);
 }
 
-int chunks(size_t n, int per) { return (int)((n + per - 1) / per); }
 
 }  // namespace
 
@@ -200,8 +209,7 @@ int tops_batch_run(tops_batch *B, void *stream) {
     n_rs1 = tmp.size();
   }
   int *ctr = B->d_counters;
-  B_TRY(batch_resample(B, false, ctr, st));
-  launches += chunks(n_rs1, 32);
+  B_TRY(batch_resample(B, false, ctr, st, &launches));
   ctr += chunks(n_rs1, 32);
   // 3. ESD over all overlaps; every pair's shifts are also copied into its
   //    own plan (tops_pair_download reads them there)
@@ -221,8 +229,7 @@ int tops_batch_run(tops_batch *B, void *stream) {
   // 4. resample with the ESD shifts
   size_t n_rs2 = 0;
   for (tops_pair *P : B->pairs) n_rs2 += P->nb;
-  B_TRY(batch_resample(B, true, ctr, st));
-  launches += chunks(n_rs2, 32);
+  B_TRY(batch_resample(B, true, ctr, st, &launches));
   ctr += chunks(n_rs2, 32);
   // 5. coherence
   B_TRY(batch_coherence(B, ctr, st));
@@ -286,11 +293,11 @@ int tops_batch_autotune(tops_batch *B, void *stream, tops_tune *best, double *be
     const tops_tune keep = B->tune;
     B->tune = t;
     float acc = 0.f;
-    int s = TOPS_OK;
+    int s = TOPS_OK, launches = 0;
     for (int rep = 0; rep < 3 && s == TOPS_OK; rep++) {   // rep 0 warms up
       if (cudaEventRecord(e0, st) != cudaSuccess) s = TOPS_E_CUDA;
       if (s == TOPS_OK)
-        s = resample ? batch_resample(B, true, B->d_counters, st)
+        s = resample ? batch_resample(B, true, B->d_counters, st, &launches)
                      : batch_coherence(B, B->d_counters, st);
       if (s == TOPS_OK && cudaEventRecord(e1, st) != cudaSuccess) s = TOPS_E_CUDA;
       if (s == TOPS_OK && cudaEventSynchronize(e1) != cudaSuccess) s = TOPS_E_CUDA;

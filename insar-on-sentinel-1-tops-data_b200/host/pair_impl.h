@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "arena.h"
+#include "launch.h"
 #include "tops_pipeline.h"
 
 inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
@@ -101,7 +102,10 @@ int pair_bind_dem(tops_pair *P, const float *d_dem, size_t dem_pitch, int dem_li
 // shifts, one per overlap.
 void pair_rs1_jobs(const tops_pair *P, std::vector<tops_resample_job> &jobs);
 void pair_esd_overlaps(const tops_pair *P, std::vector<tops_esd_overlap> &ovs);
-int pair_first_burst_copy(const tops_pair *P, cudaStream_t st);
+// With the full ReSlave computed, the first burst's ReSlaveESD is a copy of
+// its ReSlave: fills *c and returns 1 (the first rs2 job is then skipped);
+// else 0.
+int pair_first_burst_copy(const tops_pair *P, tops::RowCopy *c);
 void pair_rs2_jobs(const tops_pair *P, const double *shifts,
                    std::vector<tops_resample_job> &jobs);
 void pair_coh_jobs(const tops_pair *P, std::vector<tops_coh_job> &cj);

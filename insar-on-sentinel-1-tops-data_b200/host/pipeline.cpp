@@ -432,19 +432,9 @@ void pair_rs2_jobs(const tops_pair *P, const double *shifts,
   }
 }
 
-// With the full ReSlave computed: the first burst's ReSlaveESD copied from
-// it (device to device, on the stream after the ReSlave resample); returns
-// 1 when the copy is enqueued (the caller then skips the first rs2 job), 0
-// when that job must run, or a negative CUDA error.
-int pair_first_burst_copy(const tops_pair *P, cudaStream_t st) {
+int pair_first_burst_copy(const tops_pair *P, tops::RowCopy *c) {
   if (!P->o.reslave_full) return 0;
-  const cudaError_t e =
-      cudaMemcpy2DAsync(P->d_res_esd, P->cplx_pitch, P->d_reslave, P->cplx_pitch,
-                        (size_t)P->W * 8, P->L, cudaMemcpyDeviceToDevice, st);
-  if (e != cudaSuccess) {
-    (void)cudaGetLastError();
-    return -1;
-  }
+  *c = {P->d_reslave, P->cplx_pitch, P->d_res_esd, P->cplx_pitch, (size_t)P->W * 8, P->L};
   return 1;
 }
 
@@ -495,8 +485,9 @@ int tops_pair_run(tops_pair *P, void *stream) {
   jobs.clear();
   pair_rs2_jobs(P, P->d_shift, jobs);
   {
-    const int skip = pair_first_burst_copy(P, static_cast<cudaStream_t>(stream));
-    if (skip < 0) return TOPS_E_CUDA;
+    tops::RowCopy c;
+    const int skip = pair_first_burst_copy(P, &c);
+    if (skip) P_TRY(tops::row_copy(&c, 1, static_cast<cudaStream_t>(stream), &launches));
     if (nb - skip > 0) {
       P_TRY(tops_resample_ex(P->lut, jobs.data() + skip, nb - skip, P->o.precision, stream));
       launches += 1;
@@ -545,11 +536,9 @@ int tops_pair_stage_times(tops_pair *P, void *stream, float *ms) {
     cudaEventRecord(ev[3], st);
     jobs.clear();
     pair_rs2_jobs(P, P->d_shift, jobs);
-    const int skip = pair_first_burst_copy(P, st);
-    if (skip < 0) {
-      r = TOPS_E_CUDA;
-      break;
-    }
+    tops::RowCopy c;
+    const int skip = pair_first_burst_copy(P, &c);
+    if (skip && (r = tops::row_copy(&c, 1, st, nullptr)) != TOPS_OK) break;
     if (nb - skip > 0 &&
         (r = tops_resample_ex(P->lut, jobs.data() + skip, nb - skip, P->o.precision, stream)) !=
             TOPS_OK)

@@ -57,8 +57,9 @@ def test_batch_equals_single_pairs(T, scenes):
     plans = [_plan(T, S) for S in scenes]
     B = T.Batch(plans)
     B.run(graph=True)
-    # 2 geocoreg + 2 resample + 2 ESD + 1 coherence launches for all 7 bursts
-    assert B.launches() == 7
+    # 2 geocoreg + 2 resample + 2 ESD + 1 coherence launches for all 7 bursts,
+    # and 1 copy of the 3 first bursts' ReSlave into ReSlaveESD
+    assert B.launches() == 8
     for P, ref in zip(plans, alone):
         _same(_outputs(P), ref)
     B.close()
