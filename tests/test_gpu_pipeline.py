@@ -99,6 +99,10 @@ def test_pipeline_overlap_bands_only(T, scene_esd):
     b = run_pair(T, scene_esd, reslave_full=0)
     for k in ("reslave_esd", "coh", "cpm", "shifts"):
         assert np.array_equal(a[k], b[k]), k
+    # the first burst's ReSlaveESD is its ReSlave: copied in a, resampled with
+    # the slave's interval in b
+    L = scene_esd.swath[0].lines_per_burst
+    assert np.array_equal(a["reslave_esd"][:L], a["reslave"][:L])
 
 
 def test_plain_form_equals_pipeline(T, scene_esd):
