@@ -230,7 +230,8 @@ def run_reference(args, rank, world):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded)",
             "config": {"workload": workload_name(args.config, cfg),
-                       "window": f"{WIN_RG}x{WIN_AZ}", "step": "one burst pair"},
+                       "window": f"{WIN_RG}x{WIN_AZ}"},
+            "form": "CPU FP64 port, one burst pair per step",
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cp.threads, "kind": "port",
                              "sample": cp.describe(len(times))},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
@@ -728,8 +729,9 @@ def main():
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 geometry)",
         "data": "synthetic (seeded); inputs > L2, no flush needed",
         "config": {"workload": workload_name(args.config, cfg),
-                   "window": f"{WIN_RG}x{WIN_AZ}", "form": "device-resident batched, CUDA graph",
-                   "l2": "inputs larger than L2 (no flush)"},
+                   "window": f"{WIN_RG}x{WIN_AZ}"},
+        "form": "device-resident batched, CUDA graph",
+        "l2": "inputs larger than L2 (no flush)",
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_step_ms,
                 "form": "tops_pair_process (per-burst copy/compute pipeline)",

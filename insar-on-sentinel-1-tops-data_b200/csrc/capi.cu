@@ -35,14 +35,22 @@ int launch_geocoreg(const GeoJob *jobs, int njobs, bool dem_is_int, void *scratc
                     size_t scratch_bytes, cudaStream_t st);
 size_t geocoreg_scratch(const GeoJob *J, int n);
 
-// Grow-only per-thread device workspace with named slots.
+// Grow-only device workspace with named slots, one per (host thread,
+// device): the entry points run on the calling thread's current device, so
+// buffers of another device are never handed to them.
 struct Workspace {
   enum { kSlots = 12 };
+  int dev = -1;
   void *ptr[kSlots] = {};
   size_t cap[kSlots] = {};
   ~Workspace() {
-    for (int i = 0; i < kSlots; i++)
-      if (ptr[i]) cudaFree(ptr[i]);
+    if (dev < 0) return;
+    int cur = -1;
+    const bool have_cur = cudaGetDevice(&cur) == cudaSuccess;
+    if (cudaSetDevice(dev) == cudaSuccess)
+      for (int i = 0; i < kSlots; i++)
+        if (ptr[i]) cudaFree(ptr[i]);
+    if (have_cur) cudaSetDevice(cur);
   }
   int get(int slot, size_t bytes, void **out) {
     if (bytes == 0) bytes = 16;
@@ -61,7 +69,17 @@ struct Workspace {
     return TOPS_OK;
   }
 };
-static thread_local Workspace g_ws;
+static thread_local Workspace g_ws_dev[kMaxDevices];
+
+// The workspace of the calling thread on its current device.
+static int workspace(Workspace **out) {
+  int dev = -1;
+  TOPS_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return TOPS_E_INVALID;
+  g_ws_dev[dev].dev = dev;
+  *out = &g_ws_dev[dev];
+  return TOPS_OK;
+}
 
 static inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
@@ -72,28 +90,38 @@ static inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; 
   } while (0)
 
 struct LutScratch {
+  int dev = -1;
   tops_lut_dev *lut = nullptr;
   std::vector<float> kaz, krg;
   ~LutScratch() {
-    if (lut) tops_lut_destroy(lut);
+    if (!lut) return;
+    int cur = -1;
+    const bool have_cur = cudaGetDevice(&cur) == cudaSuccess;
+    if (cudaSetDevice(dev) == cudaSuccess) tops_lut_destroy(lut);
+    if (have_cur) cudaSetDevice(cur);
   }
 };
-static thread_local LutScratch g_lut;
+static thread_local LutScratch g_lut_dev[kMaxDevices];
 
 // The reference passes its host LUT on every call; keep one device copy per
-// thread and refresh it when the caller's table changes.
+// (thread, device) and refresh it when the caller's table changes.
 static int lut_for(const float *kaz, const float *krg, int npoints, tops_lut_dev **out) {
   if (npoints != kTaps) return TOPS_E_INVALID;
+  int dev = -1;
+  TOPS_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return TOPS_E_INVALID;
+  LutScratch &g = g_lut_dev[dev];
+  g.dev = dev;
   const size_t n = (size_t)kLutBins * kTaps;
-  if (!g_lut.lut || memcmp(g_lut.kaz.data(), kaz, n * sizeof(float)) ||
-      memcmp(g_lut.krg.data(), krg, n * sizeof(float))) {
-    if (g_lut.lut) tops_lut_destroy(g_lut.lut);
-    g_lut.lut = nullptr;
-    TOPS_TRY(tops_lut_create(kaz, krg, &g_lut.lut));
-    g_lut.kaz.assign(kaz, kaz + n);
-    g_lut.krg.assign(krg, krg + n);
+  if (!g.lut || memcmp(g.kaz.data(), kaz, n * sizeof(float)) ||
+      memcmp(g.krg.data(), krg, n * sizeof(float))) {
+    if (g.lut) tops_lut_destroy(g.lut);
+    g.lut = nullptr;
+    TOPS_TRY(tops_lut_create(kaz, krg, &g.lut));
+    g.kaz.assign(kaz, kaz + n);
+    g.krg.assign(krg, krg + n);
   }
-  *out = g_lut.lut;
+  *out = g.lut;
   return TOPS_OK;
 }
 
@@ -115,13 +143,15 @@ static int resample_host(void *SlaveArray, const double *CpmAz, const double *Cp
   if (SlaveBox[0] < 0 || SlaveBox[1] >= SamplesPerBurst) return TOPS_E_INVALID;
   tops_lut_dev *lut;
   TOPS_TRY(lut_for(KernelAz, KernelRg, Npoints, &lut));
+  Workspace *ws;
+  TOPS_TRY(workspace(&ws));
   cudaStream_t st = cudaStreamPerThread;
   const size_t spitch = align_up((size_t)sPixels * 4, 256);
   const size_t opitch = align_up((size_t)mPixels * 8, 256);
   void *d_slave, *d_out, *d_par;
-  TOPS_TRY(g_ws.get(0, spitch * sLines, &d_slave));
-  TOPS_TRY(g_ws.get(1, opitch * mLines, &d_out));
-  TOPS_TRY(g_ws.get(2, 3 * sizeof(double) * (size_t)SamplesPerBurst, &d_par));
+  TOPS_TRY(ws->get(0, spitch * sLines, &d_slave));
+  TOPS_TRY(ws->get(1, opitch * mLines, &d_out));
+  TOPS_TRY(ws->get(2, 3 * sizeof(double) * (size_t)SamplesPerBurst, &d_par));
   double *d_kt = static_cast<double *>(d_par), *d_tref = d_kt + SamplesPerBurst,
          *d_fdc = d_tref + SamplesPerBurst;
   TOPS_CUDA_TRY(cudaMemcpy2DAsync(d_slave, spitch, SlaveArray, (size_t)sPixels * 4,
@@ -179,8 +209,10 @@ static int coherence_host(int Dw, int Dh, int dx, int dy, int winRg, int winAz,
   cudaStream_t st = cudaStreamPerThread;
   const size_t mpitch = align_up((size_t)Dw * 4, 256), cpitch = align_up((size_t)Dw * 4, 256);
   void *d_m, *d_c;
-  TOPS_TRY(g_ws.get(3, mpitch * Dh, &d_m));
-  TOPS_TRY(g_ws.get(4, cpitch * Dh, &d_c));
+  Workspace *ws;
+  TOPS_TRY(workspace(&ws));
+  TOPS_TRY(ws->get(3, mpitch * Dh, &d_m));
+  TOPS_TRY(ws->get(4, cpitch * Dh, &d_c));
   TOPS_CUDA_TRY(cudaMemcpy2DAsync(d_m, mpitch, masterArray, (size_t)Dw * 4, (size_t)Dw * 4, Dh,
                                   cudaMemcpyHostToDevice, st));
   tops_coh_job j{d_m, mpitch, d_slave, (size_t)Dw * 8, static_cast<float *>(d_c), cpitch, Dh, Dw};
@@ -250,8 +282,10 @@ int GeoCoreg_warp_cuda(int m_burstIdx, int s_burstIdx, int xmin, int xmax, int y
   cudaStream_t st = cudaStreamPerThread;
   const size_t dpitch = align_up((size_t)DemPixels * 4, 256);
   void *d_dem, *d_out;
-  TOPS_TRY(g_ws.get(5, dpitch * DemLines, &d_dem));
-  TOPS_TRY(g_ws.get(6, 256, &d_out));
+  Workspace *ws;
+  TOPS_TRY(workspace(&ws));
+  TOPS_TRY(ws->get(5, dpitch * DemLines, &d_dem));
+  TOPS_TRY(ws->get(6, 256, &d_out));
   TOPS_CUDA_TRY(cudaMemcpy2DAsync(d_dem, dpitch, inputDEM, (size_t)DemPixels * 4,
                                   (size_t)DemPixels * 4, DemLines, cudaMemcpyHostToDevice, st));
   tops_geo_job g;
@@ -299,7 +333,7 @@ int GeoCoreg_warp_cuda(int m_burstIdx, int s_burstIdx, int xmin, int xmax, int y
   TOPS_TRY(fill_geo_job(g, J));
   void *d_scr;
   size_t scr = geocoreg_scratch(&J, 1);
-  TOPS_TRY(g_ws.get(7, scr, &d_scr));
+  TOPS_TRY(ws->get(7, scr, &d_scr));
   TOPS_TRY(launch_geocoreg(&J, 1, true, d_scr, scr, st));
   double h[13];
   TOPS_CUDA_TRY(cudaMemcpyAsync(h, d_cpm, 13 * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -392,9 +426,11 @@ int EstESDShifts(void *MasterFor, void *MasterBack, void *SlaveFor, void *SlaveB
   cudaStream_t st = cudaStreamPerThread;
   const size_t mbytes = (size_t)tot * ArrayPixels * 4, sbytes = (size_t)tot * ArrayPixels * 8;
   void *d_m, *d_s, *d_o;
-  TOPS_TRY(g_ws.get(8, 2 * mbytes, &d_m));
-  TOPS_TRY(g_ws.get(9, 2 * sbytes, &d_s));
-  TOPS_TRY(g_ws.get(10, sizeof(double) * 3 * (size_t)numOverlap, &d_o));
+  Workspace *ws;
+  TOPS_TRY(workspace(&ws));
+  TOPS_TRY(ws->get(8, 2 * mbytes, &d_m));
+  TOPS_TRY(ws->get(9, 2 * sbytes, &d_s));
+  TOPS_TRY(ws->get(10, sizeof(double) * 3 * (size_t)numOverlap, &d_o));
   char *mF = static_cast<char *>(d_m), *mB = mF + mbytes;
   char *sF = static_cast<char *>(d_s), *sB = sF + sbytes;
   TOPS_CUDA_TRY(cudaMemcpyAsync(mF, MasterFor, mbytes, cudaMemcpyHostToDevice, st));
@@ -420,7 +456,7 @@ int EstESDShifts(void *MasterFor, void *MasterBack, void *SlaveFor, void *SlaveB
   }
   size_t scr = esd_scratch_bytes(O.data(), numOverlap);
   void *d_scr;
-  TOPS_TRY(g_ws.get(11, scr, &d_scr));
+  TOPS_TRY(ws->get(11, scr, &d_scr));
   double *d_shift = static_cast<double *>(d_o);
   TOPS_TRY(launch_esd(O.data(), numOverlap, CohWinAz, CohWinRg, CohThresHold, d_shift, nullptr,
                       d_scr, scr, st));

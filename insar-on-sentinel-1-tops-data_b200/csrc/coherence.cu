@@ -266,15 +266,20 @@ static int launch_coh_t(const CoBatch &B, int grid, cudaStream_t st) {
 
 template <int WAZ, int WRG>
 static int coh_resident(int dev) {
-  static int resident[kMaxDevices] = {};
-  if (!resident[dev]) {
-    int per_sm = 0, sms = 0;
-    TOPS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm, coherence_kernel<WAZ, WRG>, CO_NT, 0));
-    TOPS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    resident[dev] = per_sm * sms;
-  }
-  return resident[dev];
+  static PerDeviceOnce setup;
+  int resident = 0;
+  const int s = once_per_device(
+      setup, dev,
+      [&](int &v) -> int {
+        int per_sm = 0, sms = 0;
+        TOPS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, coherence_kernel<WAZ, WRG>, CO_NT, 0));
+        TOPS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        v = per_sm * sms;
+        return TOPS_OK;
+      },
+      &resident);
+  return s == TOPS_OK ? resident : 0;
 }
 
 // The compiled (azimuth, range) windows: the config's 3 x 10 and the

@@ -4,6 +4,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+#include <mutex>
+
 #include "tops_b200.h"
 
 namespace tops {
@@ -34,6 +37,35 @@ constexpr int kMaxDevices = 64;
 constexpr double kTwoPiHi = 6.283185307179586232e+00;
 constexpr double kTwoPiLo = 2.449293598294706414e-16;
 constexpr double kInvTwoPi = 0.15915494309189533577;
+
+// ------------------------------------------- per-device one-time set-up
+// Function attributes and occupancy queries are per device.  The first host
+// thread that launches on a device runs init(value) under the lock and
+// publishes the positive value it produced; later callers read it without
+// locking.  A failed init is not published, so the next call retries it.
+struct PerDeviceOnce {
+  std::mutex mu;
+  std::atomic<int> value[kMaxDevices]{};
+};
+
+template <class F>
+int once_per_device(PerDeviceOnce &o, int dev, F init, int *out) {
+  if (dev < 0 || dev >= kMaxDevices) return TOPS_E_INVALID;
+  int v = o.value[dev].load(std::memory_order_acquire);
+  if (v == 0) {
+    std::lock_guard<std::mutex> lock(o.mu);
+    v = o.value[dev].load(std::memory_order_relaxed);
+    if (v == 0) {
+      int r = 1;
+      const int s = init(r);
+      if (s != TOPS_OK) return s;
+      v = r > 0 ? r : 1;
+      o.value[dev].store(v, std::memory_order_release);
+    }
+  }
+  if (out) *out = v;
+  return TOPS_OK;
+}
 
 // Cody-Waite reduction of a double phase to [-pi, pi] with a two-term 2*pi,
 // returned as float.  Exact to ~1e-15 rad for |phi| < 1e9.

@@ -343,16 +343,19 @@ int launch_esd(const EsdOverlap *ovs, int n_ov, int win_az, int win_rg, float th
   if (esd_scratch_bytes(ovs, n_ov) > scratch_bytes || (!scratch && n_ov > 0) || !shifts)
     return TOPS_E_INVALID;
   // the shared-memory opt-in is a per-device function attribute
-  static bool attr_done[kMaxDevices] = {};
+  static PerDeviceOnce setup;
   int dev = 0;
   TOPS_CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kMaxDevices) return TOPS_E_INVALID;
-  if (!attr_done[dev]) {
-    for (auto fn : {esd_kernel<3>, esd_kernel<6>, esd_kernel<0>})
-      TOPS_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)sizeof(EsShared)));
-    attr_done[dev] = true;
-  }
+  const int s0 = once_per_device(
+      setup, dev,
+      [&](int &) -> int {
+        for (auto fn : {esd_kernel<3>, esd_kernel<6>, esd_kernel<0>})
+          TOPS_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)sizeof(EsShared)));
+        return TOPS_OK;
+      },
+      nullptr);
+  if (s0 != TOPS_OK) return s0;
   double2 *part = static_cast<double2 *>(scratch);
   for (int o0 = 0; o0 < n_ov; o0 += ES_MAXOV) {
     EsBatch B;

@@ -1093,22 +1093,24 @@ static int launch_resample_t(const ResampleJob *jobs, int njobs, const TileCfg &
                              cudaStream_t st) {
   // the shared-memory opt-in is a per-device function attribute; the
   // persistent grid is the number of CTAs resident at once
-  static bool attr_done[kMaxDevices] = {};
-  static int resident[kMaxDevices] = {};
-  int dev = 0;
+  static PerDeviceOnce setup;
+  int dev = 0, resident = 0;
   TOPS_CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kMaxDevices) return TOPS_E_INVALID;
-  if (!attr_done[dev]) {
-    TOPS_CUDA_TRY(cudaFuncSetAttribute(resample_kernel<kSplit>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)sizeof(RsShared)));
-    int per_sm = 0, sms = 0;
-    TOPS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm, resample_kernel<kSplit>, RS_NT, sizeof(RsShared)));
-    TOPS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    resident[dev] = per_sm * sms;
-    attr_done[dev] = true;
-  }
+  const int s0 = once_per_device(
+      setup, dev,
+      [&](int &v) -> int {
+        TOPS_CUDA_TRY(cudaFuncSetAttribute(resample_kernel<kSplit>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)sizeof(RsShared)));
+        int per_sm = 0, sms = 0;
+        TOPS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, resample_kernel<kSplit>, RS_NT, sizeof(RsShared)));
+        TOPS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        v = per_sm * sms;
+        return TOPS_OK;
+      },
+      &resident);
+  if (s0 != TOPS_OK) return s0;
   if (cfg.seg_rows < 0 || cfg.seg_rows > RS_SEG || (cfg.seg_rows && cfg.seg_rows < RS_GR))
     return TOPS_E_INVALID;
   for (int j0 = 0, k = 0; j0 < njobs; j0 += RS_MAXJOBS, k++) {
@@ -1132,7 +1134,7 @@ static int launch_resample_t(const ResampleJob *jobs, int njobs, const TileCfg &
     int grid = items;
     if (B.counter) {
       TOPS_CUDA_TRY(cudaMemsetAsync(B.counter, 0, sizeof(int), st));
-      grid = min(items, cfg.grid > 0 ? cfg.grid : resident[dev]);
+      grid = min(items, cfg.grid > 0 ? cfg.grid : resident);
     }
     resample_kernel<kSplit><<<grid, RS_NT, sizeof(RsShared), st>>>(B);
     TOPS_CUDA_TRY(cudaGetLastError());

@@ -99,17 +99,23 @@ size_t tops_pair_footprint(const tops_swath_info *m, const tops_pair_opts *o, in
   pitches(W, dem_pixels, slc, cplx, coh, dem);
   const size_t lines = (size_t)nb * L;
   size_t b = 2 * lines * slc + lines * cplx + lines * coh + (size_t)dem_lines * dem;
-  if (o->reslave_full) {
+  int ov[TOPS_MAX_BURSTS] = {}, tot = 0, mx = 0;
+  tops_overlap_size(nb, m->burst_first_line_time, m->burst_last_line_time, m->dt, ov, &tot,
+                    &mx);
+  if (o->reslave_full)
     b += lines * cplx;
-  } else {
-    int ov[TOPS_MAX_BURSTS], tot = 0, mx = 0;
-    tops_overlap_size(nb, m->burst_first_line_time, m->burst_last_line_time, m->dt, ov, &tot,
-                      &mx);
+  else
     b += 2 * (size_t)(tot > 0 ? tot : 0) * cplx;
-  }
   b += 3 * sizeof(double) * (size_t)nb * W;           // deramp rows
   b += (size_t)nb * 4096 * 33 * sizeof(double);       // geocoreg partials (upper bound)
-  b += (size_t)nb * (W / 224 + 1) * 8 * 16;           // ESD partials (upper bound)
+  // ESD partials: one 16-byte sum per (224-column strip, 32-line segment)
+  // of every overlap, as the ESD kernel tiles it
+  size_t esd_items = 0;
+  for (int i = 0; i + 1 < nb; i++) {
+    const int lines_i = ov[i] > 0 ? ov[i] : 0;
+    esd_items += (size_t)((W + 223) / 224) * (size_t)(lines_i > 0 ? (lines_i + 31) / 32 : 1);
+  }
+  b += esd_items * 16;
   b += 2 * sizeof(float) * 2048 * 12 + 2048 * 4 + 4096;
   b += 32 * Arena::kAlign;                             // per-buffer alignment
   return b;

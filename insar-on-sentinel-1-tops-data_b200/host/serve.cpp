@@ -178,9 +178,20 @@ struct tops_server {
       if (!free_slot) break;
       j->admit = now();
       const int r = launch(j, *free_slot);
-      if (r == TOPS_E_NOMEM) {   // wait until running jobs release memory
-        j->admit = -1;
-        break;
+      if (r == TOPS_E_NOMEM) {
+        bool running = false;
+        for (Slot &s : slots) running = running || s.job != nullptr;
+        if (running) {   // wait until running jobs release memory
+          j->admit = -1;
+          break;
+        }
+        // nothing runs, yet the job does not fit: its buffers do not fit
+        // even the empty arena, so it never will -- end it now rather than
+        // leave the queue stalled behind it
+        queue.pop_front();
+        st.queued--;
+        finish(j, TOPS_E_NOMEM, now());
+        continue;
       }
       queue.pop_front();
       st.queued--;

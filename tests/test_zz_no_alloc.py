@@ -4,8 +4,8 @@ Some callers cannot call cudaMalloc -- code that runs inside an HBM budget
 it does not own, or loops where the allocator's implicit synchronisation is
 not allowed.  tops_esd_static keeps its scratch in a static device array of
 the library.  This checks it against tops_esd (caller-provided scratch) on
-the same device inputs, on two calls in a row, and that requests larger than
-the static array are refused.  This file is collected last on purpose.
+calls in a row with changing inputs, and that requests larger than the
+static array are refused.  This file is collected last on purpose.
 """
 import ctypes as C
 
@@ -40,30 +40,45 @@ def _overlaps(T, S, torch):
     return arr, nb - 1, (master, slave)
 
 
-def test_esd_static_matches_esd(T, scene_esd):
-    import torch
-    arr, n, keep = _overlaps(T, scene_esd, torch)
+def _esd(T, torch, fn, arr, n, scratch=None, nbytes=0):
+    """Shifts and (re, im) sums of one ESD call on the current stream."""
     stream = torch.cuda.current_stream().cuda_stream
-    nbytes = T.lib.tops_esd_scratch_bytes(arr, n)
-    assert nbytes > 0
-    scratch = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
-    ref = torch.zeros(n, dtype=torch.float64, device="cuda")
-    ref_sums = torch.zeros(2 * n, dtype=torch.float64, device="cuda")
-    T.check(T.lib.tops_esd(arr, n, 3, 10, C.c_float(0.3), C.c_void_p(ref.data_ptr()),
-                           C.c_void_p(ref_sums.data_ptr()), C.c_void_p(scratch.data_ptr()),
-                           nbytes, C.c_void_p(stream)), "tops_esd")
+    out = torch.full((n,), float("nan"), dtype=torch.float64, device="cuda")
+    sums = torch.full((2 * n,), float("nan"), dtype=torch.float64, device="cuda")
+    if fn == "tops_esd":
+        st = T.lib.tops_esd(arr, n, 3, 10, C.c_float(0.3), C.c_void_p(out.data_ptr()),
+                            C.c_void_p(sums.data_ptr()), C.c_void_p(scratch.data_ptr()), nbytes,
+                            C.c_void_p(stream))
+    else:
+        st = T.lib.tops_esd_static(arr, n, 3, 10, C.c_float(0.3), C.c_void_p(out.data_ptr()),
+                                   C.c_void_p(sums.data_ptr()), C.c_void_p(stream))
+    T.check(st, fn)
     torch.cuda.synchronize()
-    for call in range(2):
-        out = torch.full((n,), float("nan"), dtype=torch.float64, device="cuda")
-        sums = torch.zeros(2 * n, dtype=torch.float64, device="cuda")
-        T.check(T.lib.tops_esd_static(arr, n, 3, 10, C.c_float(0.3),
-                                      C.c_void_p(out.data_ptr()), C.c_void_p(sums.data_ptr()),
-                                      C.c_void_p(stream)), "tops_esd_static")
-        torch.cuda.synchronize()
-        a, r = out.cpu().numpy(), ref.cpu().numpy()
+    return out.cpu().numpy(), sums.cpu().numpy()
+
+
+def test_esd_static_matches_esd(T, scene_esd, scene_small):
+    """Three calls in a row on two different inputs (A, B, A): each result
+    is compared with tops_esd on its own input, so a result left over in the
+    shared static array from the call before would be caught."""
+    import torch
+    inputs, refs = [], []
+    for S in (scene_esd, scene_small):
+        arr, n, keep = _overlaps(T, S, torch)
+        nbytes = T.lib.tops_esd_scratch_bytes(arr, n)
+        assert nbytes > 0
+        scratch = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+        refs.append(_esd(T, torch, "tops_esd", arr, n, scratch, nbytes))
+        inputs.append((arr, n, keep))
+    # the two inputs give different answers, so a stale result cannot pass
+    assert refs[0][0].shape != refs[1][0].shape or np.any(refs[0][0] != refs[1][0])
+    for call, k in enumerate((0, 1, 0)):
+        arr, n, _ = inputs[k]
+        a, sums = _esd(T, torch, "tops_esd_static", arr, n)
+        r, r_sums = refs[k]
         assert np.all(np.isfinite(a)), (call, a)
         assert np.abs(a - r).max() <= ESD_TOL, (call, a, r)
-        assert np.array_equal(sums.cpu().numpy(), ref_sums.cpu().numpy()), call
+        assert np.array_equal(sums, r_sums), call
 
 
 def test_esd_static_rejects_oversized_request(T, scene_esd):
