@@ -12,43 +12,55 @@
 //             deramped slave d = s exp(i phi), reramped with the LUT-weighted
 //             sum of the deramp phase phi.
 //
-// B200 design (no textures, no phase array in HBM).  A CTA owns a strip of
-// RS_TW output columns and sweeps a segment of output rows in groups of RS_GR
-// rows; per group:
-//   [A] Row statistics from the offset polynomials, not per pixel: along the
-//       strip y and x are quadratics in the column, so their range follows
-//       from the two ends and the vertex.  A row whose whole strip maps to one
-//       (azimuth line, LUT bin) key -- in a TOPS pair nearly every row -- gets
-//       one shared azimuth pass.  The same bounds give the slave lines the
-//       group needs.  Warp 7, idle in the range pass [D], prepares the next
-//       group's keys, ring-row table and azimuth taps during [D], into the
-//       second of two per-row tables; the other warps never wait for it.
-//   [B] New slave rows are deramped once into a ring of RS_FR rows x RS_FW
-//       columns in shared memory: d (complex) and the FP32 residual
-//       G = phi - phi_ref of the deramp phase against a reference column.
-//   [C] Azimuth pass v(x) = sum_j kAz[j] d(L0-5+j, x) for every ring column,
-//       blocked over 4 rows x 2 columns per thread (15 ring loads and 24
-//       weight loads feed 96 packed FP32x2 FMAs).  G is exactly quadratic in
-//       azimuth time per column, so its azimuth interpolation is
-//       M0 G(L0) + g2 P1 + g1 P2 with the LUT row moments -- no taps.
-//   [D] Range pass, reramp, store.  A thread owns 2 adjacent output columns
-//       for 4 rows.  A column's range key (p0, bin) changes only every ~100
-//       rows, so its 12 range weights stay in registers; the 14 v samples of
-//       a column pair are 7 16-byte shared loads, and the phase residuals of
-//       2 rows are range-interpolated together with packed FMAs.
-// The interpolated phase is (1 + sp1) Psi_row + sum_i kRg[i] vg(x_i), where
-// Psi_row = sum_j kAz[j] phi_ref(y_j) is FP64 (reduced mod 2 pi) and
-// 1 + sp1 = sum kRg: equal to the reference's 144-tap FP64 phase sum in exact
-// arithmetic.  Rows or pixels outside these cases (several keys in a row,
-// edge and outside pixels, supports beyond the ring) take per-pixel paths
-// that compute the same formula.
+// B200 design (no textures, no phase array in HBM).  A CTA of 128 threads
+// owns a strip of RS_TW = 112 output columns and a segment of up to 252
+// output rows (a work item), swept in groups of RS_GR = 12 rows.
 //
-// Precision modes: TOPS_PREC_SPLIT (default) forms G and the reduced phase of
-// each ring sample in FP32 from per-column coefficients about the burst's
-// centre time, with the FP64 reference-row phase reduced mod 2 pi once per
-// row (double-single).  TOPS_PREC_FP64 evaluates every sample's deramp phase
-// and its reduction in FP64.  Positions, LUT bins and Psi_row are FP64 in
-// both.
+// Item prologue (all threads): per-row statistics from the offset
+// polynomials -- along the strip y is a quadratic in the column, so a row
+// whose whole strip maps to one (azimuth line, LUT bin) key (nearly every
+// row of a TOPS pair) gets one shared azimuth pass -- with the row's FP64
+// phase terms; per output column the runs of its range key (p0, bin) over
+// the item, found by bisection of the exact per-pixel position (keys change
+// every ~100+ rows), each run with its range weights' phase moments.
+//
+// Per group:
+//   [A] azimuth pass, thread = ring column (RS_FW = 128 slave columns): the
+//       thread's raw slave lines were staged in shared memory with cp.async
+//       during the previous group; each new line is deramped in registers
+//       and pushed into a 12-line register window (the window's slots rotate
+//       with the row index, so a steady row costs one deramp and no moves);
+//       v = sum_j kAz[j] d(L0-5+j) is 12 packed FP32x2 FMAs, written to a
+//       double-buffered tile.
+//   [B] range pass, thread = 2 adjacent output columns x 6 rows: the 14
+//       tile samples of the pair are 7 16-byte loads, the 12 range weights
+//       of each column stay in registers for its key run, and the reramp
+//       phase is a dot product of row terms and column-run terms (below).
+// One barrier per group separates [A] and [B]; the tile is double-buffered,
+// so [A] of the next group never waits for [B].
+//
+// The phase.  The reference reramps with the 144-tap FP64 sum
+// Phi = sum_j sum_i kAz[j] kRg[i] phi(y_j, x_i).  With phi = phi_ref(y) +
+// G(y, x), phi_ref the deramp phase of one reference column and G exactly
+// quadratic in the burst-local time tc (G = g2 tc^2 + g1 tc + g0 per
+// column), Phi = (1 + sp) Psi + G2 R2 + G1 R1 + G0 R0, with
+//   Psi = sum_j kAz[j] phi_ref(y_j)                   (row, FP64, reduced)
+//   sp  = sum_i kRg[i] - 1, Gk = sum_i kRg[i] gk(x_i)  (column key run)
+//   R2 = M0 tc0^2 + 2 tc0 dt M1 + dt^2 M2, R1 = M0 tc0 + dt M1, R0 = M0
+//        (row; M0..M2 the azimuth taps' moments, tc0 = tc(L0)),
+// equal to the reference's sum in exact arithmetic.
+//
+// Rows or pixels outside these cases (several keys in a row, edge and
+// outside pixels, range supports beyond the ring window, columns with more
+// than RS_MAXRUN key runs) take a per-pixel path that computes the same
+// formula from the slave in HBM.
+//
+// Precision modes: TOPS_PREC_SPLIT (default) forms each sample's deramp
+// phase in FP32 as rho(y) + G(y, x), rho the FP64 reference phase reduced
+// mod 2 pi once per slave line (double-single) and G the FP32 quadratic
+// about the burst's centre time.  TOPS_PREC_FP64 evaluates every sample's
+// deramp phase and its reduction in FP64.  Positions, LUT bins and Psi are
+// FP64 in both.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -59,20 +71,28 @@
 
 namespace tops {
 
-constexpr int RS_NT = 256;   // threads per CTA
-constexpr int RS_TW = 112;   // output columns per strip
-constexpr int RS_GR = 16;    // output rows per group
-constexpr int RS_FR = 32;    // ring rows (power of two)
-constexpr int RS_FW = 128;   // ring columns
-constexpr int RS_SEG = 256;  // output rows per work item
+constexpr int RS_NT = 128;                 // threads per CTA
+constexpr int RS_TW = 112;                 // output columns per strip
+constexpr int RS_FW = 128;                 // ring (slave) columns of a strip
+constexpr int RS_GR = 12;                  // rows per group (= azimuth taps)
+constexpr int RS_HR = RS_GR / 2;           // rows per range-pass thread
+constexpr int RS_SEG = 252;                // default rows per work item
+constexpr int RS_MAXSEG = 252;             // per-item tables are sized for this
+constexpr int RS_NGRP = (RS_MAXSEG + RS_GR - 1) / RS_GR;
+constexpr int RS_SR = 32;                  // staged slave lines (power of two)
+constexpr int RS_NSR = RS_MAXSEG + 44;     // slave-line phase table
+constexpr int RS_MAXRUN = 4;               // range-key runs per column and item
+constexpr int RS_MAXBIN = 16;              // distinct azimuth bins per item
+constexpr int RS_NOSLOT = 0x7fff;          // azimuth bin outside the bin table
 constexpr int RS_MAXJOBS = 32;
-constexpr int RS_DP = RS_TW / 2;   // column pairs of the range pass
-constexpr int RS_DT = RS_DP * 4;   // range-pass threads (4 row quarters of 4 rows)
-static_assert(RS_DT == RS_NT - 32, "warp 7 prepares the next group during the range pass");
-static_assert(RS_GR == 16 && RS_FW == 128 && RS_NT == 256 && RS_FR == 32,
-              "the thread mappings assume these sizes");
+constexpr int RS_DP = RS_TW / 2;           // column pairs of the range pass
+constexpr int RS_DT = 2 * RS_DP;           // range-pass threads
+static_assert(RS_FW == RS_NT, "one ring column per thread in the azimuth pass");
+static_assert(RS_DT <= RS_NT && RS_GR == 12 && RS_HR * 2 == RS_GR,
+              "thread mappings assume these sizes");
 
 enum : int { REG_OUT = 0, REG_EDGE = 1, REG_IN = 2 };
+enum : int { RM_PIXEL = 0, RM_STEADY = 1, RM_REBUILD = 2 };
 
 using RsLut = LutPtrs;
 
@@ -83,59 +103,44 @@ struct RsBatch {
   ResampleJob jobs[RS_MAXJOBS];
 };
 
-struct RsRows {
-  int v[RS_GR];                       // 1: shared azimuth pass valid for the row
-  int L0[RS_GR], bL[RS_GR];           // its azimuth line and LUT bin
-  float rho[RS_GR], psif[RS_GR];      // row phase Psi reduced mod 2 pi, and as float
+// One output row of a work item.
+struct __align__(16) RsRow {
+  float rho, psif, R2, R1;   // Psi mod 2 pi, Psi as float, residual-phase row terms
+  float R0;
+  int L0;                    // azimuth line of the shared azimuth pass
+  int bin;                   // its LUT bin | bin-table slot << 16
+  int mode;                  // RM_PIXEL: per pixel; RM_STEADY: one new window line;
+                             // RM_REBUILD: the window is filled anew
+};
+
+// Deramp terms of one slave line.
+struct RsSlaveRow {
+  double ta;                 // burst-local azimuth time
+  float rho, tc;             // reference-column phase mod 2 pi; ta - tm
 };
 
 struct __align__(16) RsShared {
-  float2 ring_d[RS_FR][RS_FW];        // deramped slave rows
-  float ring_g[RS_FR][RS_FW];         // G = phi - phi_ref of each ring sample
-  float2 vd[RS_GR][RS_FW];            // azimuth-interpolated d
-  float2 vgp[RS_GR / 2][RS_FW];       // azimuth-interpolated G of rows (2k, 2k+1)
-  float4 wpair[RS_GR][6];             // azimuth taps duplicated: (w0,w0,w1,w1), ...
-  double ring_phiref[RS_FR];          // FP64 reference-column phase of the ring row
-  double ring_ta[RS_FR];              // burst-local azimuth time of the ring row
-  float ring_rho[RS_FR];              // ring_phiref reduced mod 2 pi
-  float ring_tc[RS_FR];               // ring_ta - tm (FP32, split mode)
-  double rowA_az[RS_SEG], rowB_az[RS_SEG], rowA_rg[RS_SEG], rowB_rg[RS_SEG];
-  // per-column P^ and c5 P^2 terms; a range-pass thread reads its two
-  // columns with one 16-byte load (conflict-free across the warp)
+  float2 vd[2][RS_GR][RS_FW];         // azimuth-interpolated rows (double-buffered)
+  short2 stage[RS_SR][RS_FW];         // raw slave lines, ring indexed by line & 31
+  RsRow rows[RS_MAXSEG];
+  RsSlaveRow srow[RS_NSR];            // slave lines ys0 .. ys0 + RS_NSR - 1
+  float4 run_g[RS_TW][RS_MAXRUN];     // per range-key run: (sp, G2, G1, G0)
+  int2 run_rk[RS_TW][RS_MAXRUN];      // (first item row, key = p0 * 4096 + bin)
+  int run_n[RS_TW];                   // runs of the column (-1: more than RS_MAXRUN)
+  float4 ring_gc[RS_FW];              // per ring column (g2, g1, g0, 0)
+  float4 bin_w[RS_MAXBIN][6];         // azimuth taps as (w0,w0,w1,w1), ...
+  int bin_id[RS_MAXBIN];
   alignas(16) double col_phat[RS_TW];
-  alignas(16) double col_qaz[RS_TW];
-  alignas(16) double col_qrg[RS_TW];
-  // per-row tables of a group; the range pass of one group reads one copy
-  // while warp 7 prepares the other for the next group
-  RsRows rows[2];
-  float row_M0[RS_GR], row_P1[RS_GR], row_P2[RS_GR];
-  int g_lmin, g_lmax;                 // slave lines the group's interior pixels use
+  double col_qaz[RS_TW], col_qrg[RS_TW];
+  int4 gplan[RS_NGRP];                // per group: lines to stage before it, staged window
   double caz[6], crg[6], shift;
-  int xw;                             // absolute slave column of ring column 0
-  double ref_a0, ref_a1, ref_a2;      // deramp quadratic of the reference column
-  double tm;                          // centre time of the split-mode coefficients
-  int next_item;                      // persistent launch: the item just taken
-  // per-row key statistics of the whole work item, computed once up front:
-  // azimuth line / LUT bin of a row with one key (bin -1: none) and the
-  // slave lines its interior pixels use
-  int ri_L0[RS_SEG], ri_bL[RS_SEG], ri_lmin[RS_SEG], ri_lmax[RS_SEG];
-  // raw slave rows of the next group, copied asynchronously (cp.async)
-  // while the current group computes; each thread reads back only the
-  // elements it copied
-  alignas(16) short2 stage[RS_FR][RS_FW];
-  int pf_lo, pf_hi;                   // rows staged for this group
-  int nx_lo, nx_hi;                   // rows the next group brings
+  double ref_a0, ref_a1, ref_a2, tm;
+  int xw, ys0, nbins, ngrp, next_item;
 };
 
-// Asynchronous global -> shared copies of 4 or 8 bytes to a shared-window
-// address; src_bytes 0 fills the destination with zeros without reading.
+// Asynchronous 4-byte global -> shared copy; src_bytes 0 fills zeros.
 __device__ __forceinline__ unsigned smem_u32(const void *p) {
   return static_cast<unsigned>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void cp_async_8s(unsigned d, const void *src, int src_bytes) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src),
-               "r"(src_bytes)
-               : "memory");
 }
 __device__ __forceinline__ void cp_async_4s(unsigned d, const void *src, int src_bytes) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src),
@@ -192,6 +197,20 @@ __device__ __forceinline__ int region_of(const ResampleJob &J, int l0, int p0) {
   return REG_IN;
 }
 
+// my_polyval grouped by row: position = fma(B(row), P^, A(row) + c5 P^2)
+// with A = c0 + c1 L^ + c3 L^2 and B = c2 + c4 L^.  Every path of the kernel
+// evaluates positions with these functions, so their keys agree bit for bit.
+__device__ __forceinline__ double row_L(const ResampleJob &J, int r) {
+  return ((double)(r + J.my0) - J.midL) * J.invL;
+}
+__device__ __forceinline__ double row_a(const double *c, double L) {
+  return fma(fma(c[3], L, c[1]), L, c[0]);
+}
+__device__ __forceinline__ double row_b(const double *c, double L) { return fma(c[4], L, c[2]); }
+__device__ __forceinline__ double pix_pos(double A, double B, double P, double Q) {
+  return fma(B, P, A + Q);
+}
+
 // Range [lo, hi] of f(p) = fma(b, p, a + c p^2) -- the per-pixel form -- over
 // p in [p0, p1]: the ends and, when inside, the vertex.  Widened by 1e-9 so
 // that rounding of the per-pixel evaluation cannot leave it.
@@ -213,9 +232,18 @@ __device__ __forceinline__ void quad_span(double a, double b, double c, double p
   hi += 1e-9;
 }
 
+// Range key (p0 * 4096 + bin) of pixel (box row r, strip column c).
+__device__ __forceinline__ int rg_key(const RsShared &S, const ResampleJob &J, int r, int c) {
+  const double L = row_L(J, r);
+  const double x = pix_pos(row_a(S.crg, L), row_b(S.crg, L), S.col_phat[c], S.col_qrg[c]);
+  int p0, b;
+  split_pos(x, p0, b);
+  return p0 * 4096 + b;
+}
+
 // ---------------------------------------------------- HBM slow path
-// Per-pixel interior resample straight from the CInt16 slave in HBM (used
-// only when the support does not fit the ring window).
+// Per-pixel interior resample straight from the CInt16 slave in HBM (rows
+// and pixels the shared passes do not cover).
 __device__ float2 interior_from_global(const ResampleJob &J, const RsLut &lut, int L0, int bL,
                                        int P0, int bP) {
   const float *kl = lut.kaz + bL * kTaps;
@@ -248,108 +276,182 @@ __device__ float2 interior_from_global(const ResampleJob &J, const RsLut &lut, i
   return make_float2(sre * c + sim * s, sim * c - sre * s);
 }
 
-// ---------------------------------------------------- ring per-pixel path
-__device__ float2 interior_from_ring(const RsShared &S, const RsLut &lut, const ResampleJob &J,
-                                     const DerampQuad &refq, int L0, int bL, int P0, int bP) {
-  const float *kl = lut.kaz + bL * kTaps;
-  const float *kp = lut.krg + bP * kTaps;
-  float kpr[kTaps];
-#pragma unroll
-  for (int i = 0; i < kTaps; i++) kpr[i] = __ldg(kp + i);
-  const int xc = P0 - 5 - S.xw;
-  float sre = 0.f, sim = 0.f, sg = 0.f;
-  double psi = 0.0;
-#pragma unroll 1
-  for (int j = 0; j < kTaps; j++) {
-    int slot = (L0 - 5 + j) & (RS_FR - 1);
-    float w = __ldg(kl + j);
-    float tre = 0.f, tim = 0.f, tg = 0.f;
-#pragma unroll
-    for (int i = 0; i < kTaps; i++) {
-      float2 d = S.ring_d[slot][xc + i];
-      tre = fmaf(kpr[i], d.x, tre);
-      tim = fmaf(kpr[i], d.y, tim);
-      tg = fmaf(kpr[i], S.ring_g[slot][xc + i], tg);
-    }
-    sre = fmaf(w, tre, sre);
-    sim = fmaf(w, tim, sim);
-    sg = fmaf(w, tg, sg);
-    // the reference-column phase of the line, as the ring-row table holds it
-    const double phref = quad_eval(refq, (double)(L0 - 5 + j - J.s_first_line) * J.dt);
-    psi = fma((double)w, phref, psi);
+// Any pixel (box row r, strip column c) by the per-pixel definition.
+__device__ __forceinline__ float2 pixel_generic(const RsShared &S, const ResampleJob &J, int r,
+                                             int c) {
+  const double L = row_L(J, r);
+  const double P = S.col_phat[c];
+  const double y = pix_pos(row_a(S.caz, L) + S.shift, row_b(S.caz, L), P, S.col_qaz[c]);
+  const double x = pix_pos(row_a(S.crg, L), row_b(S.crg, L), P, S.col_qrg[c]);
+  int l0, bl, p0, bp;
+  split_pos(y, l0, bl);
+  split_pos(x, p0, bp);
+  const int reg = region_of(J, l0, p0);
+  if (reg == REG_OUT) return make_float2(0.f, 0.f);
+  if (reg == REG_EDGE) {
+    const short2 sv = J.slave[(long)(l0 - J.sy0) * J.slave_pitch + (p0 - J.sx0)];
+    return make_float2((float)sv.x, (float)sv.y);
   }
-  float phi = reduce_2pi(psi) + __ldg(lut.sp1 + bP) * (float)psi + sg;
-  return cmul_conj_phase(make_float2(sre, sim), phi);
+  return interior_from_global(J, J.lut, l0, bl, p0, bp);
 }
 
-// Range weights of one output column, held in registers while its key holds.
-struct ColW {
-  float4 w[6];   // (w0,w0,w1,w1), (w2,w2,w3,w3), ...
-  float sp1;
-  int key;       // p0 << 12 | bin of the loaded weights (-1: none)
+// Range weights and phase terms of one output column's current key run.
+struct ColRun {
+  float4 w[6];    // (w0,w0,w1,w1), (w2,w2,w3,w3), ...
+  float sp, G2, G1, G0;
+  int key;        // p0 * 4096 + bin
+  int next;       // first item row of the next run
+  int m;          // run index
+  bool ok;        // range-interior and inside the ring window: fast range pass
 };
 
-__device__ __forceinline__ void colw_load(ColW &cw, const RsLut &lut, int key) {
-  if (cw.key == key) return;
-  const int bp = key & 0xfff;
-  const float4 *kp4 = lut.krg2 + bp * (kTaps / 2);
+__device__ __forceinline__ void run_load(ColRun &cr, const RsShared &S, const ResampleJob &J,
+                                         int c, int m) {
+  const int n = S.run_n[c];
+  const int2 rk = S.run_rk[c][m];
+  const float4 g = S.run_g[c][m];
+  cr.m = m;
+  cr.key = rk.y;
+  cr.next = (m + 1 < n) ? S.run_rk[c][m + 1].x : INT32_MAX;
+  cr.sp = g.x;
+  cr.G2 = g.y;
+  cr.G1 = g.z;
+  cr.G0 = g.w;
+  const int p0 = rk.y >> 12, bp = rk.y & 4095;
+  const int xb = p0 - 5 - S.xw;
+  cr.ok = p0 >= J.sx0 + 5 && p0 <= J.sx1 - 7 && xb >= 0 && xb + 13 < RS_FW;
+  if (cr.ok) {
+    const float4 *kp4 = J.lut.krg2 + bp * (kTaps / 2);
 #pragma unroll
-  for (int q = 0; q < kTaps / 2; q++) cw.w[q] = __ldg(kp4 + q);
-  cw.sp1 = __ldg(lut.sp1 + bp);
-  cw.key = key;
+    for (int q = 0; q < kTaps / 2; q++) cr.w[q] = __ldg(kp4 + q);
+  }
 }
 
-__device__ __forceinline__ float2 wtap(const ColW &cw, int i) {
-  const float4 q = cw.w[i >> 1];
+__device__ __forceinline__ float2 wtap(const ColRun &cr, int i) {
+  const float4 q = cr.w[i >> 1];
   return (i & 1) ? make_float2(q.z, q.w) : make_float2(q.x, q.y);
 }
 
-// One interior pixel of a row with a shared azimuth pass: 12-tap range pass
-// over vd / vg of the row (single column).
-__device__ __forceinline__ float2 range_pixel(const RsShared &S, const RsRows &R, const ColW &cw,
-                                              int r, int xb) {
-  float2 acc = make_float2(0.f, 0.f);
-  float sg = 0.f;
-  const float *vgrow = reinterpret_cast<const float *>(&S.vgp[r >> 1][0]) + (r & 1);
-#pragma unroll
-  for (int i = 0; i < kTaps; i++) {
-    const float2 w = wtap(cw, i);
-    acc = __ffma2_rn(w, S.vd[r][xb + i], acc);
-    sg = fmaf(w.x, vgrow[2 * (xb + i)], sg);
-  }
-  const float phi = R.rho[r] + cw.sp1 * R.psif[r] + sg;
-  return cmul_conj_phase(acc, phi);
-}
-
 // 12-tap range pass of two adjacent columns over the 14 samples V (the first
-// column's taps start at V[odd], the second's at V[odd + 1]).
-__device__ __forceinline__ void range_pair(const ColW &c0, const ColW &c1, const float2 (&V)[14],
-                                           bool odd, float2 &s0, float2 &s1) {
-  s0 = make_float2(0.f, 0.f);
-  s1 = s0;
+// column's taps start at V[odd], the second's at V[odd + 1]); two partial
+// sums per column shorten the FMA chains.
+__device__ __forceinline__ void range_pair(const ColRun &c0, const ColRun &c1,
+                                           const float2 (&V)[14], bool odd, float2 &s0,
+                                           float2 &s1) {
+  float2 a0 = make_float2(0.f, 0.f), b0 = a0, a1 = a0, b1 = a0;
   if (odd) {
 #pragma unroll
-    for (int i = 0; i < kTaps; i++) {
-      s0 = __ffma2_rn(wtap(c0, i), V[i + 1], s0);
-      s1 = __ffma2_rn(wtap(c1, i), V[i + 2], s1);
+    for (int i = 0; i < kTaps; i += 2) {
+      a0 = __ffma2_rn(wtap(c0, i), V[i + 1], a0);
+      b0 = __ffma2_rn(wtap(c0, i + 1), V[i + 2], b0);
+      a1 = __ffma2_rn(wtap(c1, i), V[i + 2], a1);
+      b1 = __ffma2_rn(wtap(c1, i + 1), V[i + 3], b1);
     }
   } else {
 #pragma unroll
-    for (int i = 0; i < kTaps; i++) {
-      s0 = __ffma2_rn(wtap(c0, i), V[i], s0);
-      s1 = __ffma2_rn(wtap(c1, i), V[i + 1], s1);
+    for (int i = 0; i < kTaps; i += 2) {
+      a0 = __ffma2_rn(wtap(c0, i), V[i], a0);
+      b0 = __ffma2_rn(wtap(c0, i + 1), V[i + 1], b0);
+      a1 = __ffma2_rn(wtap(c1, i), V[i + 1], a1);
+      b1 = __ffma2_rn(wtap(c1, i + 1), V[i + 2], b1);
+    }
+  }
+  s0 = __fadd2_rn(a0, b0);
+  s1 = __fadd2_rn(a1, b1);
+}
+
+// 12-tap range pass of one column from a tile row (8-byte loads).
+__device__ __forceinline__ float2 range_single(const float2 *row, int xb, const ColRun &cr) {
+  float2 a = make_float2(0.f, 0.f), b = a;
+#pragma unroll
+  for (int i = 0; i < kTaps; i += 2) {
+    a = __ffma2_rn(wtap(cr, i), row[xb + i], a);
+    b = __ffma2_rn(wtap(cr, i + 1), row[xb + i + 1], b);
+  }
+  return __fadd2_rn(a, b);
+}
+
+// Reramp phase of a pixel: (1 + sp) Psi + G2 R2 + G1 R1 + G0 R0, with Psi
+// as its reduced value plus sp times its float value.
+__device__ __forceinline__ float run_phase(const RsRow &R, const ColRun &cr) {
+  return fmaf(cr.sp, R.psif, R.rho) + fmaf(cr.G2, R.R2, fmaf(cr.G1, R.R1, cr.G0 * R.R0));
+}
+
+// Deramped slave sample (line y, this thread's ring column) for the
+// azimuth-pass window: from the staged lines when the line is staged, else
+// from HBM.
+template <bool kSplit>
+__device__ __forceinline__ float2 deramp_at(const RsShared &S, const ResampleJob &J, int x,
+                                            int xa, bool xin, int y, int win_lo, int win_hi,
+                                            float g2c, float g1c, float g0c,
+                                            const DerampQuad &cq) {
+  float sx, sy;
+  if (y >= win_lo && y <= win_hi) {
+    const short2 v = S.stage[y & (RS_SR - 1)][x];
+    sx = (float)v.x;
+    sy = (float)v.y;
+  } else {
+    if (!xin || y < J.sy0 || y > J.sy1) return make_float2(0.f, 0.f);
+    const short2 v = J.slave[(long)(y - J.sy0) * J.slave_pitch + (xa - J.sx0)];
+    sx = (float)v.x;
+    sy = (float)v.y;
+  }
+  const int iy = y - S.ys0;
+  float r;
+  if (kSplit) {
+    float rho, tc;
+    if ((unsigned)iy < (unsigned)RS_NSR) {
+      rho = S.srow[iy].rho;
+      tc = S.srow[iy].tc;
+    } else {
+      const DerampQuad refq = {S.ref_a0, S.ref_a1, S.ref_a2};
+      const double ta = (double)(y - J.s_first_line) * J.dt;
+      rho = reduce_2pi(quad_eval(refq, ta));
+      tc = (float)(ta - S.tm);
+    }
+    const float G = fmaf(fmaf(g2c, tc, g1c), tc, g0c);
+    r = reduce_2pi_f(rho + G);
+  } else {
+    const double ta = ((unsigned)iy < (unsigned)RS_NSR) ? S.srow[iy].ta
+                                                         : (double)(y - J.s_first_line) * J.dt;
+    r = reduce_2pi(quad_eval(cq, ta));
+  }
+  float sn, cs;
+  __sincosf(r, &sn, &cs);
+  return make_float2(sx * cs - sy * sn, sx * sn + sy * cs);
+}
+
+// Azimuth taps of a row (bin | slot << 16) as (w, w) pairs.
+__device__ __forceinline__ void load_az_taps(const RsShared &S, const RsLut &lut, int bin,
+                                             float4 (&wz)[6]) {
+  const int slot = bin >> 16;
+  if (slot < RS_MAXBIN) {
+#pragma unroll
+    for (int q = 0; q < 6; q++) wz[q] = S.bin_w[slot][q];
+  } else {
+    const float *kl = lut.kaz + (bin & 0xffff) * kTaps;
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+      const float a = __ldg(kl + 2 * q), b = __ldg(kl + 2 * q + 1);
+      wz[q] = make_float4(a, a, b, b);
     }
   }
 }
 
-__device__ __forceinline__ void load14(const float2 *row, int base, float2 (&V)[14]) {
-  const float4 *p = reinterpret_cast<const float4 *>(row + base);
-#pragma unroll
-  for (int m = 0; m < 7; m++) {
-    const float4 t = p[m];
-    V[2 * m] = make_float2(t.x, t.y);
-    V[2 * m + 1] = make_float2(t.z, t.w);
+// Stage this thread's ring column of slave lines [lo, hi] (zeros outside
+// the slave box) into the line ring.
+__device__ __forceinline__ void stage_rows(RsShared &S, const ResampleJob &J, int x, int xa,
+                                           bool xin, int lo, int hi) {
+  const short2 *const sl = J.slave;
+  const long pitch = J.slave_pitch;
+  const unsigned rows_in = (unsigned)(J.sy1 - J.sy0);
+  long off = (long)(lo - J.sy0) * pitch + (xa - J.sx0);
+#pragma unroll 4
+  for (int y = lo; y <= hi; y++, off += pitch) {
+    const bool in = xin && (unsigned)(y - J.sy0) <= rows_in;
+    cp_async_4s(smem_u32(&S.stage[y & (RS_SR - 1)][x]), sl + (in ? off : 0), in ? 4 : 0);
   }
+  cp_async_commit();
 }
 
 // One work item (strip x segment of one job); all threads of the CTA call it
@@ -357,7 +459,6 @@ __device__ __forceinline__ void load14(const float2 *row, int base, float2 (&V)[
 template <bool kSplit>
 __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int item) {
   const int tid = threadIdx.x;
-  const int lane = tid & 31;
 
   // ---- locate the work item (job, strip, segment)
   int jb = 0;
@@ -372,8 +473,9 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
   const int cN = min(RS_TW, mpix - c0);
   const int r_begin = J.row0 + seg * J.seg_rows;
   const int r_end = min(r_begin + J.seg_rows, J.row0 + J.nrows);
+  const int nr = r_end - r_begin;
 
-  // ---- per work item setup: polynomials, shift, per-row and per-column terms
+  // ---- [P1] polynomials and shift
   if (tid < 12) {
     const double v = J.cpm_dev ? J.cpm_dev[tid] : (tid < 6 ? J.caz[tid] : J.crg[tid - 6]);
     if (tid < 6)
@@ -392,566 +494,409 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
     S.shift = sh;
   }
   __syncthreads();
-  {
-    // y = A(row) + B(row) P^ + c5 P^2 (the terms of my_polyval grouped by row)
-    const int r = r_begin + tid;
-    if (r < r_end) {
-      const double L = ((double)(r + J.my0) - J.midL) * J.invL;
-      const double *a = S.caz, *g = S.crg;
-      S.rowA_az[tid] = a[0] + a[1] * L + a[3] * L * L + S.shift;
-      S.rowB_az[tid] = a[2] + a[4] * L;
-      S.rowA_rg[tid] = g[0] + g[1] * L + g[3] * L * L;
-      S.rowB_rg[tid] = g[2] + g[4] * L;
-    }
-    if (tid < RS_TW) {
-      const double P = ((double)(c0 + min(tid, cN - 1)) - J.midP) * J.invP;
-      S.col_phat[tid] = P;
-      S.col_qaz[tid] = S.caz[5] * P * P;
-      S.col_qrg[tid] = S.crg[5] * P * P;
-    }
+
+  // ---- [P2] column terms; the ring window and the reference column
+  if (tid < RS_TW) {
+    const double P = ((double)(c0 + min(tid, cN - 1)) - J.midP) * J.invP;
+    S.col_phat[tid] = P;
+    S.col_qaz[tid] = S.caz[5] * P * P;
+    S.col_qrg[tid] = S.crg[5] * P * P;
   }
-  if (tid == 0) {
-    // range position at the segment corners and edge midpoints -> ring window
-    double pmin = 1e300, pmax = -1e300;
+  if (tid == RS_NT - 1) {
+    // range position at the segment corners and edge midpoints -> window
+    double pmin = 1e300;
     for (int a = 0; a < 3; a++) {
-      int rr = (a == 0) ? r_begin : (a == 1 ? (r_begin + r_end - 1) / 2 : r_end - 1);
-      double L = ((double)(rr + J.my0) - J.midL) * J.invL;
+      const int rr = (a == 0) ? r_begin : (a == 1 ? (r_begin + r_end - 1) / 2 : r_end - 1);
+      const double L = row_L(J, rr);
       for (int b = 0; b < 3; b++) {
-        int cc = (b == 0) ? c0 : (b == 1 ? c0 + (cN - 1) / 2 : c0 + cN - 1);
-        double P = ((double)cc - J.midP) * J.invP;
+        const int cc = (b == 0) ? c0 : (b == 1 ? c0 + (cN - 1) / 2 : c0 + cN - 1);
+        const double P = ((double)cc - J.midP) * J.invP;
         const double *c = S.crg;
-        double x = c[0] + c[1] * L + c[2] * P + c[3] * L * L + c[4] * L * P + c[5] * P * P;
+        const double x = c[0] + c[1] * L + c[2] * P + c[3] * L * L + c[4] * L * P + c[5] * P * P;
         pmin = fmin(pmin, x);
-        pmax = fmax(pmax, x);
       }
     }
-    // The range pass reads ring columns [p0 - 6, p0 + 8]: the window starts
-    // at the leftmost such column, one column lower when needed for an even
-    // offset from the box edge (8-byte pair loads).  A strip spanning up to
-    // RS_FW - 16 samples then fits; wider spans fall back per pixel.
-    const int lo = (int)floor(pmin) - 6;
-    const int xw = lo - ((lo - J.sx0) & 1);
+    // the range pass reads ring columns [p0 - 5, p0 + 8] of a column pair;
+    // one column of margin for the position's variation inside the strip
+    const int xw = (int)floor(pmin) - 6;
     S.xw = xw;
-    int xr = min(max(xw + RS_FW / 2, J.sx0), J.sx1);
+    const int xr = min(max(xw + RS_FW / 2, J.sx0), J.sx1);
     const DerampQuad q = deramp_quad(J.kt[xr], J.tref[xr], J.fdc[xr]);
     S.ref_a0 = q.a0;
     S.ref_a1 = q.a1;
     S.ref_a2 = q.a2;
     S.tm = 0.5 * (double)(J.sy0 + J.sy1 - 2 * J.s_first_line) * J.dt;
-    S.nx_lo = 1;   // nothing staged for the first group
-    S.nx_hi = 0;
   }
   __syncthreads();
 
-  // ---- per-row key statistics of the whole item (one thread per row):
-  // along the strip y and x are quadratics in the column, so their ranges
-  // follow from the ends and the vertex.  A row whose strip maps to one
-  // (azimuth line, LUT bin) key, whose azimuth support is interior and whose
-  // range support fits the ring window gets the shared azimuth pass.
-  if (tid < r_end - r_begin) {
-    const int ri = tid;
-    const double p0 = S.col_phat[0], p1 = S.col_phat[cN - 1];
-    double ylo, yhi, xlo, xhi;
-    quad_span(S.rowA_az[ri], S.rowB_az[ri], S.caz[5], p0, p1, ylo, yhi);
-    quad_span(S.rowA_rg[ri], S.rowB_rg[ri], S.crg[5], p0, p1, xlo, xhi);
-    int l0lo, blo, l0hi, bhi, x0lo, xblo, x0hi, xbhi;
+  // ---- [P3] this thread's ring column: deramp coefficients
+  const int xw = S.xw;
+  const int x = tid;                     // ring column
+  const int xa = xw + x;                 // absolute slave column
+  const bool xin = xa >= J.sx0 && xa <= J.sx1;
+  const double tm = S.tm;
+  DerampQuad cq;
+  float g2c, g1c, g0c;   // G = phi - phi_ref about tm: g2 tc^2 + g1 tc + g0
+  {
+    const DerampQuad refq = {S.ref_a0, S.ref_a1, S.ref_a2};
+    cq = refq;
+    if (xin) cq = deramp_quad(J.kt[xa], J.tref[xa], J.fdc[xa]);
+    const double d2 = cq.a2 - refq.a2, d1 = cq.a1 - refq.a1, d0 = cq.a0 - refq.a0;
+    g2c = (float)d2;
+    g1c = (float)(2.0 * d2 * tm + d1);
+    g0c = (float)((d2 * tm + d1) * tm + d0);
+  }
+  S.ring_gc[x] = make_float4(g2c, g1c, g0c, 0.f);
+
+  // ---- [P4] per-row statistics: one shared azimuth pass where the whole
+  // strip maps to one (line, bin) key inside the slave box's interior
+  for (int ri = tid; ri < nr; ri += RS_NT) {
+    const double L = row_L(J, r_begin + ri);
+    const double Aaz = row_a(S.caz, L) + S.shift, Baz = row_b(S.caz, L);
+    double ylo, yhi;
+    quad_span(Aaz, Baz, S.caz[5], S.col_phat[0], S.col_phat[cN - 1], ylo, yhi);
+    int l0lo, blo, l0hi, bhi;
     split_pos(ylo, l0lo, blo);
     split_pos(yhi, l0hi, bhi);
-    split_pos(xlo, x0lo, xblo);
-    split_pos(xhi, x0hi, xbhi);
-    const bool az_any = !(l0hi < J.sy0 + 5 || l0lo > J.sy1 - 7);
-    const bool rg_any = !(x0hi < J.sx0 + 5 || x0lo > J.sx1 - 7);
-    int lmin = INT32_MAX, lmax = INT32_MIN;
-    if (az_any && rg_any) {
-      lmin = max(l0lo, J.sy0 + 5);
-      lmax = min(l0hi, J.sy1 - 7);
+    const bool fast = (l0lo == l0hi) && (blo == bhi) && l0lo >= J.sy0 + 5 && l0hi <= J.sy1 - 7;
+    RsRow R;
+    R.L0 = l0lo;
+    R.bin = blo | (RS_NOSLOT << 16);
+    R.mode = fast ? 1 : 0;
+    R.rho = R.psif = R.R2 = R.R1 = R.R0 = 0.f;
+    if (fast) {
+      // Psi = sum_j kAz[j] phi_ref(L0 - 5 + j) (FP64) and the taps' moments
+      const DerampQuad refq = {S.ref_a0, S.ref_a1, S.ref_a2};
+      const float *kl = lut.kaz + blo * kTaps;
+      double psi = 0.0, m0 = 0.0, m1 = 0.0, m2 = 0.0;
+#pragma unroll 4
+      for (int j = 0; j < kTaps; j++) {
+        const double w = (double)__ldg(kl + j), u = (double)(j - 5);
+        const double ta = (double)(l0lo - 5 + j - J.s_first_line) * J.dt;
+        psi = fma(w, quad_eval(refq, ta), psi);
+        m0 += w;
+        m1 = fma(w, u, m1);
+        m2 = fma(w, u * u, m2);
+      }
+      const double tc0 = (double)(l0lo - J.s_first_line) * J.dt - tm;
+      const double dt = J.dt;
+      R.rho = reduce_2pi(psi);
+      R.psif = (float)psi;
+      R.R2 = (float)(m0 * tc0 * tc0 + 2.0 * tc0 * dt * m1 + dt * dt * m2);
+      R.R1 = (float)(m0 * tc0 + dt * m1);
+      R.R0 = (float)m0;
     }
-    const bool uniform = (l0lo == l0hi) && (blo == bhi);
-    const bool az_in = l0lo >= J.sy0 + 5 && l0hi <= J.sy1 - 7;
-    // the range pass reads ring columns [p0 - 6, p0 + 8] of its pixels
-    const bool win = (x0lo - 6 - S.xw >= 0) && (x0hi + 8 - S.xw < RS_FW);
-    S.ri_L0[ri] = l0lo;
-    S.ri_bL[ri] = (uniform && az_in && rg_any && win) ? blo : -1;
-    S.ri_lmin[ri] = lmin;
-    S.ri_lmax[ri] = lmax;
+    S.rows[ri] = R;
   }
+  __syncthreads();
 
-  // ---- per-thread constants of the ring / azimuth-pass column pair
-  const int xr0 = 2 * (tid & 63);            // ring columns xr0, xr0 + 1
-  const int xa0 = S.xw + xr0;                // absolute slave columns xa0, xa0 + 1
-  const bool xin0 = xa0 >= J.sx0 && xa0 <= J.sx1;
-  const bool xin1 = xa0 + 1 >= J.sx0 && xa0 + 1 <= J.sx1;
-  const bool pair8 = xin0 && xin1 && J.slave_al8;   // one 8-byte copy per staged row
-  const DerampQuad refq = {S.ref_a0, S.ref_a1, S.ref_a2};
-  const double tm = S.tm;
-  DerampQuad cq0 = refq, cq1 = refq;
-  if (xin0) cq0 = deramp_quad(J.kt[xa0], J.tref[xa0], J.fdc[xa0]);
-  if (xin1) cq1 = deramp_quad(J.kt[xa0 + 1], J.tref[xa0 + 1], J.fdc[xa0 + 1]);
-  // G = phi - phi_ref about tm: g2 tc^2 + g1 tc + g0 (tc = ta - tm)
-  float g2c0, g1c0, g0c0, g2c1, g1c1, g0c1;
+  // ---- [P5] window modes: a row continues the previous row's window when
+  // its line is the next one (slots rotate with the item row)
+  int mode_a = 0, mode_b = 0;
   {
-    const double d2 = cq0.a2 - refq.a2, d1 = cq0.a1 - refq.a1, d0 = cq0.a0 - refq.a0;
-    g2c0 = (float)d2;
-    g1c0 = (float)(2.0 * d2 * tm + d1);
-    g0c0 = (float)((d2 * tm + d1) * tm + d0);
-    const double e2 = cq1.a2 - refq.a2, e1 = cq1.a1 - refq.a1, e0 = cq1.a0 - refq.a0;
-    g2c1 = (float)e2;
-    g1c1 = (float)(2.0 * e2 * tm + e1);
-    g0c1 = (float)((e2 * tm + e1) * tm + e0);
+    auto mode_of = [&](int ri) {
+      const RsRow &R = S.rows[ri];
+      if (!R.mode) return (int)RM_PIXEL;
+      if (ri > 0 && S.rows[ri - 1].mode && S.rows[ri - 1].L0 + 1 == R.L0) return (int)RM_STEADY;
+      return (int)RM_REBUILD;
+    };
+    if (tid < nr) mode_a = mode_of(tid);
+    if (tid + RS_NT < nr) mode_b = mode_of(tid + RS_NT);
   }
+  __syncthreads();
+  if (tid < nr) S.rows[tid].mode = mode_a;
+  if (tid + RS_NT < nr) S.rows[tid + RS_NT].mode = mode_b;
+  __syncthreads();
 
-  // ---- per-thread constants of the range pass (2 columns x 4 rows)
-  const int dcp = tid % RS_DP, drq = tid / RS_DP;
+  // ---- [P6] thread 0: azimuth-bin table, staging plan and slave-line
+  // range; threads 16..127: range-key runs of the columns
+  if (tid == 0) {
+    int nbins = 0, last_bin = -1, last_slot = RS_NOSLOT, ymin = INT32_MAX;
+    for (int ri = 0; ri < nr; ri++) {
+      RsRow &R = S.rows[ri];
+      if (!R.mode) continue;
+      const int b = R.bin & 0xffff;
+      if (b != last_bin) {
+        int slot = RS_NOSLOT;
+        for (int q = 0; q < nbins; q++)
+          if (S.bin_id[q] == b) slot = q;
+        if (slot == RS_NOSLOT && nbins < RS_MAXBIN) {
+          S.bin_id[nbins] = b;
+          slot = nbins++;
+        }
+        last_bin = b;
+        last_slot = slot;
+      }
+      R.bin = b | (last_slot << 16);
+      ymin = min(ymin, R.L0 - 5);
+    }
+    S.nbins = nbins;
+    S.ys0 = ymin == INT32_MAX ? 0 : ymin;
+    // staging plan: the lines each group's window pushes need, copied
+    // before the group (at most RS_SR lines kept)
+    const int ngrp = (nr + RS_GR - 1) / RS_GR;
+    int st_lo = 1, st_hi = 0;
+    for (int g = 0; g < ngrp; g++) {
+      int lo = INT32_MAX, hi = INT32_MIN;
+      for (int k = 0; k < RS_GR && g * RS_GR + k < nr; k++) {
+        const RsRow &R = S.rows[g * RS_GR + k];
+        if (R.mode == RM_STEADY) {
+          lo = min(lo, R.L0 + 6);
+          hi = max(hi, R.L0 + 6);
+        } else if (R.mode == RM_REBUILD) {
+          lo = min(lo, R.L0 - 5);
+          hi = max(hi, R.L0 + 6);
+        }
+      }
+      int c_lo = 1, c_hi = 0;
+      if (lo <= hi) {
+        lo = max(lo, hi - (RS_SR - 1));
+        if (st_lo <= st_hi && lo >= st_lo && lo <= st_hi + 1) {
+          c_lo = st_hi + 1;   // extend the staged window
+          c_hi = hi;
+          st_hi = max(st_hi, hi);
+          st_lo = max(st_lo, st_hi - (RS_SR - 1));
+        } else {
+          c_lo = lo;          // restart it
+          c_hi = hi;
+          st_lo = lo;
+          st_hi = hi;
+        }
+      }
+      S.gplan[g] = make_int4(c_lo, c_hi, st_lo, st_hi);
+    }
+    S.ngrp = ngrp;
+  } else if (tid >= RS_NT - RS_TW) {
+    const int c = tid - (RS_NT - RS_TW);
+    if (c < cN) {
+      // runs of the range key over the item rows, by bisection of the exact
+      // per-pixel key on the pieces where the position is monotone in the row
+      auto keyat = [&](int ri) { return rg_key(S, J, r_begin + ri, c); };
+      int ends[2] = {nr - 1, nr - 1};
+      int np = 1;
+      {
+        // x(L) = g0 + g2 P + g5 P^2 + (g1 + g4 P) L + g3 L^2: vertex in L
+        const double *g = S.crg;
+        const double P = S.col_phat[c];
+        if (g[3] != 0.0) {
+          const double Lv = -(g[1] + g[4] * P) / (2.0 * g[3]);
+          const double rv = Lv / J.invL + J.midL - (double)J.my0 - (double)r_begin;
+          if (rv > 0.0 && rv < (double)(nr - 1)) {
+            ends[0] = (int)rv;
+            np = 2;
+          }
+        }
+      }
+      int n = 0;
+      bool dense = false;
+      int a = 0;
+      for (int pc = 0; pc < np && !dense; pc++) {
+        const int bend = ends[pc];
+        int r = a, k = keyat(a);
+        const int kb = keyat(bend);
+        for (;;) {
+          if (n == RS_MAXRUN) {
+            dense = true;
+            break;
+          }
+          // the run's range weights: phase moments over the ring columns
+          const int p0 = k >> 12, bp = k & 4095;
+          const int xb = p0 - 5 - xw;
+          float4 gg = make_float4(__ldg(lut.sp1 + bp), 0.f, 0.f, 0.f);
+          if (xb >= 0 && xb + kTaps <= RS_FW) {
+            const float *kp = lut.krg + bp * kTaps;
+            float G2 = 0.f, G1 = 0.f, G0 = 0.f;
+#pragma unroll
+            for (int i = 0; i < kTaps; i++) {
+              const float w = __ldg(kp + i);
+              const float4 gc = S.ring_gc[xb + i];
+              G2 = fmaf(w, gc.x, G2);
+              G1 = fmaf(w, gc.y, G1);
+              G0 = fmaf(w, gc.z, G0);
+            }
+            gg.y = G2;
+            gg.z = G1;
+            gg.w = G0;
+          }
+          S.run_rk[c][n] = make_int2(r, k);
+          S.run_g[c][n] = gg;
+          n++;
+          if (k == kb) break;   // monotone: the rest of the piece has this key
+          int lo = r, hi = bend, khi = kb;
+          while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            const int km = keyat(mid);
+            if (km == k) {
+              lo = mid;
+            } else {
+              hi = mid;
+              khi = km;
+            }
+          }
+          r = hi;
+          k = khi;
+        }
+        a = bend + 1;
+      }
+      S.run_n[c] = dense ? -1 : n;
+    }
+  }
+  __syncthreads();
+
+  // ---- [P7] stage the first group's lines; slave-line phase table; the
+  // azimuth taps of the bin table
+  {
+    const int4 p = S.gplan[0];
+    if (p.x <= p.y) stage_rows(S, J, x, xa, xin, p.x, p.y);
+  }
+  {
+    const DerampQuad refq = {S.ref_a0, S.ref_a1, S.ref_a2};
+    for (int i = tid; i < RS_NSR; i += RS_NT) {
+      const int y = S.ys0 + i;
+      const double ta = (double)(y - J.s_first_line) * J.dt;
+      RsSlaveRow sr;
+      sr.ta = ta;
+      sr.rho = kSplit ? reduce_2pi(quad_eval(refq, ta)) : 0.f;
+      sr.tc = (float)(ta - tm);
+      S.srow[i] = sr;
+    }
+  }
+  for (int e = tid; e < S.nbins * 6; e += RS_NT) {
+    const int slot = e / 6, q = e - slot * 6;
+    const float *kl = lut.kaz + S.bin_id[slot] * kTaps + 2 * q;
+    const float a = __ldg(kl), b = __ldg(kl + 1);
+    S.bin_w[slot][q] = make_float4(a, a, b, b);
+  }
+  __syncthreads();
+
+  // ---- range-pass thread: column pair (dc, dc + 1), rows 6h .. 6h + 5 of a group
+  const int dp = tid % RS_DP, dh = tid / RS_DP;
   const bool dthread = tid < RS_DT;
-  const int dc = 2 * dcp;                    // strip-local columns dc, dc + 1
+  const int dc = 2 * dp;
   const bool dval0 = dthread && dc < cN, dval1 = dthread && dc + 1 < cN;
-  ColW cw0, cw1;   // range weights of the two columns, kept across groups
-  cw0.key = -1;
-  cw1.key = -1;
+  const bool dense0 = dval0 && S.run_n[dc] < 0, dense1 = dval1 && S.run_n[dc + 1] < 0;
+  ColRun cr0, cr1;
+  cr0.ok = cr1.ok = false;
+  cr0.next = cr1.next = INT32_MAX;
+  cr0.key = cr1.key = 0;
+  cr0.m = cr1.m = 0;
+  if (dval0 && !dense0) run_load(cr0, S, J, dc, 0);
+  if (dval1 && !dense1) run_load(cr1, S, J, dc + 1, 0);
   const bool out16 = J.out_al16 != 0;
 
-  int loaded_lo = INT32_MIN, loaded_hi = INT32_MIN;  // valid ring rows (uniform)
-  // ---- [A] + row setup of the group starting at row rgp into row table nb,
-  // run by warp 7 (idle in the range pass) one group ahead: the group's row
-  // keys, the ring-row table of the slave lines it brings, the rows the group
-  // after it brings (staged while it computes), and per row the azimuth taps,
-  // their moments and the row phase.  Lanes 0..15 take the rows of group
-  // rgp, lanes 16..31 those of the group after it.
-  auto prep_group = [&](int rgp, int nb) {
-    RsRows &Q = S.rows[nb];
-    {
-      const int half = lane >> 4, r = lane & 15;
-      const int rgx = rgp + half * RS_GR;
-      int v = 0, lmin = INT32_MAX, lmax = INT32_MIN, L0 = 0, bL = 0;
-      if (rgx + r < r_end) {
-        const int ri = rgx - r_begin + r;
-        L0 = S.ri_L0[ri];
-        bL = S.ri_bL[ri];
-        lmin = S.ri_lmin[ri];
-        lmax = S.ri_lmax[ri];
-        v = bL >= 0;
-      }
-      int gmin = lmin, gmax = lmax;
+  // azimuth-pass state: the 12-line window of this ring column (slot of
+  // line L0 - 5 + j at row k of a group: (k + j) % 12) and the current taps
+  float2 w[RS_GR];
 #pragma unroll
-      for (int o = 8; o > 0; o >>= 1) {   // within each half
-        gmin = min(gmin, __shfl_xor_sync(0xffffffffu, gmin, o));
-        gmax = max(gmax, __shfl_xor_sync(0xffffffffu, gmax, o));
-      }
-      const int cmin = __shfl_sync(0xffffffffu, gmin, 0);
-      const int cmax = __shfl_sync(0xffffffffu, gmax, 0);
-      const int nmin = __shfl_sync(0xffffffffu, gmin, 16);
-      const int nmax = __shfl_sync(0xffffffffu, gmax, 16);
-      const bool cok = cmin <= cmax && (cmax - cmin + 12 <= RS_FR);
-      const bool nok = rgp + RS_GR < r_end && nmin <= nmax && (nmax - nmin + 12 <= RS_FR);
-      if (half == 0) {
-        Q.v[r] = v && cok;
-        Q.L0[r] = L0;
-        Q.bL[r] = max(bL, 0);
-      }
-      if (lane == 0) {
-        S.g_lmin = cok ? cmin : 1;
-        S.g_lmax = cok ? cmax : 0;
-        S.pf_lo = S.nx_lo;   // the rows staged for this group
-        S.pf_hi = S.nx_hi;
-      }
-      // ring-row table of the rows this group brings (at most RS_FR rows),
-      // and the ring state after it
-      int ll = loaded_lo, lh = loaded_hi;
-      if (cok) {
-        const int need_lo = cmin - 5, need_hi = cmax + 6;
-        const bool cont = need_lo >= ll && need_lo <= lh + 1;
-        const int new_lo = cont ? lh + 1 : need_lo;
-        const int y = new_lo + lane;
-        if (y <= need_hi) {
-          const int slot = y & (RS_FR - 1);
-          const double ta = (double)(y - J.s_first_line) * J.dt;
-          const double phref = quad_eval(refq, ta);
-          S.ring_phiref[slot] = phref;
-          S.ring_ta[slot] = ta;
-          S.ring_rho[slot] = reduce_2pi(phref);
-          S.ring_tc[slot] = (float)(ta - tm);
-        }
-        if (!cont) ll = need_lo;
-        lh = max(lh, need_hi);
-        ll = max(ll, lh - RS_FR + 1);
-      }
-      if (lane == 0) {
-        int lo = 1, hi = 0;
-        if (nok) {
-          const int need_lo = nmin - 5, need_hi = nmax + 6;
-          const bool cont = need_lo >= ll && need_lo <= lh + 1;
-          lo = cont ? lh + 1 : need_lo;
-          hi = need_hi;
-        }
-        S.nx_lo = lo;
-        S.nx_hi = hi;
-      }
-    }
-    __syncwarp();
-    // azimuth taps (w, w) pairs, their moments M0..M2 and the row phase
-    // Psi = sum_j kAz[j] phi_ref(L0 - 5 + j): 8 lanes per row, 4 rows per
-    // pass; lane j < 6 takes taps 2j, 2j+1
-#pragma unroll 1
-    for (int r = lane >> 3; r < RS_GR; r += 4) {
-      const int j = lane & 7;
-      const bool rv = Q.v[r] != 0;
-      float m0 = 0.f, m1 = 0.f, m2 = 0.f;
-      double psi = 0.0;
-      if (rv && j < kTaps / 2) {
-        const int L0 = Q.L0[r];
-        const float *kl = lut.kaz + Q.bL[r] * kTaps + 2 * j;
-        const float w0 = __ldg(kl), w1 = __ldg(kl + 1);
-        S.wpair[r][j] = make_float4(w0, w0, w1, w1);
-        const float u0 = (float)(2 * j - 5), u1 = (float)(2 * j - 4);
-        m0 = w0 + w1;
-        m1 = fmaf(w0, u0, w1 * u1);
-        m2 = fmaf(w0, u0 * u0, w1 * (u1 * u1));
-        psi = fma((double)w0, S.ring_phiref[(L0 - 5 + 2 * j) & (RS_FR - 1)],
-                  (double)w1 * S.ring_phiref[(L0 - 4 + 2 * j) & (RS_FR - 1)]);
-      }
+  for (int j = 0; j < RS_GR; j++) w[j] = make_float2(0.f, 0.f);
+  float4 wz[6];
 #pragma unroll
-      for (int o = 4; o > 0; o >>= 1) {
-        m0 += __shfl_xor_sync(0xffffffffu, m0, o);
-        m1 += __shfl_xor_sync(0xffffffffu, m1, o);
-        m2 += __shfl_xor_sync(0xffffffffu, m2, o);
-        psi += __shfl_xor_sync(0xffffffffu, psi, o);
-      }
-      if (rv && j == 0) {
-        const double tc = (double)(Q.L0[r] - J.s_first_line) * J.dt - tm;
-        S.row_M0[r] = m0;
-        S.row_P1[r] = (float)(2.0 * tc * J.dt * m1 + J.dt * J.dt * m2);
-        S.row_P2[r] = (float)(J.dt * m1);
-        Q.rho[r] = reduce_2pi(psi);
-        Q.psif[r] = (float)psi;
-      }
-    }
-  };
-  __syncthreads();
-  if (tid >= RS_DT) prep_group(r_begin, 0);
-  __syncthreads();
+  for (int q = 0; q < 6; q++) wz[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+  int wz_bin = -1;
 
-  int buf = 0;   // row table of the current group
-  for (int rg = r_begin; rg < r_end; rg += RS_GR, buf ^= 1) {
-    const int gr = min(RS_GR, r_end - rg);
-    const RsRows &R = S.rows[buf];
-    // ---- [B] ring loads of the new slave rows (2 columns per thread)
-    const int glmin = S.g_lmin, glmax = S.g_lmax;
-    const bool ring_ok = glmin <= glmax;
-    // Raw slave rows [lo, hi] (at most RS_FR) into the staging rows: this
-    // thread copies its column pair of rows lo + rp + 4u to stage[4u + rp];
-    // zeros outside the slave box.  The job fields are read once per call;
-    // the source offset and the destination step by 4 rows per copy.
-    const int rp = tid >> 6;   // row phase
-    auto stage_rows = [&](int lo, int hi) {
-      hi = min(hi, lo + RS_FR - 1);
-      int y = lo + rp;
-      if (y <= hi) {
-        const short2 *const sl = J.slave;
-        const long pitch = J.slave_pitch;
-        const int sy0 = J.sy0;
-        const unsigned rows_in = (unsigned)(J.sy1 - J.sy0);
-        long off = (long)(y - sy0) * pitch + (xa0 - J.sx0);
-        unsigned dst = smem_u32(&S.stage[rp][xr0]);
-        constexpr unsigned kStep = 4u * RS_FW * sizeof(short2);
-        if (pair8) {
-#pragma unroll 4
-          for (; y <= hi; y += 4, off += 4 * pitch, dst += kStep) {
-            const bool yin = (unsigned)(y - sy0) <= rows_in;
-            cp_async_8s(dst, sl + (yin ? off : 0), yin ? 8 : 0);
+  const int ngrp = S.ngrp;
+  for (int g = 0; g < ngrp; g++) {
+    const int rg0 = g * RS_GR;            // first item row of the group
+    const int buf = g & 1;
+    const int4 plan = S.gplan[g];
+    cp_async_wait_all();                  // this thread's staged lines of the group
+    // ---- [A] azimuth pass of the group's rows
+#pragma unroll
+    for (int k = 0; k < RS_GR; k++) {
+      const int ri = rg0 + k;
+      if (ri < nr) {
+        const RsRow &R = S.rows[ri];
+        const int mode = R.mode;
+        if (mode != RM_PIXEL) {
+          const int L0 = R.L0;
+          if (mode == RM_STEADY) {
+            w[(k + 11) % RS_GR] = deramp_at<kSplit>(S, J, x, xa, xin, L0 + 6, plan.z, plan.w,
+                                                    g2c, g1c, g0c, cq);
+          } else {
+#pragma unroll
+            for (int j = 0; j < RS_GR; j++)
+              w[(k + j) % RS_GR] = deramp_at<kSplit>(S, J, x, xa, xin, L0 - 5 + j, plan.z,
+                                                     plan.w, g2c, g1c, g0c, cq);
           }
-        } else {
-#pragma unroll 1
-          for (; y <= hi; y += 4, off += 4 * pitch, dst += kStep) {
-            const bool yin = (unsigned)(y - sy0) <= rows_in;
-            const bool i0 = yin && xin0, i1 = yin && xin1;
-            cp_async_4s(dst, sl + (i0 ? off : 0), i0 ? 4 : 0);
-            cp_async_4s(dst + 4, sl + (i1 ? off + 1 : 0), i1 ? 4 : 0);
+          const int bin = R.bin;
+          if (bin != wz_bin) {
+            load_az_taps(S, lut, bin, wz);
+            wz_bin = bin;
           }
+          float2 a = make_float2(0.f, 0.f), b = a;
+#pragma unroll
+          for (int j = 0; j < RS_GR; j += 2) {
+            const float4 q = wz[j >> 1];
+            a = __ffma2_rn(make_float2(q.x, q.y), w[(k + j) % RS_GR], a);
+            b = __ffma2_rn(make_float2(q.z, q.w), w[(k + j + 1) % RS_GR], b);
+          }
+          S.vd[buf][k][x] = __fadd2_rn(a, b);
         }
       }
-      cp_async_commit();
-    };
-    // this thread's copies for the group (staged during the previous one)
-    cp_async_wait_all();
-    if (ring_ok) {
-      const int need_lo = glmin - 5, need_hi = glmax + 6;
-      const bool cont = need_lo >= loaded_lo && need_lo <= loaded_hi + 1;
-      const int new_lo = cont ? loaded_hi + 1 : need_lo;
-      if (S.pf_lo != new_lo || S.pf_hi != need_hi) {
-        // not staged (first group of the item): copy now and wait
-        stage_rows(new_lo, need_hi);
-        cp_async_wait_all();
-      }
-      // deramp of the new rows (column pair of this thread) into the ring
-      const int sy0 = J.sy0;
-      const unsigned rows_in = (unsigned)(J.sy1 - J.sy0);
-      const int last = min(need_hi, new_lo + RS_FR - 1);
-#pragma unroll 2
-      for (int y = new_lo + rp, u4 = rp; y <= last; y += 4, u4 += 4) {
-        const int slot = y & (RS_FR - 1);
-        const short4 ab = *reinterpret_cast<const short4 *>(&S.stage[u4][xr0]);
-        const short2 a = make_short2(ab.x, ab.y), b = make_short2(ab.z, ab.w);
-        float2 d0 = make_float2(0.f, 0.f), d1 = d0;
-        float G0 = 0.f, G1 = 0.f;
-        if ((unsigned)(y - sy0) <= rows_in) {
-          float r0, r1;
-          if (kSplit) {
-            const float tc = S.ring_tc[slot], rho = S.ring_rho[slot];
-            G0 = fmaf(fmaf(g2c0, tc, g1c0), tc, g0c0);
-            G1 = fmaf(fmaf(g2c1, tc, g1c1), tc, g0c1);
-            r0 = reduce_2pi_f(rho + G0);
-            r1 = reduce_2pi_f(rho + G1);
-          } else {
-            const double ta = S.ring_ta[slot], phref = S.ring_phiref[slot];
-            const double p0 = quad_eval(cq0, ta), p1 = quad_eval(cq1, ta);
-            G0 = (float)(p0 - phref);
-            G1 = (float)(p1 - phref);
-            r0 = reduce_2pi(p0);
-            r1 = reduce_2pi(p1);
-          }
-          float sn, cs;
-          if (xin0) {
-            __sincosf(r0, &sn, &cs);
-            d0.x = (float)a.x * cs - (float)a.y * sn;
-            d0.y = (float)a.x * sn + (float)a.y * cs;
-          } else {
-            G0 = 0.f;
-          }
-          if (xin1) {
-            __sincosf(r1, &sn, &cs);
-            d1.x = (float)b.x * cs - (float)b.y * sn;
-            d1.y = (float)b.x * sn + (float)b.y * cs;
-          } else {
-            G1 = 0.f;
-          }
-        }
-        *reinterpret_cast<float4 *>(&S.ring_d[slot][xr0]) = make_float4(d0.x, d0.y, d1.x, d1.y);
-        *reinterpret_cast<float2 *>(&S.ring_g[slot][xr0]) = make_float2(G0, G1);
-      }
-      if (!cont) loaded_lo = need_lo;
-      loaded_hi = max(loaded_hi, need_hi);
-      loaded_lo = max(loaded_lo, loaded_hi - RS_FR + 1);
     }
-    // stage the next group's new rows (the staged values above are consumed:
-    // their ring stores are issued); they land while this group computes
-    if (S.nx_lo <= S.nx_hi) stage_rows(S.nx_lo, S.nx_hi);
-    __syncthreads();
-
-    // ---- [C] shared azimuth pass: 2 ring columns x 4 rows per thread
-    {
-      const int q = tid >> 6;      // rows 4q .. 4q+3
-      const int r0 = 4 * q;
-      if (r0 < gr) {
-        const int L00 = R.L0[r0];
-        bool blk = r0 + 4 <= gr;
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-          const int r = min(r0 + k, RS_GR - 1);
-          blk = blk && R.v[r] && R.L0[r] == L00 + k;
-        }
-        if (blk) {
-          float2 a0[4], a1[4];
-#pragma unroll
-          for (int k = 0; k < 4; k++) a0[k] = a1[k] = make_float2(0.f, 0.f);
-#pragma unroll
-          for (int jj = 0; jj < kTaps + 3; jj++) {
-            const float4 dd =
-                *reinterpret_cast<const float4 *>(&S.ring_d[(L00 - 5 + jj) & (RS_FR - 1)][xr0]);
-            const float2 e0 = make_float2(dd.x, dd.y), e1 = make_float2(dd.z, dd.w);
-#pragma unroll
-            for (int k = 0; k < 4; k++) {
-              const int j = jj - k;
-              if (j >= 0 && j < kTaps) {
-                const float4 wp = S.wpair[r0 + k][j >> 1];
-                const float2 w = (j & 1) ? make_float2(wp.z, wp.w) : make_float2(wp.x, wp.y);
-                a0[k] = __ffma2_rn(w, e0, a0[k]);
-                a1[k] = __ffma2_rn(w, e1, a1[k]);
-              }
-            }
-          }
-          float vg0[4], vg1[4];
-#pragma unroll
-          for (int k = 0; k < 4; k++) {
-            const int r = r0 + k;
-            const float2 gc =
-                *reinterpret_cast<const float2 *>(&S.ring_g[(L00 + k) & (RS_FR - 1)][xr0]);
-            const float M0 = S.row_M0[r], P1 = S.row_P1[r], P2 = S.row_P2[r];
-            vg0[k] = fmaf(M0, gc.x, fmaf(g2c0, P1, g1c0 * P2));
-            vg1[k] = fmaf(M0, gc.y, fmaf(g2c1, P1, g1c1 * P2));
-            *reinterpret_cast<float4 *>(&S.vd[r][xr0]) =
-                make_float4(a0[k].x, a0[k].y, a1[k].x, a1[k].y);
-          }
-          *reinterpret_cast<float4 *>(&S.vgp[2 * q][xr0]) =
-              make_float4(vg0[0], vg0[1], vg1[0], vg1[1]);
-          *reinterpret_cast<float4 *>(&S.vgp[2 * q + 1][xr0]) =
-              make_float4(vg0[2], vg0[3], vg1[2], vg1[3]);
-        } else {
-#pragma unroll 1
-          for (int k = 0; k < 4 && r0 + k < gr; k++) {
-            const int r = r0 + k;
-            if (!R.v[r]) continue;
-            const int L0 = R.L0[r];
-            float2 a0 = make_float2(0.f, 0.f), a1 = a0;
-#pragma unroll
-            for (int j = 0; j < kTaps; j++) {
-              const float4 wp = S.wpair[r][j >> 1];
-              const float2 w = (j & 1) ? make_float2(wp.z, wp.w) : make_float2(wp.x, wp.y);
-              const float4 dd =
-                  *reinterpret_cast<const float4 *>(&S.ring_d[(L0 - 5 + j) & (RS_FR - 1)][xr0]);
-              a0 = __ffma2_rn(w, make_float2(dd.x, dd.y), a0);
-              a1 = __ffma2_rn(w, make_float2(dd.z, dd.w), a1);
-            }
-            const float2 gc =
-                *reinterpret_cast<const float2 *>(&S.ring_g[L0 & (RS_FR - 1)][xr0]);
-            const float M0 = S.row_M0[r], P1 = S.row_P1[r], P2 = S.row_P2[r];
-            float *vg = reinterpret_cast<float *>(&S.vgp[r >> 1][xr0]) + (r & 1);
-            vg[0] = fmaf(M0, gc.x, fmaf(g2c0, P1, g1c0 * P2));
-            vg[2] = fmaf(M0, gc.y, fmaf(g2c1, P1, g1c1 * P2));
-            *reinterpret_cast<float4 *>(&S.vd[r][xr0]) = make_float4(a0.x, a0.y, a1.x, a1.y);
-          }
-        }
-      }
+    // stage the next group's new lines; they land while [B] runs
+    if (g + 1 < ngrp) {
+      const int4 pn = S.gplan[g + 1];
+      if (pn.x <= pn.y) stage_rows(S, J, x, xa, xin, pn.x, pn.y);
     }
     __syncthreads();
 
-    // ---- [D] range pass, reramp, store: 2 columns x 4 rows per thread
-    if (dthread) {
-#pragma unroll 2
-      for (int h = 0; h < 2; h++) {
-        const int ra = 4 * drq + 2 * h;     // rows ra, ra + 1 (ra even)
-        if (ra >= gr) break;
-        const bool two = ra + 1 < gr;
-        // range keys of the 2 x 2 pixels
-        // (entries beyond cN - 1 hold the last column's terms)
-        int p0v[2][2], bpv[2][2];
-        const double2 cph = *reinterpret_cast<const double2 *>(&S.col_phat[dc]);
-        const double2 cq = *reinterpret_cast<const double2 *>(&S.col_qrg[dc]);
+    // ---- [B] range pass, reramp, store: 2 columns x 6 rows per thread
+    if (dval0) {
+#pragma unroll 1
+      for (int kk = 0; kk < RS_HR; kk++) {
+        const int k = dh * RS_HR + kk;
+        const int ri = rg0 + k;
+        if (ri >= nr) break;
+        while (ri >= cr0.next) run_load(cr0, S, J, dc, cr0.m + 1);
+        while (ri >= cr1.next) run_load(cr1, S, J, dc + 1, cr1.m + 1);
+        const RsRow R = S.rows[ri];
+        const int r = r_begin + ri;       // box row
+        float2 *orow = J.out + (long)(r - J.row0) * J.out_pitch + c0 + dc;
+        const float2 *vrow = &S.vd[buf][k][0];
+        const bool rfast = R.mode != RM_PIXEL;
+        const bool ok0 = rfast && !dense0 && cr0.ok;
+        const bool ok1 = rfast && dval1 && !dense1 && cr1.ok;
+        const int xb0 = (cr0.key >> 12) - 5 - xw;
+        if (ok0 && ok1 && (cr1.key >> 12) == (cr0.key >> 12) + 1) {
+          const int base = xb0 & ~1;
+          const bool odd = (xb0 & 1) != 0;
+          float2 V[14];
+          const float4 *p = reinterpret_cast<const float4 *>(vrow + base);
 #pragma unroll
-        for (int k = 0; k < 2; k++) {
-          const int ri = rg - r_begin + ra + k;
-          const double A = S.rowA_rg[ri], Bc = S.rowB_rg[ri];
-          split_pos(fma(Bc, cph.x, A + cq.x), p0v[k][0], bpv[k][0]);
-          split_pos(fma(Bc, cph.y, A + cq.y), p0v[k][1], bpv[k][1]);
-        }
-        // Fast pair: both rows with a shared azimuth pass, each row's two
-        // pixels interior, adjacent (p0 steps by one) and inside the ring
-        // window.  A column's range key may change between the two rows
-        // (about once per 100 rows); its weights are then reloaded for the
-        // second row and its phase residual is interpolated per row.
-        bool fast = two && dval1 && out16 && R.v[ra] && R.v[ra + 1];
-#pragma unroll
-        for (int k = 0; k < 2; k++) {
-          const int xbk = p0v[k][0] - 5 - S.xw;
-          fast = fast && p0v[k][1] == p0v[k][0] + 1 && p0v[k][0] >= J.sx0 + 5 &&
-                 p0v[k][1] <= J.sx1 - 7 && xbk >= 1 && xbk + 13 < RS_FW;
-        }
-        if (fast) {
-          const int key00 = (p0v[0][0] << 12) | bpv[0][0], key01 = (p0v[0][1] << 12) | bpv[0][1];
-          const int key10 = (p0v[1][0] << 12) | bpv[1][0], key11 = (p0v[1][1] << 12) | bpv[1][1];
-          const bool same = key00 == key10 && key01 == key11;
-          float2 acc[2][2];
-          float sg[2][2];
-#pragma unroll
-          for (int k = 0; k < 2; k++) {
-            colw_load(cw0, lut, k ? key10 : key00);
-            colw_load(cw1, lut, k ? key11 : key01);
-            const int xb = p0v[k][0] - 5 - S.xw;   // ring column of the first tap
-            const int base = xb & ~1;              // 16-byte aligned start
-            const bool odd = (xb & 1) != 0;
-            {
-              float2 V[14];
-              load14(&S.vd[ra + k][0], base, V);
-              range_pair(cw0, cw1, V, odd, acc[k][0], acc[k][1]);
-            }
-            // phase residuals from the (row ra, row ra+1) pairs: both rows
-            // at once when the keys agree, else each row with its weights
-            if (k == 0 || !same) {
-              float2 Gp[14], g0, g1;
-              load14(&S.vgp[ra >> 1][0], base, Gp);
-              range_pair(cw0, cw1, Gp, odd, g0, g1);
-              if (k == 0) {
-                sg[0][0] = g0.x;
-                sg[0][1] = g1.x;
-                sg[1][0] = g0.y;
-                sg[1][1] = g1.y;
-              } else {
-                sg[1][0] = g0.y;
-                sg[1][1] = g1.y;
-              }
-            }
+          for (int m = 0; m < 7; m++) {
+            const float4 t = p[m];
+            V[2 * m] = make_float2(t.x, t.y);
+            V[2 * m + 1] = make_float2(t.z, t.w);
           }
-#pragma unroll
-          for (int k = 0; k < 2; k++) {
-            const int r = ra + k;
-            const float rho = R.rho[r], psif = R.psif[r];
-            // sp1 of the column's row-k bin (cw holds row 1's weights now)
-            const float sp0 = (k == 0 && !same) ? __ldg(lut.sp1 + bpv[0][0]) : cw0.sp1;
-            const float sp1 = (k == 0 && !same) ? __ldg(lut.sp1 + bpv[0][1]) : cw1.sp1;
-            const float2 o0 = cmul_conj_phase(acc[k][0], rho + sp0 * psif + sg[k][0]);
-            const float2 o1 = cmul_conj_phase(acc[k][1], rho + sp1 * psif + sg[k][1]);
-            float2 *orow = J.out + (long)(rg + r - J.row0) * J.out_pitch + c0 + dc;
+          float2 s0, s1;
+          range_pair(cr0, cr1, V, odd, s0, s1);
+          const float2 o0 = cmul_conj_phase(s0, run_phase(R, cr0));
+          const float2 o1 = cmul_conj_phase(s1, run_phase(R, cr1));
+          if (out16) {
             *reinterpret_cast<float4 *>(orow) = make_float4(o0.x, o0.y, o1.x, o1.y);
+          } else {
+            orow[0] = o0;
+            orow[1] = o1;
           }
         } else {
-          // per pixel: any region, any key
-#pragma unroll 1
-          for (int k = 0; k < 2; k++) {
-            const int r = ra + k;
-            if (r >= gr) break;
-            const int ri = rg - r_begin + r;
-            const bool rv = R.v[r];
-#pragma unroll 1
-            for (int c = 0; c < 2; c++) {
-              if (!(c ? dval1 : dval0)) continue;
-              const int col = dc + c;
-              int l0, bl;
-              if (rv) {
-                l0 = R.L0[r];
-                bl = R.bL[r];
-              } else {
-                const double y =
-                    fma(S.rowB_az[ri], S.col_phat[col], S.rowA_az[ri] + S.col_qaz[col]);
-                split_pos(y, l0, bl);
-              }
-              // (selects, not a dynamic index: keeps p0v / bpv in registers)
-              const int p0 = k ? (c ? p0v[1][1] : p0v[1][0]) : (c ? p0v[0][1] : p0v[0][0]);
-              const int bp = k ? (c ? bpv[1][1] : bpv[1][0]) : (c ? bpv[0][1] : bpv[0][0]);
-              const int reg = region_of(J, l0, p0);
-              float2 res = make_float2(0.f, 0.f);
-              if (reg == REG_EDGE) {
-                const short2 sv = J.slave[(long)(l0 - J.sy0) * J.slave_pitch + (p0 - J.sx0)];
-                res = make_float2((float)sv.x, (float)sv.y);
-              } else if (reg == REG_IN) {
-                const int xbp = p0 - 5 - S.xw;
-                const bool in_win = xbp >= 0 && xbp + kTaps <= RS_FW;
-                if (rv && in_win) {
-                  if (c) {
-                    colw_load(cw1, lut, (p0 << 12) | bp);
-                    res = range_pixel(S, R, cw1, r, xbp);
-                  } else {
-                    colw_load(cw0, lut, (p0 << 12) | bp);
-                    res = range_pixel(S, R, cw0, r, xbp);
-                  }
-                } else if (ring_ok && in_win && l0 - 5 >= loaded_lo && l0 + 6 <= loaded_hi) {
-                  res = interior_from_ring(S, lut, J, refq, l0, bl, p0, bp);
-                } else {
-                  res = interior_from_global(J, lut, l0, bl, p0, bp);
-                }
-              }
-              J.out[(long)(rg + r - J.row0) * J.out_pitch + c0 + col] = res;
-            }
+          // per column: single fast range pass, else the per-pixel path
+          orow[0] = ok0 ? cmul_conj_phase(range_single(vrow, xb0, cr0), run_phase(R, cr0))
+                        : pixel_generic(S, J, r, dc);
+          if (dval1) {
+            const int xb1 = (cr1.key >> 12) - 5 - xw;
+            orow[1] = ok1 ? cmul_conj_phase(range_single(vrow, xb1, cr1), run_phase(R, cr1))
+                          : pixel_generic(S, J, r, dc + 1);
           }
         }
       }
-    } else if (rg + RS_GR < r_end) {
-      prep_group(rg + RS_GR, buf ^ 1);
     }
-    __syncthreads();
   }
+  __syncthreads();   // the next item's prologue rewrites the tables
 }
 
 template <bool kSplit>
-__global__ void __launch_bounds__(RS_NT, 2)
+__global__ void __launch_bounds__(RS_NT, 3)
     resample_kernel(const __grid_constant__ RsBatch B) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   RsShared &S = *reinterpret_cast<RsShared *>(smem_raw);
@@ -1111,7 +1056,7 @@ static int launch_resample_t(const ResampleJob *jobs, int njobs, const TileCfg &
       },
       &resident);
   if (s0 != TOPS_OK) return s0;
-  if (cfg.seg_rows < 0 || cfg.seg_rows > RS_SEG || (cfg.seg_rows && cfg.seg_rows < RS_GR))
+  if (cfg.seg_rows < 0 || cfg.seg_rows > RS_MAXSEG || (cfg.seg_rows && cfg.seg_rows < RS_GR))
     return TOPS_E_INVALID;
   for (int j0 = 0, k = 0; j0 < njobs; j0 += RS_MAXJOBS, k++) {
     RsBatch B;
