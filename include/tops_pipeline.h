@@ -165,7 +165,7 @@ typedef struct tops_batch tops_batch;
 
 /* Tile and scheduling of the resample and coherence launches. */
 typedef struct {
-  int rs_seg_rows;      /* resample output rows per work item, 16..256 (0: 256) */
+  int rs_seg_rows;      /* resample output rows per work item, 12..252 (0: 252) */
   int rs_persistent;    /* 1: persistent kernel pulling items from a queue */
   int coh_seg_rows;     /* coherence rows per work item, 8..512 (0: 128) */
   int coh_persistent;

@@ -3,7 +3,7 @@
 // (rows per item) and the scheduling mode.
 //
 //   seg_rows  output rows per work item (0: the kernel's default); the
-//             resample kernel takes 16..256, the coherence kernel 8..512
+//             resample kernel takes 12..252, the coherence kernel 8..512
 //   counters  if non-null: persistent launch.  `grid` CTAs (0: as many as
 //             fit on the device at once) pull work items from a queue -- the
 //             device int counters[k], set to 0 on the stream before the k-th

@@ -81,7 +81,7 @@ constexpr int RS_MAXSEG = 252;             // per-item tables are sized for this
 constexpr int RS_NGRP = (RS_MAXSEG + RS_GR - 1) / RS_GR;
 constexpr int RS_SR = 32;                  // staged slave lines (power of two)
 constexpr int RS_NSR = RS_MAXSEG + 44;     // slave-line phase table
-constexpr int RS_MAXRUN = 4;               // range-key runs per column and item
+constexpr int RS_MAXRUN = 6;               // range-key runs per column and item
 constexpr int RS_MAXBIN = 16;              // distinct azimuth bins per item
 constexpr int RS_NOSLOT = 0x7fff;          // azimuth bin outside the bin table
 constexpr int RS_MAXJOBS = 32;
@@ -113,10 +113,13 @@ struct __align__(16) RsRow {
                              // RM_REBUILD: the window is filled anew
 };
 
-// Deramp terms of one slave line.
-struct RsSlaveRow {
-  double ta;                 // burst-local azimuth time
-  float rho, tc;             // reference-column phase mod 2 pi; ta - tm
+// Deramp terms of one slave line: the burst-local azimuth time (FP64
+// mode), or the reference-column phase mod 2 pi and ta - tm (split mode).
+union RsSlaveRow {
+  double ta;
+  struct {
+    float rho, tc;
+  } f;
 };
 
 struct __align__(16) RsShared {
@@ -133,6 +136,8 @@ struct __align__(16) RsShared {
   alignas(16) double col_phat[RS_TW];
   double col_qaz[RS_TW], col_qrg[RS_TW];
   int4 gplan[RS_NGRP];                // per group: lines to stage before it, staged window
+  int2 grange[RS_NGRP];               // per group: lines its window pushes need
+  int scan[RS_NT / 32];               // per-warp totals of the bin-change scan
   double caz[6], crg[6], shift;
   double ref_a0, ref_a1, ref_a2, tm;
   int xw, ys0, nbins, ngrp, next_item;
@@ -327,6 +332,26 @@ __device__ __forceinline__ void run_load(ColRun &cr, const RsShared &S, const Re
   }
 }
 
+// The run state of a column whose keys are taken per pixel (more key runs
+// than the table holds): weights and phase terms of `key`.
+__device__ __forceinline__ void run_from_key(ColRun &cr, const RsShared &S, const ResampleJob &J,
+                                             int key, float4 terms) {
+  cr.key = key;
+  cr.next = INT32_MAX;
+  cr.sp = terms.x;
+  cr.G2 = terms.y;
+  cr.G1 = terms.z;
+  cr.G0 = terms.w;
+  const int p0 = key >> 12, bp = key & 4095;
+  const int xb = p0 - 5 - S.xw;
+  cr.ok = p0 >= J.sx0 + 5 && p0 <= J.sx1 - 7 && xb >= 0 && xb + 13 < RS_FW;
+  if (cr.ok) {
+    const float4 *kp4 = J.lut.krg2 + bp * (kTaps / 2);
+#pragma unroll
+    for (int q = 0; q < kTaps / 2; q++) cr.w[q] = __ldg(kp4 + q);
+  }
+}
+
 __device__ __forceinline__ float2 wtap(const ColRun &cr, int i) {
   const float4 q = cr.w[i >> 1];
   return (i & 1) ? make_float2(q.z, q.w) : make_float2(q.x, q.y);
@@ -401,8 +426,8 @@ __device__ __forceinline__ float2 deramp_at(const RsShared &S, const ResampleJob
   if (kSplit) {
     float rho, tc;
     if ((unsigned)iy < (unsigned)RS_NSR) {
-      rho = S.srow[iy].rho;
-      tc = S.srow[iy].tc;
+      rho = S.srow[iy].f.rho;
+      tc = S.srow[iy].f.tc;
     } else {
       const DerampQuad refq = {S.ref_a0, S.ref_a1, S.ref_a2};
       const double ta = (double)(y - J.s_first_line) * J.dt;
@@ -452,6 +477,31 @@ __device__ __forceinline__ void stage_rows(RsShared &S, const ResampleJob &J, in
     cp_async_4s(smem_u32(&S.stage[y & (RS_SR - 1)][x]), sl + (in ? off : 0), in ? 4 : 0);
   }
   cp_async_commit();
+}
+
+// Phase terms of a range-key run: (sp, G2, G1, G0) with Gk = sum_i kRg[i]
+// gk(x_i) over the ring columns of its taps (0 when they leave the window).
+__device__ __forceinline__ float4 run_terms(const RsShared &S, const RsLut &lut, int xw,
+                                            int key) {
+  const int p0 = key >> 12, bp = key & 4095;
+  const int xb = p0 - 5 - xw;
+  float4 gg = make_float4(__ldg(lut.sp1 + bp), 0.f, 0.f, 0.f);
+  if (xb >= 0 && xb + kTaps <= RS_FW) {
+    const float *kp = lut.krg + bp * kTaps;
+    float G2 = 0.f, G1 = 0.f, G0 = 0.f;
+#pragma unroll
+    for (int i = 0; i < kTaps; i++) {
+      const float w = __ldg(kp + i);
+      const float4 gc = S.ring_gc[xb + i];
+      G2 = fmaf(w, gc.x, G2);
+      G1 = fmaf(w, gc.y, G1);
+      G0 = fmaf(w, gc.z, G0);
+    }
+    gg.y = G2;
+    gg.z = G1;
+    gg.w = G0;
+  }
+  return gg;
 }
 
 // One work item (strip x segment of one job); all threads of the CTA call it
@@ -520,6 +570,7 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
     // one column of margin for the position's variation inside the strip
     const int xw = (int)floor(pmin) - 6;
     S.xw = xw;
+    S.ys0 = INT32_MAX;   // first slave line used: minimum taken in [P6a]
     const int xr = min(max(xw + RS_FW / 2, J.sx0), J.sx1);
     const DerampQuad q = deramp_quad(J.kt[xr], J.tref[xr], J.fdc[xr]);
     S.ref_a0 = q.a0;
@@ -608,38 +659,37 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
   if (tid + RS_NT < nr) S.rows[tid + RS_NT].mode = mode_b;
   __syncthreads();
 
-  // ---- [P6] thread 0: azimuth-bin table, staging plan and slave-line
-  // range; threads 16..127: range-key runs of the columns
-  if (tid == 0) {
-    int nbins = 0, last_bin = -1, last_slot = RS_NOSLOT, ymin = INT32_MAX;
-    for (int ri = 0; ri < nr; ri++) {
-      RsRow &R = S.rows[ri];
-      if (!R.mode) continue;
-      const int b = R.bin & 0xffff;
-      if (b != last_bin) {
-        int slot = RS_NOSLOT;
-        for (int q = 0; q < nbins; q++)
-          if (S.bin_id[q] == b) slot = q;
-        if (slot == RS_NOSLOT && nbins < RS_MAXBIN) {
-          S.bin_id[nbins] = b;
-          slot = nbins++;
-        }
-        last_bin = b;
-        last_slot = slot;
-      }
-      R.bin = b | (last_slot << 16);
-      ymin = min(ymin, R.L0 - 5);
+  // ---- [P6a] azimuth-bin table (a slot per change of the bin between
+  // consecutive rows, ranked by a block-wide scan), each group's line
+  // range, the first slave line used; thread t takes rows 2t and 2t + 1
+  {
+    const int lane = tid & 31, warp = tid >> 5;
+    const int r0 = 2 * tid, r1 = r0 + 1;
+    auto bin_change = [&](int ri) -> int {
+      if (ri >= nr || !S.rows[ri].mode) return 0;
+      if (ri == 0 || !S.rows[ri - 1].mode) return 1;
+      return (S.rows[ri - 1].bin & 0xffff) != (S.rows[ri].bin & 0xffff) ? 1 : 0;
+    };
+    const int f0 = bin_change(r0), f1 = bin_change(r1);
+    int v = f0 + f1;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += t;
     }
-    S.nbins = nbins;
-    S.ys0 = ymin == INT32_MAX ? 0 : ymin;
-    // staging plan: the lines each group's window pushes need, copied
-    // before the group (at most RS_SR lines kept)
+    if (lane == 31) S.scan[warp] = v;
+    int ymin = INT32_MAX;
+    if (r0 < nr && S.rows[r0].mode) ymin = S.rows[r0].L0 - 5;
+    if (r1 < nr && S.rows[r1].mode) ymin = min(ymin, S.rows[r1].L0 - 5);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) ymin = min(ymin, __shfl_xor_sync(0xffffffffu, ymin, o));
+    if (lane == 0 && ymin != INT32_MAX) atomicMin(&S.ys0, ymin);
+    // lines the pushes of group g need (thread g)
     const int ngrp = (nr + RS_GR - 1) / RS_GR;
-    int st_lo = 1, st_hi = 0;
-    for (int g = 0; g < ngrp; g++) {
+    if (tid < ngrp) {
       int lo = INT32_MAX, hi = INT32_MIN;
-      for (int k = 0; k < RS_GR && g * RS_GR + k < nr; k++) {
-        const RsRow &R = S.rows[g * RS_GR + k];
+      for (int k = 0; k < RS_GR && tid * RS_GR + k < nr; k++) {
+        const RsRow &R = S.rows[tid * RS_GR + k];
         if (R.mode == RM_STEADY) {
           lo = min(lo, R.L0 + 6);
           hi = max(hi, R.L0 + 6);
@@ -648,6 +698,43 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
           hi = max(hi, R.L0 + 6);
         }
       }
+      S.grange[tid] = make_int2(lo, hi);
+    }
+    __syncthreads();
+    int off = 0, total = 0;
+#pragma unroll
+    for (int q = 0; q < RS_NT / 32; q++) {
+      const int t = S.scan[q];
+      off += q < warp ? t : 0;
+      total += t;
+    }
+    const int incl0 = off + v - f1, incl1 = incl0 + f1;   // inclusive ranks
+    auto set_slot = [&](int ri, int incl, int f) {
+      if (ri >= nr || !S.rows[ri].mode) return;
+      const int b = S.rows[ri].bin & 0xffff;
+      const int slot = incl - 1 < RS_MAXBIN ? incl - 1 : RS_NOSLOT;
+      S.rows[ri].bin = b | (slot << 16);
+      if (f && slot < RS_MAXBIN) S.bin_id[slot] = b;
+    };
+    set_slot(r0, incl0, f0);
+    set_slot(r1, incl1, f1);
+    if (tid == 0) {
+      S.nbins = min(total, RS_MAXBIN);
+      S.ngrp = ngrp;
+    }
+  }
+  __syncthreads();
+
+  // ---- [P6b] thread 0: the staging plan (a short chain over the groups);
+  // threads 16..127: range-key runs of the columns
+  if (tid == 0) {
+    if (S.ys0 == INT32_MAX) S.ys0 = 0;
+    // the lines each group's window pushes need, copied before the group
+    // (at most RS_SR lines kept)
+    int st_lo = 1, st_hi = 0;
+    for (int g = 0; g < S.ngrp; g++) {
+      int lo = S.grange[g].x;
+      const int hi = S.grange[g].y;
       int c_lo = 1, c_hi = 0;
       if (lo <= hi) {
         lo = max(lo, hi - (RS_SR - 1));
@@ -665,12 +752,13 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
       }
       S.gplan[g] = make_int4(c_lo, c_hi, st_lo, st_hi);
     }
-    S.ngrp = ngrp;
   } else if (tid >= RS_NT - RS_TW) {
     const int c = tid - (RS_NT - RS_TW);
     if (c < cN) {
       // runs of the range key over the item rows, by bisection of the exact
-      // per-pixel key on the pieces where the position is monotone in the row
+      // per-pixel key on the pieces where the position is monotone in the
+      // row; a piece that starts with the key the previous one ended with
+      // continues its run
       auto keyat = [&](int ri) { return rg_key(S, J, r_begin + ri, c); };
       int ends[2] = {nr - 1, nr - 1};
       int np = 1;
@@ -687,7 +775,7 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
           }
         }
       }
-      int n = 0;
+      int n = 0, last_key = INT32_MIN;
       bool dense = false;
       int a = 0;
       for (int pc = 0; pc < np && !dense; pc++) {
@@ -695,32 +783,16 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
         int r = a, k = keyat(a);
         const int kb = keyat(bend);
         for (;;) {
-          if (n == RS_MAXRUN) {
-            dense = true;
-            break;
-          }
-          // the run's range weights: phase moments over the ring columns
-          const int p0 = k >> 12, bp = k & 4095;
-          const int xb = p0 - 5 - xw;
-          float4 gg = make_float4(__ldg(lut.sp1 + bp), 0.f, 0.f, 0.f);
-          if (xb >= 0 && xb + kTaps <= RS_FW) {
-            const float *kp = lut.krg + bp * kTaps;
-            float G2 = 0.f, G1 = 0.f, G0 = 0.f;
-#pragma unroll
-            for (int i = 0; i < kTaps; i++) {
-              const float w = __ldg(kp + i);
-              const float4 gc = S.ring_gc[xb + i];
-              G2 = fmaf(w, gc.x, G2);
-              G1 = fmaf(w, gc.y, G1);
-              G0 = fmaf(w, gc.z, G0);
+          if (k != last_key) {
+            if (n == RS_MAXRUN) {
+              dense = true;
+              break;
             }
-            gg.y = G2;
-            gg.z = G1;
-            gg.w = G0;
+            S.run_rk[c][n] = make_int2(r, k);
+            S.run_g[c][n] = run_terms(S, lut, xw, k);
+            n++;
+            last_key = k;
           }
-          S.run_rk[c][n] = make_int2(r, k);
-          S.run_g[c][n] = gg;
-          n++;
           if (k == kb) break;   // monotone: the rest of the piece has this key
           int lo = r, hi = bend, khi = kb;
           while (hi - lo > 1) {
@@ -755,9 +827,12 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
       const int y = S.ys0 + i;
       const double ta = (double)(y - J.s_first_line) * J.dt;
       RsSlaveRow sr;
-      sr.ta = ta;
-      sr.rho = kSplit ? reduce_2pi(quad_eval(refq, ta)) : 0.f;
-      sr.tc = (float)(ta - tm);
+      if (kSplit) {
+        sr.f.rho = reduce_2pi(quad_eval(refq, ta));
+        sr.f.tc = (float)(ta - tm);
+      } else {
+        sr.ta = ta;
+      }
       S.srow[i] = sr;
     }
   }
@@ -778,7 +853,7 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
   ColRun cr0, cr1;
   cr0.ok = cr1.ok = false;
   cr0.next = cr1.next = INT32_MAX;
-  cr0.key = cr1.key = 0;
+  cr0.key = cr1.key = INT32_MIN;   // a per-pixel-key column loads its first key
   cr0.m = cr1.m = 0;
   if (dval0 && !dense0) run_load(cr0, S, J, dc, 0);
   if (dval1 && !dense1) run_load(cr1, S, J, dc + 1, 0);
@@ -848,15 +923,25 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
         const int k = dh * RS_HR + kk;
         const int ri = rg0 + k;
         if (ri >= nr) break;
-        while (ri >= cr0.next) run_load(cr0, S, J, dc, cr0.m + 1);
-        while (ri >= cr1.next) run_load(cr1, S, J, dc + 1, cr1.m + 1);
-        const RsRow R = S.rows[ri];
         const int r = r_begin + ri;       // box row
+        if (dense0) {
+          const int key = rg_key(S, J, r, dc);
+          if (key != cr0.key) run_from_key(cr0, S, J, key, run_terms(S, lut, xw, key));
+        } else {
+          while (ri >= cr0.next) run_load(cr0, S, J, dc, cr0.m + 1);
+        }
+        if (dense1) {
+          const int key = rg_key(S, J, r, dc + 1);
+          if (key != cr1.key) run_from_key(cr1, S, J, key, run_terms(S, lut, xw, key));
+        } else {
+          while (ri >= cr1.next) run_load(cr1, S, J, dc + 1, cr1.m + 1);
+        }
+        const RsRow R = S.rows[ri];
         float2 *orow = J.out + (long)(r - J.row0) * J.out_pitch + c0 + dc;
         const float2 *vrow = &S.vd[buf][k][0];
         const bool rfast = R.mode != RM_PIXEL;
-        const bool ok0 = rfast && !dense0 && cr0.ok;
-        const bool ok1 = rfast && dval1 && !dense1 && cr1.ok;
+        const bool ok0 = rfast && cr0.ok;
+        const bool ok1 = rfast && dval1 && cr1.ok;
         const int xb0 = (cr0.key >> 12) - 5 - xw;
         if (ok0 && ok1 && (cr1.key >> 12) == (cr0.key >> 12) + 1) {
           const int base = xb0 & ~1;

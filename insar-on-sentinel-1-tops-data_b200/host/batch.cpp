@@ -178,7 +178,7 @@ int tops_batch_destroy(tops_batch *B) {
 
 int tops_batch_set_tune(tops_batch *B, const tops_tune *t) {
   if (!B || !t) return TOPS_E_INVALID;
-  if (t->rs_seg_rows < 0 || t->rs_seg_rows > 256 || (t->rs_seg_rows && t->rs_seg_rows < 16) ||
+  if (t->rs_seg_rows < 0 || t->rs_seg_rows > 252 || (t->rs_seg_rows && t->rs_seg_rows < 12) ||
       t->coh_seg_rows < 0 || t->coh_seg_rows > 512 || (t->coh_seg_rows && t->coh_seg_rows < 8))
     return TOPS_E_INVALID;
   B->tune = *t;
@@ -309,7 +309,7 @@ int tops_batch_autotune(tops_batch *B, void *stream, tops_tune *best, double *be
     ms = acc / 2.f;
     return s;
   };
-  const int rs_seg[] = {64, 128, 256};
+  const int rs_seg[] = {84, 168, 252};
   const int coh_seg[] = {64, 128, 256, 512};
   float best_rs = 1e30f, best_coh = 1e30f;
   tops_tune bt;

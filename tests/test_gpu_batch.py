@@ -70,7 +70,7 @@ def test_persistent_queue_equals_grid_launch(T, scenes):
     B = T.Batch(plans)
     B.run()
     ref = [_outputs(P) for P in plans]
-    B.tune(T.Tune(256, 1, 128, 1))
+    B.tune(T.Tune(252, 1, 128, 1))
     B.run(graph=True)
     for P, r in zip(plans, ref):
         _same(_outputs(P), r)
@@ -93,7 +93,7 @@ def test_autotune_picks_a_valid_tile(T, scenes):
     B.run()
     ref = [_outputs(P) for P in plans]
     best, ms = B.autotune()
-    assert best.rs_seg_rows in (64, 128, 256) and best.rs_persistent in (0, 1)
+    assert best.rs_seg_rows in (84, 168, 252) and best.rs_persistent in (0, 1)
     assert best.coh_seg_rows in (64, 128, 256, 512) and best.coh_persistent in (0, 1)
     assert np.all(ms > 0)
     t = B.tune()
