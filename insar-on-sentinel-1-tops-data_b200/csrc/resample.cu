@@ -92,7 +92,7 @@ static_assert(RS_DT <= RS_NT && RS_GR == 12 && RS_HR * 2 == RS_GR,
               "thread mappings assume these sizes");
 
 enum : int { REG_OUT = 0, REG_EDGE = 1, REG_IN = 2 };
-enum : int { RM_PIXEL = 0, RM_STEADY = 1, RM_REBUILD = 2 };
+enum : int { RM_PIXEL = 0, RM_SHARED = 1 };
 
 using RsLut = LutPtrs;
 
@@ -109,8 +109,8 @@ struct __align__(16) RsRow {
   float R0;
   int L0;                    // azimuth line of the shared azimuth pass
   int bin;                   // its LUT bin | bin-table slot << 16
-  int mode;                  // RM_PIXEL: per pixel; RM_STEADY: one new window line;
-                             // RM_REBUILD: the window is filled anew
+  int mode;                  // RM_SHARED: the row takes the shared azimuth pass;
+                             // RM_PIXEL: its pixels take the per-pixel path
 };
 
 // Deramp terms of one slave line: the burst-local azimuth time (FP64
@@ -123,7 +123,7 @@ union RsSlaveRow {
 };
 
 struct __align__(16) RsShared {
-  float2 vd[2][RS_GR][RS_FW];         // azimuth-interpolated rows (double-buffered)
+  float2 vd[RS_GR][RS_FW];            // azimuth-interpolated rows of the group
   short2 stage[RS_SR][RS_FW];         // raw slave lines, ring indexed by line & 31
   RsRow rows[RS_MAXSEG];
   RsSlaveRow srow[RS_NSR];            // slave lines ys0 .. ys0 + RS_NSR - 1
@@ -136,7 +136,11 @@ struct __align__(16) RsShared {
   alignas(16) double col_phat[RS_TW];
   double col_qaz[RS_TW], col_qrg[RS_TW];
   int4 gplan[RS_NGRP];                // per group: lines to stage before it, staged window
+  int4 gwin[RS_NGRP];                 // per group: window on, filled at its start, line of row 0,
+                                      // rows without a shared azimuth pass (bit mask)
   int2 grange[RS_NGRP];               // per group: lines its window pushes need
+  int gen_n[RS_NGRP];                 // per group: pixels deferred to the per-pixel pass
+  unsigned short gen[RS_GR * RS_TW];  // their (row in group) * 128 + column
   int scan[RS_NT / 32];               // per-warp totals of the bin-change scan
   double caz[6], crg[6], shift;
   double ref_a0, ref_a1, ref_a2, tm;
@@ -641,36 +645,49 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
   }
   __syncthreads();
 
-  // ---- [P5] window modes: a row continues the previous row's window when
-  // its line is the next one (slots rotate with the item row)
-  int mode_a = 0, mode_b = 0;
-  {
-    auto mode_of = [&](int ri) {
-      const RsRow &R = S.rows[ri];
-      if (!R.mode) return (int)RM_PIXEL;
-      if (ri > 0 && S.rows[ri - 1].mode && S.rows[ri - 1].L0 + 1 == R.L0) return (int)RM_STEADY;
-      return (int)RM_REBUILD;
-    };
-    if (tid < nr) mode_a = mode_of(tid);
-    if (tid + RS_NT < nr) mode_b = mode_of(tid + RS_NT);
+  // ---- [P5] thread 0: the window of the azimuth pass over the groups.
+  // The window advances one line per row; it is (re)filled at the start of
+  // a group whose first row takes a shared pass on a line the window does
+  // not expect.  A row takes the shared pass when its line is the window's.
+  if (tid == 0) {
+    const int ngrp = (nr + RS_GR - 1) / RS_GR;
+    bool on = false;
+    int base_row = 0, base_L0 = 0;
+    for (int g = 0; g < ngrp; g++) {
+      const int p = g * RS_GR;
+      const RsRow &R = S.rows[p];
+      bool fill = false;
+      if (R.mode && (!on || R.L0 != base_L0 + (p - base_row))) {
+        fill = true;
+        on = true;
+        base_row = p;
+        base_L0 = R.L0;
+      }
+      S.gwin[g] = make_int4(on ? 1 : 0, fill ? 1 : 0, on ? base_L0 + (p - base_row) : 0, 0);
+      S.gen_n[g] = 0;
+    }
+    S.ngrp = ngrp;
   }
   __syncthreads();
-  if (tid < nr) S.rows[tid].mode = mode_a;
-  if (tid + RS_NT < nr) S.rows[tid + RS_NT].mode = mode_b;
-  __syncthreads();
 
-  // ---- [P6a] azimuth-bin table (a slot per change of the bin between
-  // consecutive rows, ranked by a block-wide scan), each group's line
-  // range, the first slave line used; thread t takes rows 2t and 2t + 1
+  // ---- [P6a] row modes; azimuth-bin table (a slot per change of the bin
+  // between consecutive shared rows, ranked by a block-wide scan); each
+  // group's line range and per-pixel rows; the first slave line used.
+  // Thread t takes rows 2t and 2t + 1.
   {
     const int lane = tid & 31, warp = tid >> 5;
     const int r0 = 2 * tid, r1 = r0 + 1;
-    auto bin_change = [&](int ri) -> int {
-      if (ri >= nr || !S.rows[ri].mode) return 0;
-      if (ri == 0 || !S.rows[ri - 1].mode) return 1;
-      return (S.rows[ri - 1].bin & 0xffff) != (S.rows[ri].bin & 0xffff) ? 1 : 0;
+    auto shared_row = [&](int ri) -> bool {
+      if (ri >= nr) return false;
+      const RsRow &R = S.rows[ri];
+      const int4 gw = S.gwin[ri / RS_GR];
+      return R.mode && gw.x && R.L0 == gw.z + ri % RS_GR;
     };
-    const int f0 = bin_change(r0), f1 = bin_change(r1);
+    const bool h0 = shared_row(r0), h1 = shared_row(r1);
+    const bool p0 = r0 > 0 && shared_row(r0 - 1);
+    auto bin_of = [&](int ri) { return S.rows[ri].bin & 0xffff; };
+    const int f0 = h0 && (!p0 || bin_of(r0 - 1) != bin_of(r0)) ? 1 : 0;
+    const int f1 = h1 && (!h0 || bin_of(r0) != bin_of(r1)) ? 1 : 0;
     int v = f0 + f1;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -679,27 +696,21 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
     }
     if (lane == 31) S.scan[warp] = v;
     int ymin = INT32_MAX;
-    if (r0 < nr && S.rows[r0].mode) ymin = S.rows[r0].L0 - 5;
-    if (r1 < nr && S.rows[r1].mode) ymin = min(ymin, S.rows[r1].L0 - 5);
+    const int ngrp = S.ngrp;
+    if (tid < ngrp) {
+      const int4 gw = S.gwin[tid];
+      const int gr = min(RS_GR, nr - tid * RS_GR);
+      if (gw.x) ymin = gw.z - (gw.y ? 5 : -6);
+      int mask = 0;
+      for (int k = 0; k < gr; k++)
+        if (!shared_row(tid * RS_GR + k)) mask |= 1 << k;
+      S.grange[tid] = gw.x ? make_int2(gw.y ? gw.z - 5 : gw.z + 6, gw.z + gr - 1 + 6)
+                           : make_int2(1, 0);
+      S.gwin[tid].w = mask;
+    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) ymin = min(ymin, __shfl_xor_sync(0xffffffffu, ymin, o));
     if (lane == 0 && ymin != INT32_MAX) atomicMin(&S.ys0, ymin);
-    // lines the pushes of group g need (thread g)
-    const int ngrp = (nr + RS_GR - 1) / RS_GR;
-    if (tid < ngrp) {
-      int lo = INT32_MAX, hi = INT32_MIN;
-      for (int k = 0; k < RS_GR && tid * RS_GR + k < nr; k++) {
-        const RsRow &R = S.rows[tid * RS_GR + k];
-        if (R.mode == RM_STEADY) {
-          lo = min(lo, R.L0 + 6);
-          hi = max(hi, R.L0 + 6);
-        } else if (R.mode == RM_REBUILD) {
-          lo = min(lo, R.L0 - 5);
-          hi = max(hi, R.L0 + 6);
-        }
-      }
-      S.grange[tid] = make_int2(lo, hi);
-    }
     __syncthreads();
     int off = 0, total = 0;
 #pragma unroll
@@ -709,19 +720,22 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
       total += t;
     }
     const int incl0 = off + v - f1, incl1 = incl0 + f1;   // inclusive ranks
-    auto set_slot = [&](int ri, int incl, int f) {
-      if (ri >= nr || !S.rows[ri].mode) return;
-      const int b = S.rows[ri].bin & 0xffff;
+    auto set_row = [&](int ri, bool h, int incl, int f) {
+      if (ri >= nr) return;
+      RsRow &R = S.rows[ri];
+      if (!h) {
+        R.mode = RM_PIXEL;
+        return;
+      }
+      const int b = R.bin & 0xffff;
       const int slot = incl - 1 < RS_MAXBIN ? incl - 1 : RS_NOSLOT;
-      S.rows[ri].bin = b | (slot << 16);
+      R.bin = b | (slot << 16);
+      R.mode = RM_SHARED;
       if (f && slot < RS_MAXBIN) S.bin_id[slot] = b;
     };
-    set_slot(r0, incl0, f0);
-    set_slot(r1, incl1, f1);
-    if (tid == 0) {
-      S.nbins = min(total, RS_MAXBIN);
-      S.ngrp = ngrp;
-    }
+    set_row(r0, h0, incl0, f0);
+    set_row(r1, h1, incl1, f1);
+    if (tid == 0) S.nbins = min(total, RS_MAXBIN);
   }
   __syncthreads();
 
@@ -853,14 +867,14 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
   ColRun cr0, cr1;
   cr0.ok = cr1.ok = false;
   cr0.next = cr1.next = INT32_MAX;
-  cr0.key = cr1.key = INT32_MIN;   // a per-pixel-key column loads its first key
+  cr0.key = cr1.key = 0;
   cr0.m = cr1.m = 0;
   if (dval0 && !dense0) run_load(cr0, S, J, dc, 0);
   if (dval1 && !dense1) run_load(cr1, S, J, dc + 1, 0);
   const bool out16 = J.out_al16 != 0;
 
-  // azimuth-pass state: the 12-line window of this ring column (slot of
-  // line L0 - 5 + j at row k of a group: (k + j) % 12) and the current taps
+  // azimuth-pass state: the 12-line window of this ring column (line
+  // wl0 + k - 5 + j of group row k in slot (k + j) % 12) and the taps
   float2 w[RS_GR];
 #pragma unroll
   for (int j = 0; j < RS_GR; j++) w[j] = make_float2(0.f, 0.f);
@@ -872,40 +886,43 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
   const int ngrp = S.ngrp;
   for (int g = 0; g < ngrp; g++) {
     const int rg0 = g * RS_GR;            // first item row of the group
-    const int buf = g & 1;
+    const int gr = min(RS_GR, nr - rg0);
     const int4 plan = S.gplan[g];
+    const int4 gw = S.gwin[g];
+    const int pixmask = gw.w;
     cp_async_wait_all();                  // this thread's staged lines of the group
-    // ---- [A] azimuth pass of the group's rows
+    // ---- [A] azimuth pass of the group's rows (the taps are loaded anew per
+    // group, so they hold no registers during [B] and [C])
+    wz_bin = -1;
+    if (gw.x) {
+      const int wl0 = gw.z;
+      if (gw.y) {
+        // fill the window of row 0 (slots 0..10; row 0 pushes slot 11)
 #pragma unroll
-    for (int k = 0; k < RS_GR; k++) {
-      const int ri = rg0 + k;
-      if (ri < nr) {
-        const RsRow &R = S.rows[ri];
-        const int mode = R.mode;
-        if (mode != RM_PIXEL) {
-          const int L0 = R.L0;
-          if (mode == RM_STEADY) {
-            w[(k + 11) % RS_GR] = deramp_at<kSplit>(S, J, x, xa, xin, L0 + 6, plan.z, plan.w,
-                                                    g2c, g1c, g0c, cq);
-          } else {
+        for (int j = 0; j < RS_GR - 1; j++)
+          w[j] = deramp_at<kSplit>(S, J, x, xa, xin, wl0 - 5 + j, plan.z, plan.w, g2c, g1c,
+                                   g0c, cq);
+      }
 #pragma unroll
-            for (int j = 0; j < RS_GR; j++)
-              w[(k + j) % RS_GR] = deramp_at<kSplit>(S, J, x, xa, xin, L0 - 5 + j, plan.z,
-                                                     plan.w, g2c, g1c, g0c, cq);
-          }
-          const int bin = R.bin;
-          if (bin != wz_bin) {
-            load_az_taps(S, lut, bin, wz);
-            wz_bin = bin;
-          }
-          float2 a = make_float2(0.f, 0.f), b = a;
+      for (int k = 0; k < RS_GR; k++) {
+        if (k < gr) {
+          w[(k + 11) % RS_GR] = deramp_at<kSplit>(S, J, x, xa, xin, wl0 + k + 6, plan.z, plan.w,
+                                                  g2c, g1c, g0c, cq);
+          if (!((pixmask >> k) & 1)) {
+            const int bin = S.rows[rg0 + k].bin;
+            if (bin != wz_bin) {
+              load_az_taps(S, lut, bin, wz);
+              wz_bin = bin;
+            }
+            float2 a = make_float2(0.f, 0.f), b = a;
 #pragma unroll
-          for (int j = 0; j < RS_GR; j += 2) {
-            const float4 q = wz[j >> 1];
-            a = __ffma2_rn(make_float2(q.x, q.y), w[(k + j) % RS_GR], a);
-            b = __ffma2_rn(make_float2(q.z, q.w), w[(k + j + 1) % RS_GR], b);
+            for (int j = 0; j < RS_GR; j += 2) {
+              const float4 q = wz[j >> 1];
+              a = __ffma2_rn(make_float2(q.x, q.y), w[(k + j) % RS_GR], a);
+              b = __ffma2_rn(make_float2(q.z, q.w), w[(k + j + 1) % RS_GR], b);
+            }
+            S.vd[k][x] = __fadd2_rn(a, b);
           }
-          S.vd[buf][k][x] = __fadd2_rn(a, b);
         }
       }
     }
@@ -916,34 +933,23 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
     }
     __syncthreads();
 
-    // ---- [B] range pass, reramp, store: 2 columns x 6 rows per thread
+    // ---- [B] range pass, reramp, store: 2 columns x 6 rows per thread;
+    // pixels the shared passes do not cover are listed for [C]
     if (dval0) {
 #pragma unroll 1
       for (int kk = 0; kk < RS_HR; kk++) {
         const int k = dh * RS_HR + kk;
+        if (k >= gr) break;
+        if ((pixmask >> k) & 1) continue;   // the whole row is done in [C]
         const int ri = rg0 + k;
-        if (ri >= nr) break;
+        while (ri >= cr0.next) run_load(cr0, S, J, dc, cr0.m + 1);
+        while (ri >= cr1.next) run_load(cr1, S, J, dc + 1, cr1.m + 1);
         const int r = r_begin + ri;       // box row
-        if (dense0) {
-          const int key = rg_key(S, J, r, dc);
-          if (key != cr0.key) run_from_key(cr0, S, J, key, run_terms(S, lut, xw, key));
-        } else {
-          while (ri >= cr0.next) run_load(cr0, S, J, dc, cr0.m + 1);
-        }
-        if (dense1) {
-          const int key = rg_key(S, J, r, dc + 1);
-          if (key != cr1.key) run_from_key(cr1, S, J, key, run_terms(S, lut, xw, key));
-        } else {
-          while (ri >= cr1.next) run_load(cr1, S, J, dc + 1, cr1.m + 1);
-        }
-        const RsRow R = S.rows[ri];
         float2 *orow = J.out + (long)(r - J.row0) * J.out_pitch + c0 + dc;
-        const float2 *vrow = &S.vd[buf][k][0];
-        const bool rfast = R.mode != RM_PIXEL;
-        const bool ok0 = rfast && cr0.ok;
-        const bool ok1 = rfast && dval1 && cr1.ok;
+        const float2 *vrow = &S.vd[k][0];
         const int xb0 = (cr0.key >> 12) - 5 - xw;
-        if (ok0 && ok1 && (cr1.key >> 12) == (cr0.key >> 12) + 1) {
+        if (cr0.ok && cr1.ok && dval1 && (cr1.key >> 12) == (cr0.key >> 12) + 1) {
+          const RsRow R = S.rows[ri];
           const int base = xb0 & ~1;
           const bool odd = (xb0 & 1) != 0;
           float2 V[14];
@@ -965,15 +971,54 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
             orow[1] = o1;
           }
         } else {
-          // per column: single fast range pass, else the per-pixel path
-          orow[0] = ok0 ? cmul_conj_phase(range_single(vrow, xb0, cr0), run_phase(R, cr0))
-                        : pixel_generic(S, J, r, dc);
-          if (dval1) {
-            const int xb1 = (cr1.key >> 12) - 5 - xw;
-            orow[1] = ok1 ? cmul_conj_phase(range_single(vrow, xb1, cr1), run_phase(R, cr1))
-                          : pixel_generic(S, J, r, dc + 1);
+          // per column, from the run key: outside the slave box 0, at its
+          // edge the nearest sample, inside the window the tile's range
+          // pass, else [C]
+          const RsRow R = S.rows[ri];
+#pragma unroll
+          for (int cc = 0; cc < 2; cc++) {
+            if (cc == 1 && !dval1) break;
+            const ColRun &cr = cc ? cr1 : cr0;
+            const bool dense = cc ? dense1 : dense0;
+            const int p0 = cr.key >> 12;
+            if (dense || (p0 >= J.sx0 + 5 && p0 <= J.sx1 - 7 && !cr.ok)) {
+              const int e = atomicAdd(&S.gen_n[g], 1);
+              S.gen[e] = (unsigned short)(k * 128 + dc + cc);
+            } else if (cr.ok) {
+              orow[cc] = cmul_conj_phase(range_single(vrow, p0 - 5 - xw, cr), run_phase(R, cr));
+            } else if (p0 < J.sx0 || p0 > J.sx1) {
+              orow[cc] = make_float2(0.f, 0.f);
+            } else {
+              const short2 sv = J.slave[(long)(R.L0 - J.sy0) * J.slave_pitch + (p0 - J.sx0)];
+              orow[cc] = make_float2((float)sv.x, (float)sv.y);
+            }
           }
         }
+      }
+    }
+    __syncthreads();
+
+    // ---- [C] per-pixel path, all threads: the rows without a shared pass,
+    // then the listed pixels
+    {
+      const int npr = __popc(pixmask);
+      const int nrow_units = npr * cN;
+      const int total = nrow_units + S.gen_n[g];
+      for (int u = tid; u < total; u += RS_NT) {
+        int k, c;
+        if (u < nrow_units) {
+          int nth = u / cN;
+          c = u - nth * cN;
+          int m = pixmask;
+          while (nth-- > 0) m &= m - 1;   // drop the lower set bits
+          k = __ffs(m) - 1;
+        } else {
+          const int code = S.gen[u - nrow_units];
+          k = code >> 7;
+          c = code & 127;
+        }
+        const int r = r_begin + rg0 + k;
+        J.out[(long)(r - J.row0) * J.out_pitch + c0 + c] = pixel_generic(S, J, r, c);
       }
     }
   }
