@@ -40,6 +40,10 @@ typedef struct {
                                the reference passes them (Func.cpp:2383) */
   int precision;            /* resample deramp phase: TOPS_PREC_SPLIT (default)
                                or TOPS_PREC_FP64 */
+  int compensated;          /* 1: ESD phasor sums with Kahan compensation and
+                               coherence window sums without the sliding
+                               update (pairwise per output); 0 (default): the
+                               plain fixed-order FP32 sums */
 } tops_pair_opts;
 
 int tops_pair_opts_default(tops_pair_opts *o);

@@ -29,7 +29,7 @@ int launch_coherence(const CohJob *jobs, int njobs, int win_rg, int win_az, cons
                      cudaStream_t st);
 int launch_esd(const EsdOverlap *ovs, int n_ov, int win_az, int win_rg, float thr,
                double *shifts, double *sums, void *scratch, size_t scratch_bytes,
-               cudaStream_t st);
+               cudaStream_t st, int compensated);
 size_t esd_scratch_bytes(const EsdOverlap *ov, int n);
 int launch_geocoreg(const GeoJob *jobs, int njobs, bool dem_is_int, void *scratch,
                     size_t scratch_bytes, cudaStream_t st);
@@ -459,7 +459,7 @@ int EstESDShifts(void *MasterFor, void *MasterBack, void *SlaveFor, void *SlaveB
   TOPS_TRY(ws->get(11, scr, &d_scr));
   double *d_shift = static_cast<double *>(d_o);
   TOPS_TRY(launch_esd(O.data(), numOverlap, CohWinAz, CohWinRg, CohThresHold, d_shift, nullptr,
-                      d_scr, scr, st));
+                      d_scr, scr, st, 0));
   TOPS_CUDA_TRY(cudaMemcpyAsync(ShiftArray, d_shift, sizeof(double) * numOverlap,
                                 cudaMemcpyDeviceToHost, st));
   TOPS_CUDA_TRY(cudaStreamSynchronize(st));

@@ -20,8 +20,11 @@
 // 16-byte stores.  Other window heights (WAZ = 0) reload the halo rows of
 // each group.  HBM traffic is the algorithmic 4 + 8 + 4 bytes per pixel plus
 // the column halo.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -39,6 +42,7 @@ constexpr int CO_MAX_WIN_RG = CO_NT - CO_TW + 1;
 
 struct CoBatch {
   int njobs, total_items, win_rg, win_az;
+  int compensated;         // 1: each output's window summed pairwise
   int *counter;            // persistent launch: work-item queue (else null)
   CohJob jobs[CO_MAXJOBS];
 };
@@ -62,6 +66,22 @@ __device__ __forceinline__ void add4(float4 &a, const float4 &b) {
   a = make_float4(c.x, c.y, p.x, p.y);
 }
 
+// Pairwise sum of n window columns V[idx(0)] .. V[idx(n - 1)] (the
+// compensated mode: no sliding update, rounding error O(log n)).
+template <class Idx>
+__device__ __forceinline__ float4 window_pairwise(const float4 *V, int n, Idx idx) {
+  float4 p[16];
+  int m = 0;
+  for (int i = 0; i + 1 < n; i += 2, m++) {
+    p[m] = V[idx(i)];
+    add4(p[m], V[idx(i + 1)]);
+  }
+  if (n & 1) p[m++] = V[idx(n - 1)];
+  for (int h = 1; h < m; h <<= 1)
+    for (int i = 0; i + h < m; i += 2 * h) add4(p[i], p[i + h]);
+  return p[0];
+}
+
 // Horizontal pass of one group: CO_CPI consecutive outputs per item.  The
 // amplitude mask |s| < 0.001 of the reference (EstCoh.cu:393, 446) is
 // evaluated as |s|^2 < 1e-6.  WRG > 0: range window known at compile time;
@@ -70,7 +90,7 @@ __device__ __forceinline__ void add4(float4 &a, const float4 &b) {
 template <int WRG>
 __device__ __forceinline__ void coh_horizontal(const CoShared &S, const CohJob &J, int tid,
                                                int rg, int gr, int c0, int cN, int win_rg_rt,
-                                               int dx_rt) {
+                                               int dx_rt, bool comp) {
   constexpr int NG = CO_TW / CO_CPI;
   static_assert(CO_CPI % 8 == 0, "items must start at multiples of 8 columns");
   const int win_rg = WRG > 0 ? WRG : win_rg_rt;
@@ -91,7 +111,9 @@ __device__ __forceinline__ void coh_horizontal(const CoShared &S, const CohJob &
     float out[CO_CPI];
 #pragma unroll
     for (int u = 0; u < CO_CPI; u++) {
-      if (u > 0) {
+      if (comp) {
+        w = window_pairwise(V, win_rg, [&](int i) { return pad8(u + i); });
+      } else if (u > 0) {
         const float4 a = V[pad8(u - 1 + win_rg)];
         const float4 b = V[pad8(u - 1)];
         const float2 m1 = make_float2(-1.f, -1.f);
@@ -196,7 +218,7 @@ __device__ __forceinline__ void coherence_item(CoShared &S, const CoBatch &B, in
 #pragma unroll
       for (int j = 0; j < NQ; j++) q[j] = p[CO_GR + j];
       __syncthreads();
-      coh_horizontal<WRG>(S, J, tid, rg, gr, c0, cN, win_rg, dx);
+      coh_horizontal<WRG>(S, J, tid, rg, gr, c0, cN, win_rg, dx, B.compensated != 0);
       __syncthreads();
     }
   } else {
@@ -229,7 +251,7 @@ __device__ __forceinline__ void coherence_item(CoShared &S, const CoBatch &B, in
         S.spow[k][pad8(tid)] = spow[k];
       }
       __syncthreads();
-      coh_horizontal<WRG>(S, J, tid, rg, gr, c0, cN, win_rg, dx);
+      coh_horizontal<WRG>(S, J, tid, rg, gr, c0, cN, win_rg, dx, B.compensated != 0);
       __syncthreads();
     }
   }
@@ -255,6 +277,354 @@ __global__ void __launch_bounds__(CO_NT, 3) coherence_kernel(const __grid_consta
     item = S.next_item;
     __syncthreads();
   }
+}
+
+// ------------------------------------------------ TMA-staged variant
+// For the pipeline's 10-sample range window.  A CTA of CT_NT threads owns a
+// strip of CT_TW output columns and a segment of rows; its input rows come
+// in chunks of CT_CH rows x CT_LW columns (master as 32-bit, slave as 64-bit
+// elements), each chunk one cp.async.bulk.tensor box per image on an
+// mbarrier, CT_NST - 1 chunks ahead of the one being summed.  The box
+// starts CT_XOFF = dx columns left of the strip, a multiple of 4, so every
+// box's x coordinate is 16-byte aligned in both images; the copy engine
+// fills rows and columns outside the image with zeros -- the zero pad.  The
+// sums are those of coherence_item, in the same order, so the two kernels
+// agree bit for bit.
+constexpr int CT_NT = 256;
+constexpr int CT_LW = 256;                 // loaded columns (box width)
+constexpr int CT_CH = 4;                   // rows per chunk (box height)
+constexpr int CT_NST = 4;                  // chunk slots
+constexpr int CT_WRG = 10;                 // range window of this variant
+constexpr int CT_DX = (CT_WRG - 1) / 2;    // 4
+constexpr int CT_XOFF = CT_DX;             // box start left of the strip
+constexpr int CT_TW = 240;                 // output columns per strip
+constexpr int CT_CPI = 4;                  // outputs per horizontal item
+constexpr int CT_SEG = 256;                // rows per work item
+constexpr int CT_MAXJOBS = 16;
+constexpr long CT_WAIT_LIMIT = 1L << 26;   // mbarrier polls before a chunk is given up
+static_assert(CT_XOFF % 4 == 0 && CT_XOFF == CT_DX, "box x coordinates stay 16-byte aligned");
+static_assert(CT_XOFF + CT_TW + CT_WRG - 1 - CT_DX <= CT_LW, "the strip's boxes cover its windows");
+static_assert(CT_TW % CT_CPI == 0 && CT_CH * (CT_TW / CT_CPI) <= CT_NT, "one horizontal item per thread");
+
+__host__ __device__ constexpr int pad4(int x) { return x + (x >> 2); }
+
+struct __align__(64) CtBatch {
+  CUtensorMap tm_m[CT_MAXJOBS];   // master: int32 [lines][pixels], box CT_LW x CT_CH
+  CUtensorMap tm_s[CT_MAXJOBS];   // slave: 64-bit [lines][pixels], same box
+  CohJob jobs[CT_MAXJOBS];
+  int njobs, total_items;
+  int compensated;                // 1: each output's window summed pairwise
+  int *counter;                   // persistent launch: work-item queue (else null)
+};
+
+struct __align__(128) CtShared {
+  int m[CT_NST][CT_CH][CT_LW];          // master chunks (CInt16 pairs)
+  float2 s[CT_NST][CT_CH][CT_LW];       // slave chunks
+  float4 V[CT_CH][pad4(CT_LW)];         // vertical sums (re, im, |s|^2, |m|^2)
+  float spow[CT_CH][pad4(CT_LW)];       // |s|^2 of the centre pixel
+  unsigned long long full[CT_NST];      // one mbarrier per slot
+  int next_item;
+};
+
+__device__ int g_coh_wait_faults;       // chunks whose wait ran out (0 normally)
+
+__device__ __forceinline__ unsigned ct_smem(const void *p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void ct_mbar_init(unsigned long long *bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(ct_smem(bar)) : "memory");
+}
+__device__ __forceinline__ void ct_expect_tx(unsigned long long *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(ct_smem(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool ct_try_wait(unsigned long long *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(ct_smem(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void ct_tma_2d(void *dst, const CUtensorMap *tm, int x, int y,
+                                          unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(ct_smem(dst)),
+      "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(ct_smem(bar))
+      : "memory");
+}
+// Waits for the slot's chunk with a bounded number of polls; false if it
+// never arrived (recorded in g_coh_wait_faults).
+__device__ __forceinline__ bool ct_wait(unsigned long long *bar, unsigned parity) {
+  for (long it = 0; it < CT_WAIT_LIMIT; it++)
+    if (ct_try_wait(bar, parity)) return true;
+  return false;
+}
+
+// One work item; returns false (all threads) when a chunk never arrived.
+// `seq` counts the chunks this CTA has consumed (slot and mbarrier phase).
+template <int WAZ>
+__device__ __forceinline__ bool coh_tma_item(CtShared &S, const CtBatch &B, int item,
+                                             unsigned &seq) {
+  constexpr int DY = (WAZ - 1) / 2;
+  constexpr int NQ = WAZ - 1;
+  constexpr int H = (NQ + CT_CH - 1) / CT_CH;   // chunks holding the first halo rows
+  constexpr unsigned kChunkBytes = CT_CH * CT_LW * (4 + 8);
+  const int tid = threadIdx.x;
+  int jb = 0;
+  while (jb + 1 < B.njobs && B.jobs[jb + 1].item_begin <= item) jb++;
+  const CohJob &J = B.jobs[jb];
+  const int local = item - J.item_begin;
+  const int strip = local % J.strips, seg = local / J.strips;
+  const int c0 = strip * CT_TW;
+  const int cN = min(CT_TW, J.pixels - c0);
+  const int r_begin = seg * J.seg_rows;
+  const int r_end = min(r_begin + J.seg_rows, J.lines);
+  const int nout = (r_end - r_begin + CT_CH - 1) / CT_CH;
+  const int T = H + nout;
+  const int x0 = c0 - CT_XOFF;
+  // chunk u holds input rows base(u) .. base(u) + CT_CH - 1: output chunk
+  // u - H's new rows, the halo rows r_begin - DY .. r_begin - DY + NQ - 1
+  // at the end of the first H chunks
+  auto base = [&](int u) { return r_begin + CT_CH * (u - H) + (NQ - DY); };
+  auto issue = [&](int u) {
+    const unsigned slot = (seq + u) % CT_NST;
+    ct_expect_tx(&S.full[slot], kChunkBytes);
+    ct_tma_2d(&S.m[slot][0][0], &B.tm_m[jb], x0, base(u), &S.full[slot]);
+    ct_tma_2d(&S.s[slot][0][0], &B.tm_s[jb], x0, base(u), &S.full[slot]);
+  };
+  if (tid == 0)
+    for (int u = 0; u < CT_NST - 1 && u < T; u++) issue(u);
+
+  float4 q[NQ > 0 ? NQ : 1];
+#pragma unroll
+  for (int j = 0; j < NQ; j++) q[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+  const int t = tid;                       // loaded column
+  bool ok = true;
+  for (int u = 0; u < T; u++) {
+    const unsigned slot = (seq + u) % CT_NST;
+    const unsigned parity = ((seq + u) / CT_NST) & 1u;
+    const bool got = ct_wait(&S.full[slot], parity);
+    if (__syncthreads_or(!got)) {
+      ok = false;
+      if (tid == 0) {
+        atomicAdd(&g_coh_wait_faults, 1);
+        // let the copies in flight land (bounded) before the CTA moves on
+        for (int v = u; v < T && v < u + CT_NST - 1; v++)
+          (void)ct_wait(&S.full[(seq + v) % CT_NST], ((seq + v) / CT_NST) & 1u);
+      }
+      __syncthreads();
+      break;
+    }
+    // the next chunk into the slot freed by the previous one
+    if (tid == 0 && u + CT_NST - 1 < T) issue(u + CT_NST - 1);
+    if (u < H) {
+      // halo rows: products of input rows r_begin - DY + i
+#pragma unroll
+      for (int hu = 0; hu < H; hu++) {
+        if (u == hu) {
+#pragma unroll
+          for (int k = 0; k < CT_CH; k++) {
+            const int i = CT_CH * (hu - H) + NQ + k;
+            if (i >= 0 && i < NQ) {
+              const int mv = S.m[slot][k][t];
+              q[i] = coh_product(*reinterpret_cast<const short2 *>(&mv), S.s[slot][k][t]);
+            }
+          }
+        }
+      }
+      continue;
+    }
+    // vertical sums of the chunk's output rows (as coherence_item sums them)
+#pragma unroll
+    for (int k = 0; k < CT_CH; k++) {
+      const int mv = S.m[slot][k][t];
+      const float4 p = coh_product(*reinterpret_cast<const short2 *>(&mv), S.s[slot][k][t]);
+      float4 a = NQ > 0 ? q[0] : p;
+#pragma unroll
+      for (int j = 1; j < NQ; j++) add4(a, q[j]);
+      if (NQ > 0) add4(a, p);
+      S.V[k][pad4(t)] = a;
+      S.spow[k][pad4(t)] = (DY < NQ) ? q[DY < NQ ? DY : 0].z : p.z;
+#pragma unroll
+      for (int j = 0; j + 1 < NQ; j++) q[j] = q[j + 1];
+      if (NQ > 0) q[NQ - 1] = p;
+    }
+    __syncthreads();
+    // horizontal box: CT_CPI consecutive outputs per item; an item starts at
+    // a multiple of 4 columns, so every padded offset below is a constant
+    {
+      constexpr int NG = CT_TW / CT_CPI;
+      const int k = tid / NG;
+      const int cg = (tid - k * NG) * CT_CPI;
+      const int o = r_begin + CT_CH * (u - H) + k;   // output row
+      if (k < CT_CH && o < r_end && cg < cN) {
+        const float4 *V = &S.V[k][pad4(cg)];
+        const float *Jd = &S.spow[k][pad4(cg)];
+        float4 w = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int i = 0; i < CT_WRG; i++) add4(w, V[pad4(i)]);
+        float out[CT_CPI];
+        const bool comp = B.compensated != 0;
+#pragma unroll
+        for (int uu = 0; uu < CT_CPI; uu++) {
+          if (comp) {
+            w = window_pairwise(V, CT_WRG, [&](int i) { return pad4(uu + i); });
+          } else if (uu > 0) {
+            const float4 a = V[pad4(uu - 1 + CT_WRG)];
+            const float4 b = V[pad4(uu - 1)];
+            const float2 m1 = make_float2(-1.f, -1.f);
+            const float2 wc = __fadd2_rn(make_float2(w.x, w.y),
+                                         __ffma2_rn(make_float2(b.x, b.y), m1, make_float2(a.x, a.y)));
+            const float2 wp = __fadd2_rn(make_float2(w.z, w.w),
+                                         __ffma2_rn(make_float2(b.z, b.w), m1, make_float2(a.z, a.w)));
+            w = make_float4(wc.x, wc.y, wp.x, wp.y);
+          }
+          const float pp = w.z * w.w;
+          const float num = fmaf(w.x, w.x, w.y * w.y);
+          float g = (pp > 0.f && num > 0.f) ? num * rsqrtf(num) * rsqrtf(pp) : 0.f;
+          if (Jd[pad4(uu + CT_XOFF)] < 1e-6f) g = 0.f;
+          out[uu] = g;
+        }
+        float *orow = J.coh + (long)o * J.coh_pitch + c0 + cg;
+        if (cg + CT_CPI <= cN && ((reinterpret_cast<uintptr_t>(orow) & 15) == 0)) {
+          *reinterpret_cast<float4 *>(orow) = make_float4(out[0], out[1], out[2], out[3]);
+        } else {
+#pragma unroll
+          for (int uu = 0; uu < CT_CPI; uu++)
+            if (cg + uu < cN) orow[uu] = out[uu];
+        }
+      }
+    }
+    __syncthreads();
+  }
+  seq += T;
+  return ok;
+}
+
+template <int WAZ>
+__global__ void __launch_bounds__(CT_NT, 3) coh_tma_kernel(const __grid_constant__ CtBatch B) {
+  extern __shared__ __align__(128) unsigned char ct_smem_raw[];
+  CtShared &S = *reinterpret_cast<CtShared *>(ct_smem_raw);
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < CT_NST; k++) ct_mbar_init(&S.full[k]);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  unsigned seq = 0;
+  int item = blockIdx.x;
+  if (B.counter) {
+    if (threadIdx.x == 0) S.next_item = atomicAdd(B.counter, 1);
+    __syncthreads();
+    item = S.next_item;
+    __syncthreads();
+  }
+  while (item < B.total_items) {
+    if (!coh_tma_item<WAZ>(S, B, item, seq)) break;
+    if (!B.counter) break;
+    if (threadIdx.x == 0) S.next_item = atomicAdd(B.counter, 1);
+    __syncthreads();
+    item = S.next_item;
+    __syncthreads();
+  }
+}
+
+// cuTensorMapEncodeTiled from the driver (no link-time dependency on it).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static std::once_flag once;
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    (void)cudaGetLastError();
+  });
+  return fn;
+}
+
+// The TMA variant takes a job when both images start on a 16-byte boundary
+// and their row pitches are multiples of 16 bytes (a tensor map's rules).
+static bool tma_eligible(const CohJob &J) {
+  const uintptr_t m = reinterpret_cast<uintptr_t>(J.master);
+  const uintptr_t s = reinterpret_cast<uintptr_t>(J.slave);
+  return (m % 16 == 0) && (s % 16 == 0) && ((J.master_pitch * 4) % 16 == 0) &&
+         ((J.slave_pitch * 8) % 16 == 0) && J.pixels >= 1 && J.lines >= 1;
+}
+
+static int encode_maps(const CohJob &J, CUtensorMap *tm_m, CUtensorMap *tm_s) {
+  auto fn = tensor_map_encoder();
+  if (!fn) return TOPS_E_CUDA;
+  const cuuint64_t dims[2] = {(cuuint64_t)J.pixels, (cuuint64_t)J.lines};
+  const cuuint32_t box[2] = {(cuuint32_t)CT_LW, (cuuint32_t)CT_CH};
+  const cuuint32_t estr[2] = {1, 1};
+  const cuuint64_t sm[1] = {(cuuint64_t)J.master_pitch * 4};
+  const cuuint64_t ss[1] = {(cuuint64_t)J.slave_pitch * 8};
+  CUresult r = fn(tm_m, CU_TENSOR_MAP_DATA_TYPE_INT32, 2, const_cast<short2 *>(J.master), dims,
+                  sm, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return TOPS_E_INVALID;
+  r = fn(tm_s, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<float2 *>(J.slave), dims, ss, box,
+         estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? TOPS_OK : TOPS_E_INVALID;
+}
+
+template <int WAZ>
+static int launch_coh_tma(const CohJob *jobs, int njobs, const TileCfg &cfg, int dev,
+                          cudaStream_t st) {
+  static PerDeviceOnce setup;
+  int resident = 0;
+  const int s0 = once_per_device(
+      setup, dev,
+      [&](int &v) -> int {
+        TOPS_CUDA_TRY(cudaFuncSetAttribute(coh_tma_kernel<WAZ>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)sizeof(CtShared)));
+        int per_sm = 0, sms = 0;
+        TOPS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, coh_tma_kernel<WAZ>, CT_NT, sizeof(CtShared)));
+        TOPS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        v = per_sm * sms;
+        return TOPS_OK;
+      },
+      &resident);
+  if (s0 != TOPS_OK) return s0;
+  for (int j0 = 0, k = 0; j0 < njobs; j0 += CT_MAXJOBS, k++) {
+    CtBatch B;
+    B.njobs = 0;
+    B.compensated = cfg.compensated;
+    B.counter = cfg.counters ? cfg.counters + k : nullptr;
+    int items = 0;
+    for (int j = j0; j < njobs && j < j0 + CT_MAXJOBS; j++) {
+      CohJob &J = B.jobs[B.njobs];
+      J = jobs[j];
+      J.seg_rows = cfg.seg_rows ? cfg.seg_rows : CT_SEG;
+      J.segs = (J.lines + J.seg_rows - 1) / J.seg_rows;
+      J.strips = (J.pixels + CT_TW - 1) / CT_TW;
+      J.item_begin = items;
+      items += J.strips * J.segs;
+      const int s = encode_maps(J, &B.tm_m[B.njobs], &B.tm_s[B.njobs]);
+      if (s != TOPS_OK) return s;
+      B.njobs++;
+    }
+    B.total_items = items;
+    if (!items) continue;
+    int grid = items;
+    if (B.counter) {
+      TOPS_CUDA_TRY(cudaMemsetAsync(B.counter, 0, sizeof(int), st));
+      grid = min(items, cfg.grid > 0 ? cfg.grid : resident);
+    }
+    coh_tma_kernel<WAZ><<<grid, CT_NT, sizeof(CtShared), st>>>(B);
+    TOPS_CUDA_TRY(cudaGetLastError());
+  }
+  return TOPS_OK;
 }
 
 template <int WAZ, int WRG>
@@ -308,9 +678,18 @@ int launch_coherence(const CohJob *jobs, int njobs, int win_rg, int win_az, cons
   int dev = 0;
   TOPS_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDevices) return TOPS_E_INVALID;
+  // the TMA-staged kernel for the pipeline's 10-sample range window
+  if (win_rg == CT_WRG && (win_az == 3 || win_az == 6) && tensor_map_encoder()) {
+    bool all = true;
+    for (int j = 0; j < njobs; j++) all = all && tma_eligible(jobs[j]);
+    if (all)
+      return win_az == 3 ? launch_coh_tma<3>(jobs, njobs, cfg, dev, st)
+                         : launch_coh_tma<6>(jobs, njobs, cfg, dev, st);
+  }
   for (int j0 = 0, k = 0; j0 < njobs; j0 += CO_MAXJOBS, k++) {
     CoBatch B;
     B.njobs = 0;
+    B.compensated = cfg.compensated;
     B.win_rg = win_rg;
     B.win_az = win_az;
     B.counter = cfg.counters ? cfg.counters + k : nullptr;

@@ -40,6 +40,7 @@ constexpr int ES_MAXOV = 32;
 struct EsBatch {
   int n_ov, total_items, win_rg, win_az;
   float thr;
+  int compensated;   // 1: per-thread phasor sums with Kahan compensation
   EsdOverlap ov[ES_MAXOV];
 };
 
@@ -91,6 +92,22 @@ __global__ void __launch_bounds__(ES_NT, 2) esd_kernel(const __grid_constant__ E
   const int x = c0 - dw + tid;
   const bool xin = tid < nload && x >= 0 && x < O.pixels;
   float accr = 0.f, acci = 0.f;
+  float cr = 0.f, ci = 0.f;   // Kahan compensation terms (compensated mode)
+  const bool comp = B.compensated != 0;
+  // adds one unit phasor to the thread's sums
+  auto accumulate = [&](float re, float im) {
+    if (comp) {
+      const float yr = re - cr, yi = im - ci;
+      const float tr = accr + yr, ti = acci + yi;
+      cr = (tr - accr) - yr;
+      ci = (ti - acci) - yi;
+      accr = tr;
+      acci = ti;
+    } else {
+      accr += re;
+      acci += im;
+    }
+  };
 
   // horizontal box, mask and unit phasor of the group's rows (shared-memory
   // vertical sums and centre interferograms), accumulated into accr / acci
@@ -124,8 +141,7 @@ __global__ void __launch_bounds__(ES_NT, 2) esd_kernel(const __grid_constant__ E
         const float n2 = dre * dre + dim * dim;
         if (n2 > 0.f) {
           const float inv = rsqrtf(n2);
-          accr += dre * inv;
-          acci += dim * inv;
+          accumulate(dre * inv, dim * inv);
         } else {
           // An exactly-zero double difference (a slave sample outside its
           // box) has the phase atan2 gives its signed zeros: 0, -0, pi or
@@ -133,8 +149,7 @@ __global__ void __launch_bounds__(ES_NT, 2) esd_kernel(const __grid_constant__ E
           // same signs of zero as the reference's cuCmulf products.
           float sn, cs;
           sincosf(atan2f(dim, dre), &sn, &cs);
-          accr += cs;
-          acci += sn;
+          accumulate(cs, sn);
         }
       }
     }
@@ -260,7 +275,12 @@ __global__ void __launch_bounds__(ES_NT, 2) esd_kernel(const __grid_constant__ E
     __syncthreads();
   }
   }
-  // ---- block reduction (fixed order)
+  // ---- block reduction (fixed order); Kahan's best estimate is the sum
+  // less its compensation term
+  if (comp) {
+    accr -= cr;
+    acci -= ci;
+  }
   for (int o = 16; o > 0; o >>= 1) {
     accr += __shfl_xor_sync(0xffffffffu, accr, o);
     acci += __shfl_xor_sync(0xffffffffu, acci, o);
@@ -338,7 +358,7 @@ size_t esd_scratch_bytes(const EsdOverlap *ov, int n) {
 
 int launch_esd(const EsdOverlap *ovs, int n_ov, int win_az, int win_rg, float thr,
                double *shifts, double *sums, void *scratch, size_t scratch_bytes,
-               cudaStream_t st) {
+               cudaStream_t st, int compensated) {
   if (win_rg < 1 || win_az < 1 || win_rg > ES_NT - ES_TW + 1) return TOPS_E_INVALID;
   if (esd_scratch_bytes(ovs, n_ov) > scratch_bytes || (!scratch && n_ov > 0) || !shifts)
     return TOPS_E_INVALID;
@@ -363,6 +383,7 @@ int launch_esd(const EsdOverlap *ovs, int n_ov, int win_az, int win_rg, float th
     B.win_rg = win_rg;
     B.win_az = win_az;
     B.thr = thr;
+    B.compensated = compensated;
     int items = 0;
     for (int o = o0; o < n_ov && o < o0 + ES_MAXOV; o++) {
       B.ov[B.n_ov] = ovs[o];
@@ -406,7 +427,7 @@ extern "C" int tops_esd(const tops_esd_overlap *ovs, int n_ov, int win_az, int w
     if (s != TOPS_OK) return s;
   }
   return launch_esd(O.data(), n_ov, win_az, win_rg, coh_thr, shifts_dev, sums_dev, scratch_dev,
-                    scratch_bytes, static_cast<cudaStream_t>(stream));
+                    scratch_bytes, static_cast<cudaStream_t>(stream), 0);
 }
 
 // --------------------------------------------------- allocation-free ESD
@@ -466,5 +487,22 @@ extern "C" int tops_esd_static(const tops_esd_overlap *ovs, int n_ov, int win_az
   // nothing in the shared array has to be cleared first
   return launch_esd(O, n_ov, win_az, win_rg, coh_thr, shifts_dev, sums_dev, scratch,
                     (size_t)ESD_STATIC_PARTIALS * sizeof(double2),
-                    static_cast<cudaStream_t>(stream));
+                    static_cast<cudaStream_t>(stream), 0);
 }
+
+namespace tops {
+
+int esd_launch(const tops_esd_overlap *ovs, int n_ov, int win_az, int win_rg, float coh_thr,
+               double *shifts_dev, double *sums_dev, void *scratch_dev, size_t scratch_bytes,
+               int compensated, cudaStream_t st) {
+  if ((!ovs && n_ov > 0) || n_ov < 0) return TOPS_E_INVALID;
+  std::vector<EsdOverlap> O(n_ov);
+  for (int i = 0; i < n_ov; i++) {
+    int s = fill_esd_overlap(ovs[i], O[i]);
+    if (s != TOPS_OK) return s;
+  }
+  return launch_esd(O.data(), n_ov, win_az, win_rg, coh_thr, shifts_dev, sums_dev, scratch_dev,
+                    scratch_bytes, st, compensated);
+}
+
+}  // namespace tops

@@ -20,6 +20,7 @@ struct TileCfg {
   int seg_rows = 0;
   int *counters = nullptr;
   int grid = 0;
+  int compensated = 0;   // coherence: window sums without the sliding update
 };
 
 int resample_launch(const tops_lut_dev *lut, const tops_resample_job *jobs, int njobs,
@@ -30,6 +31,11 @@ int resample_launch_multi(const tops_lut_dev *const *luts, const tops_resample_j
                           int njobs, int precision, const TileCfg &cfg, cudaStream_t st);
 int coherence_launch(const tops_coh_job *jobs, int njobs, int win_rg, int win_az,
                      const TileCfg &cfg, cudaStream_t st);
+// tops_esd with the accumulation mode: compensated = 1 sums each thread's
+// unit phasors with Kahan compensation.
+int esd_launch(const tops_esd_overlap *ovs, int n_ov, int win_az, int win_rg, float coh_thr,
+               double *shifts_dev, double *sums_dev, void *scratch_dev, size_t scratch_bytes,
+               int compensated, cudaStream_t st);
 // Same-device 2-D copies (dst row i = src row i) with the debursting gather
 // kernel, several in one launch (blockIdx.y picks the copy): HBM speed,
 // where the copy engine reaches about a third of it.  Pitches and row_bytes

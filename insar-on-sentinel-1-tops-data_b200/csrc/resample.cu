@@ -259,11 +259,13 @@ __device__ float2 interior_from_global(const ResampleJob &J, const RsLut &lut, i
   const float *kp = lut.krg + bP * kTaps;
   float sre = 0.f, sim = 0.f;
   double ph = 0.0;
+#pragma unroll 1
   for (int j = 0; j < kTaps; j++) {
     int y = L0 - 5 + j;
     double ta = (double)(y - J.s_first_line) * J.dt;
     float tre = 0.f, tim = 0.f;
     double tph = 0.0;
+#pragma unroll 1
     for (int i = 0; i < kTaps; i++) {
       int x = P0 - 5 + i;
       short2 s = J.slave[(long)(y - J.sy0) * J.slave_pitch + (x - J.sx0)];
@@ -326,31 +328,17 @@ __device__ __forceinline__ void run_load(ColRun &cr, const RsShared &S, const Re
   cr.G2 = g.y;
   cr.G1 = g.z;
   cr.G0 = g.w;
-  const int p0 = rk.y >> 12, bp = rk.y & 4095;
+  const int p0 = rk.y >> 12;
   const int xb = p0 - 5 - S.xw;
   cr.ok = p0 >= J.sx0 + 5 && p0 <= J.sx1 - 7 && xb >= 0 && xb + 13 < RS_FW;
-  if (cr.ok) {
-    const float4 *kp4 = J.lut.krg2 + bp * (kTaps / 2);
-#pragma unroll
-    for (int q = 0; q < kTaps / 2; q++) cr.w[q] = __ldg(kp4 + q);
-  }
 }
 
-// The run state of a column whose keys are taken per pixel (more key runs
-// than the table holds): weights and phase terms of `key`.
-__device__ __forceinline__ void run_from_key(ColRun &cr, const RsShared &S, const ResampleJob &J,
-                                             int key, float4 terms) {
-  cr.key = key;
-  cr.next = INT32_MAX;
-  cr.sp = terms.x;
-  cr.G2 = terms.y;
-  cr.G1 = terms.z;
-  cr.G0 = terms.w;
-  const int p0 = key >> 12, bp = key & 4095;
-  const int xb = p0 - 5 - S.xw;
-  cr.ok = p0 >= J.sx0 + 5 && p0 <= J.sx1 - 7 && xb >= 0 && xb + 13 < RS_FW;
+// The range weights of the column's current run (fast runs only).  They are
+// loaded at the start of each group's range pass and after a run change, so
+// they hold no registers during the azimuth pass.
+__device__ __forceinline__ void run_weights(ColRun &cr, const ResampleJob &J) {
   if (cr.ok) {
-    const float4 *kp4 = J.lut.krg2 + bp * (kTaps / 2);
+    const float4 *kp4 = J.lut.krg2 + (cr.key & 4095) * (kTaps / 2);
 #pragma unroll
     for (int q = 0; q < kTaps / 2; q++) cr.w[q] = __ldg(kp4 + q);
   }
@@ -444,6 +432,26 @@ __device__ __forceinline__ float2 deramp_at(const RsShared &S, const ResampleJob
     const double ta = ((unsigned)iy < (unsigned)RS_NSR) ? S.srow[iy].ta
                                                          : (double)(y - J.s_first_line) * J.dt;
     r = reduce_2pi(quad_eval(cq, ta));
+  }
+  float sn, cs;
+  __sincosf(r, &sn, &cs);
+  return make_float2(sx * cs - sy * sn, sx * sn + sy * cs);
+}
+
+// deramp_at for a line known to be staged and in the slave-line table.
+template <bool kSplit>
+__device__ __forceinline__ float2 deramp_staged(const RsShared &S, int x, int y, int ys0,
+                                                float g2c, float g1c, float g0c,
+                                                const DerampQuad &cq) {
+  const short2 v = S.stage[y & (RS_SR - 1)][x];
+  const float sx = (float)v.x, sy = (float)v.y;
+  const RsSlaveRow sr = S.srow[y - ys0];
+  float r;
+  if (kSplit) {
+    const float G = fmaf(fmaf(g2c, sr.f.tc, g1c), sr.f.tc, g0c);
+    r = reduce_2pi_f(sr.f.rho + G);
+  } else {
+    r = reduce_2pi(quad_eval(cq, sr.ta));
   }
   float sn, cs;
   __sincosf(r, &sn, &cs);
@@ -557,10 +565,15 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
     S.col_qrg[tid] = S.crg[5] * P * P;
   }
   if (tid == RS_NT - 1) {
-    // range position at the segment corners and edge midpoints -> window
+    // range position at the corners and edge midpoints of the strip over
+    // the whole master box -> window.  The window, and with it the reference
+    // column of the phase split, depends on the strip only, so a job that
+    // produces a subset of the rows gives those rows bit for bit as the
+    // whole job does.
     double pmin = 1e300;
+    const int box_rows = J.my1 - J.my0 + 1;
     for (int a = 0; a < 3; a++) {
-      const int rr = (a == 0) ? r_begin : (a == 1 ? (r_begin + r_end - 1) / 2 : r_end - 1);
+      const int rr = (a == 0) ? 0 : (a == 1 ? (box_rows - 1) / 2 : box_rows - 1);
       const double L = row_L(J, rr);
       for (int b = 0; b < 3; b++) {
         const int cc = (b == 0) ? c0 : (b == 1 ? c0 + (cN - 1) / 2 : c0 + cN - 1);
@@ -663,6 +676,8 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
         base_row = p;
         base_L0 = R.L0;
       }
+      // (window on, bit 0: filled here | bit 1: check-free loop, line of
+      // row 0, per-pixel rows)
       S.gwin[g] = make_int4(on ? 1 : 0, fill ? 1 : 0, on ? base_L0 + (p - base_row) : 0, 0);
       S.gen_n[g] = 0;
     }
@@ -765,6 +780,13 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
         }
       }
       S.gplan[g] = make_int4(c_lo, c_hi, st_lo, st_hi);
+      // a full group whose rows all take the shared pass and whose lines are
+      // all staged and in the slave-line table takes the check-free loop
+      const int4 gw = S.gwin[g];
+      const int lo_need = (gw.y & 1) ? gw.z - 5 : gw.z + 6;
+      const bool simple = gw.x && g * RS_GR + RS_GR <= nr && gw.w == 0 && lo_need >= st_lo &&
+                          hi <= st_hi && lo_need >= S.ys0 && hi < S.ys0 + RS_NSR;
+      if (simple) S.gwin[g].y = gw.y | 2;
     }
   } else if (tid >= RS_NT - RS_TW) {
     const int c = tid - (RS_NT - RS_TW);
@@ -894,9 +916,35 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
     // ---- [A] azimuth pass of the group's rows (the taps are loaded anew per
     // group, so they hold no registers during [B] and [C])
     wz_bin = -1;
-    if (gw.x) {
+    if (gw.y & 2) {
+      // every row takes the shared pass, every line is staged
       const int wl0 = gw.z;
-      if (gw.y) {
+      const int ys0 = S.ys0;
+      if (gw.y & 1) {
+#pragma unroll
+        for (int j = 0; j < RS_GR - 1; j++)
+          w[j] = deramp_staged<kSplit>(S, x, wl0 - 5 + j, ys0, g2c, g1c, g0c, cq);
+      }
+#pragma unroll
+      for (int k = 0; k < RS_GR; k++) {
+        w[(k + 11) % RS_GR] = deramp_staged<kSplit>(S, x, wl0 + k + 6, ys0, g2c, g1c, g0c, cq);
+        const int bin = S.rows[rg0 + k].bin;
+        if (bin != wz_bin) {
+          load_az_taps(S, lut, bin, wz);
+          wz_bin = bin;
+        }
+        float2 a = make_float2(0.f, 0.f), b = a;
+#pragma unroll
+        for (int j = 0; j < RS_GR; j += 2) {
+          const float4 q = wz[j >> 1];
+          a = __ffma2_rn(make_float2(q.x, q.y), w[(k + j) % RS_GR], a);
+          b = __ffma2_rn(make_float2(q.z, q.w), w[(k + j + 1) % RS_GR], b);
+        }
+        S.vd[k][x] = __fadd2_rn(a, b);
+      }
+    } else if (gw.x) {
+      const int wl0 = gw.z;
+      if (gw.y & 1) {
         // fill the window of row 0 (slots 0..10; row 0 pushes slot 11)
 #pragma unroll
         for (int j = 0; j < RS_GR - 1; j++)
@@ -936,14 +984,22 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
     // ---- [B] range pass, reramp, store: 2 columns x 6 rows per thread;
     // pixels the shared passes do not cover are listed for [C]
     if (dval0) {
+      run_weights(cr0, J);
+      run_weights(cr1, J);
 #pragma unroll 1
       for (int kk = 0; kk < RS_HR; kk++) {
         const int k = dh * RS_HR + kk;
         if (k >= gr) break;
         if ((pixmask >> k) & 1) continue;   // the whole row is done in [C]
         const int ri = rg0 + k;
-        while (ri >= cr0.next) run_load(cr0, S, J, dc, cr0.m + 1);
-        while (ri >= cr1.next) run_load(cr1, S, J, dc + 1, cr1.m + 1);
+        if (ri >= cr0.next) {
+          while (ri >= cr0.next) run_load(cr0, S, J, dc, cr0.m + 1);
+          run_weights(cr0, J);
+        }
+        if (ri >= cr1.next) {
+          while (ri >= cr1.next) run_load(cr1, S, J, dc + 1, cr1.m + 1);
+          run_weights(cr1, J);
+        }
         const int r = r_begin + ri;       // box row
         float2 *orow = J.out + (long)(r - J.row0) * J.out_pitch + c0 + dc;
         const float2 *vrow = &S.vd[k][0];
@@ -1004,6 +1060,13 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
       const int npr = __popc(pixmask);
       const int nrow_units = npr * cN;
       const int total = nrow_units + S.gen_n[g];
+      // the tile is free after [B]: each thread parks its column of the
+      // window there while the per-pixel path runs, so the window holds no
+      // registers during it
+      if (total > 0) {
+#pragma unroll
+        for (int j = 0; j < RS_GR; j++) S.vd[j][x] = w[j];
+      }
       for (int u = tid; u < total; u += RS_NT) {
         int k, c;
         if (u < nrow_units) {
@@ -1019,6 +1082,10 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
         }
         const int r = r_begin + rg0 + k;
         J.out[(long)(r - J.row0) * J.out_pitch + c0 + c] = pixel_generic(S, J, r, c);
+      }
+      if (total > 0) {
+#pragma unroll
+        for (int j = 0; j < RS_GR; j++) w[j] = S.vd[j][x];
       }
     }
   }

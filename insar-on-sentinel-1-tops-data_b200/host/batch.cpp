@@ -113,8 +113,9 @@ int batch_resample(tops_batch *B, bool esd_pass, int *counters, cudaStream_t st,
 int batch_coherence(tops_batch *B, int *counters, cudaStream_t st) {
   std::vector<tops_coh_job> cj;
   for (tops_pair *P : B->pairs) pair_coh_jobs(P, cj);
-  return tops::coherence_launch(cj.data(), (int)cj.size(), B->o.win_rg, B->o.win_az,
-                                tile(B->tune.coh_seg_rows, B->tune.coh_persistent, counters), st);
+  tops::TileCfg cfg = tile(B->tune.coh_seg_rows, B->tune.coh_persistent, counters);
+  cfg.compensated = B->o.compensated;
+  return tops::coherence_launch(cj.data(), (int)cj.size(), B->o.win_rg, B->o.win_az, cfg, st);
 }
 
 
@@ -129,7 +130,7 @@ int tops_batch_create(tops_pair *const *pairs, int n, tops_batch **out) {
     if (!P || !P->dem_set) return TOPS_E_INVALID;
     const tops_pair_opts &a = P->o, &b = pairs[0]->o;
     if (a.win_rg != b.win_rg || a.win_az != b.win_az || a.esd_threshold != b.esd_threshold ||
-        a.precision != b.precision)
+        a.precision != b.precision || a.compensated != b.compensated)
       return TOPS_E_INVALID;
     for (int k = 0; k < i; k++)
       if (pairs[k] == P) return TOPS_E_INVALID;
@@ -216,8 +217,8 @@ int tops_batch_run(tops_batch *B, void *stream) {
   if (B->n_ov > 0) {
     std::vector<tops_esd_overlap> ovs;
     for (tops_pair *P : B->pairs) pair_esd_overlaps(P, ovs);
-    B_TRY(tops_esd(ovs.data(), B->n_ov, B->o.win_az, B->o.win_rg, B->o.esd_threshold, B->d_shift,
-                   B->d_sums, B->d_esd_scratch, B->esd_scratch, stream));
+    B_TRY(tops::esd_launch(ovs.data(), B->n_ov, B->o.win_az, B->o.win_rg, B->o.esd_threshold, B->d_shift,
+                   B->d_sums, B->d_esd_scratch, B->esd_scratch, B->o.compensated, static_cast<cudaStream_t>(stream)));
     launches += 2 * chunks(ovs.size(), 32);
     for (size_t p = 0; p < B->pairs.size(); p++) {
       tops_pair *P = B->pairs[p];

@@ -10,6 +10,14 @@
 #include "launch.h"
 #include "tops_pipeline.h"
 
+// Coherence launch controls of a plan: the default tile, the accumulation
+// mode of its options.
+inline tops::TileCfg coh_cfg(const tops_pair_opts &o) {
+  tops::TileCfg c;
+  c.compensated = o.compensated;
+  return c;
+}
+
 inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 struct OrbitFit {

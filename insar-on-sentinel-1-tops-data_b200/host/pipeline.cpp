@@ -13,6 +13,7 @@
 
 #include <vector>
 
+#include "launch.h"
 #include "pair_impl.h"
 
 namespace {
@@ -81,6 +82,7 @@ int tops_pair_opts_default(tops_pair_opts *o) {
   o->reslave_full = 1;
   o->burst0_deramp_rows = 1;
   o->precision = TOPS_PREC_SPLIT;
+  o->compensated = 0;
   return TOPS_OK;
 }
 
@@ -482,8 +484,8 @@ int tops_pair_run(tops_pair *P, void *stream) {
   if (nb > 1) {
     std::vector<tops_esd_overlap> ovs;
     pair_esd_overlaps(P, ovs);
-    P_TRY(tops_esd(ovs.data(), nb - 1, P->o.win_az, P->o.win_rg, P->o.esd_threshold, P->d_shift,
-                   P->d_sums, P->d_esd_scratch, P->esd_scratch, stream));
+    P_TRY(tops::esd_launch(ovs.data(), nb - 1, P->o.win_az, P->o.win_rg, P->o.esd_threshold, P->d_shift,
+                   P->d_sums, P->d_esd_scratch, P->esd_scratch, P->o.compensated, static_cast<cudaStream_t>(stream)));
     launches += 2;
   }
   // 4. resample with the ESD shift of the preceding overlap (first burst
@@ -502,7 +504,7 @@ int tops_pair_run(tops_pair *P, void *stream) {
   // 5. coherence of master vs ReSlaveESD
   std::vector<tops_coh_job> cj;
   pair_coh_jobs(P, cj);
-  P_TRY(tops_coherence(cj.data(), nb, P->o.win_rg, P->o.win_az, stream));
+  P_TRY(tops::coherence_launch(cj.data(), nb, P->o.win_rg, P->o.win_az, coh_cfg(P->o), static_cast<cudaStream_t>(stream)));
   launches += 1;
   P->n_launches = launches;
   return TOPS_OK;
@@ -534,8 +536,8 @@ int tops_pair_stage_times(tops_pair *P, void *stream, float *ms) {
     cudaEventRecord(ev[2], st);
     if (nb > 1) {
       pair_esd_overlaps(P, ovs);
-      if ((r = tops_esd(ovs.data(), nb - 1, P->o.win_az, P->o.win_rg, P->o.esd_threshold,
-                        P->d_shift, P->d_sums, P->d_esd_scratch, P->esd_scratch, stream)) !=
+      if ((r = tops::esd_launch(ovs.data(), nb - 1, P->o.win_az, P->o.win_rg, P->o.esd_threshold,
+                        P->d_shift, P->d_sums, P->d_esd_scratch, P->esd_scratch, P->o.compensated, static_cast<cudaStream_t>(stream))) !=
           TOPS_OK)
         break;
     }
@@ -551,7 +553,7 @@ int tops_pair_stage_times(tops_pair *P, void *stream, float *ms) {
       break;
     cudaEventRecord(ev[4], st);
     pair_coh_jobs(P, cj);
-    if ((r = tops_coherence(cj.data(), nb, P->o.win_rg, P->o.win_az, stream)) != TOPS_OK) break;
+    if ((r = tops::coherence_launch(cj.data(), nb, P->o.win_rg, P->o.win_az, coh_cfg(P->o), static_cast<cudaStream_t>(stream))) != TOPS_OK) break;
     if (cudaEventRecord(ev[5], st) != cudaSuccess || cudaEventSynchronize(ev[5]) != cudaSuccess) {
       r = TOPS_E_CUDA;
       break;
@@ -585,8 +587,8 @@ int tops_pair_run_per_burst(tops_pair *P, void *stream) {
     std::vector<tops_esd_overlap> ovs;
     pair_esd_overlaps(P, ovs);
     for (int i = 0; i < nb - 1; i++) {
-      P_TRY(tops_esd(&ovs[i], 1, P->o.win_az, P->o.win_rg, P->o.esd_threshold, P->d_shift + i,
-                     P->d_sums + 2 * i, P->d_esd_scratch, P->esd_scratch, stream));
+      P_TRY(tops::esd_launch(&ovs[i], 1, P->o.win_az, P->o.win_rg, P->o.esd_threshold, P->d_shift + i,
+                     P->d_sums + 2 * i, P->d_esd_scratch, P->esd_scratch, P->o.compensated, static_cast<cudaStream_t>(stream)));
       launches += 2;
     }
   }
@@ -599,7 +601,7 @@ int tops_pair_run_per_burst(tops_pair *P, void *stream) {
   std::vector<tops_coh_job> cj;
   pair_coh_jobs(P, cj);
   for (const tops_coh_job &c : cj) {
-    P_TRY(tops_coherence(&c, 1, P->o.win_rg, P->o.win_az, stream));
+    P_TRY(tops::coherence_launch(&c, 1, P->o.win_rg, P->o.win_az, coh_cfg(P->o), static_cast<cudaStream_t>(stream)));
     launches += 1;
   }
   P->n_launches = launches;
@@ -724,13 +726,13 @@ int tops_pair_process(tops_pair *P, const void *master, const void *slave, void 
                                cudaMemcpyDeviceToHost, P->s_down));
     }
     if (b > 0) {
-      P_TRY(tops_esd(&ovs[b - 1], 1, P->o.win_az, P->o.win_rg, P->o.esd_threshold,
+      P_TRY(tops::esd_launch(&ovs[b - 1], 1, P->o.win_az, P->o.win_rg, P->o.esd_threshold,
                      P->d_shift + (b - 1), P->d_sums + 2 * (b - 1), P->d_esd_scratch,
-                     P->esd_scratch, stream));
+                     P->esd_scratch, P->o.compensated, static_cast<cudaStream_t>(stream)));
       launches += 2;
     }
     P_TRY(tops_resample_ex(P->lut, &rs2[b], 1, P->o.precision, stream));
-    P_TRY(tops_coherence(&cj[b], 1, P->o.win_rg, P->o.win_az, stream));
+    P_TRY(tops::coherence_launch(&cj[b], 1, P->o.win_rg, P->o.win_az, coh_cfg(P->o), static_cast<cudaStream_t>(stream)));
     launches += 2;
     P_CUDA(cudaEventRecord(ev_done[b], st));
     P_CUDA(cudaStreamWaitEvent(P->s_down, ev_done[b], 0));

@@ -535,7 +535,7 @@ def geocoreg_warp(dem_int, lat0, lon0, dlat, dlon, xmin, xmax, ymin, ymax, m_bur
 class PairOpts(C.Structure):
     _fields_ = [("win_rg", C.c_int), ("win_az", C.c_int), ("esd_threshold", C.c_float),
                 ("reslave_full", C.c_int), ("burst0_deramp_rows", C.c_int),
-                ("precision", C.c_int)]
+                ("precision", C.c_int), ("compensated", C.c_int)]
 
 
 class DemWindow(C.Structure):
