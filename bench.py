@@ -251,17 +251,17 @@ def batch_shapes():
                  dem_lines=3600, dem_pixels=3600, seed=40 + k) for k in range(3)]
 
 
-def run_batch(args, rank, world):
+def batch_scenes(T):
+    t0 = time.time()
+    scenes = [T.Scene(**sh) for sh in batch_shapes()]
+    return scenes, time.time() - t0
+
+
+def batch_result(T, torch, scenes, steps, warmup, world=1):
     """Batched uneven bursts: the 3 sub-swath pairs as one batch (one launch
     per stage, autotuned tiles, one CUDA graph) against the per-burst launch
     loop on the same device-resident data."""
-    import torch
-    import topsb200 as T
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     shapes = batch_shapes()
-    t0 = time.time()
-    scenes = [T.Scene(**sh) for sh in shapes]
-    gen_s = time.time() - t0
     stream = torch.cuda.Stream()
     sp = stream.cuda_stream
     opts = T.pair_opts(win_rg=WIN_RG, win_az=WIN_AZ)
@@ -292,18 +292,18 @@ def run_batch(args, rank, world):
         return e0.elapsed_time(e1) / steps
 
     with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
-        ms_batch = timed(lambda: B.run(sp, graph=True), args.steps, args.warmup)
+        ms_batch = timed(lambda: B.run(sp, graph=True), steps, warmup)
     launches_batch = B.launches()
 
     def loop():
         for P in plans:
             P.run_per_burst(sp)
-    ms_loop = timed(loop, max(2, args.steps // 4), 1)
+    ms_loop = timed(loop, max(2, steps // 4), 1)
     launches_loop = sum(P.buffers().n_launches for P in plans)
     value = world * n_pairs * 1e3 / ms_batch
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_batch, "higher_is_better": True,
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
+        "warmup": warmup, "ms_per_step": ms_batch, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 geometry)",
         "data": "synthetic (seeded); inputs > L2, no flush needed",
         "config": {"workload": "batch: 3 sub-swath pairs x 9 bursts, uneven sizes " +
@@ -314,19 +314,29 @@ def run_batch(args, rank, world):
         "tune": {"rs_seg_rows": tune.rs_seg_rows, "rs_persistent": tune.rs_persistent,
                  "coh_seg_rows": tune.coh_seg_rows, "coh_persistent": tune.coh_persistent,
                  "resample_esd_ms": float(stage_ms[0]), "coherence_ms": float(stage_ms[1])},
-        "gpu_launches": args.steps * launches_batch, "gpu_launches_per_step": launches_batch,
+        "gpu_launches": steps * launches_batch, "gpu_launches_per_step": launches_batch,
         "per_burst_loop": {"value": n_pairs * 1e3 / ms_loop, "unit": UNIT, "ms_per_step": ms_loop,
                            "launches_per_step": launches_loop,
                            "batched_over_loop": ms_loop / ms_batch},
         "resample_roofline": {"achieved_gbs": 12.0 * npx / (float(stage_ms[0]) * 1e6),
                               "peak_gbs": peaks()[0],
                               "frac": 12.0 * npx / (float(stage_ms[0]) * 1e6) / peaks()[0]},
-        "clocks": clk.summary(), "scene_gen_s": gen_s,
+        "clocks": clk.summary(),
     }
-    print(json.dumps(line), flush=True)
     B.close()
     for P in plans:
         P.close()
+    return line
+
+
+def run_batch(args, rank, world):
+    import torch
+    import topsb200 as T
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    scenes, gen_s = batch_scenes(T)
+    line = batch_result(T, torch, scenes, args.steps, args.warmup, world)
+    line["scene_gen_s"] = gen_s
+    print(json.dumps(line), flush=True)
 
 
 SERVE_RATE = 40.0          # jobs/s (Poisson)
@@ -350,7 +360,7 @@ def serve_jobs(n, shapes):
 SERVE_SEED = 7
 
 
-def run_serve(args, rank, world):
+def serve_result(T, torch, scenes, n_jobs, world=1):
     """Serving: a seeded Poisson stream of burst-pair jobs (1-9 bursts of the
     three uneven sub-swaths) through the serving loop -- admission by HBM
     footprint under a 150 GB budget, one stream per slot, DEM tiles resident.
@@ -358,13 +368,7 @@ def run_serve(args, rank, world):
     pass (all jobs at once) for the saturation throughput.  Jobs produce the
     final products (ReSlaveESD, coherence, offsets, shifts); the first-pass
     resample covers only the overlap bands ESD needs."""
-    import torch
-    import topsb200 as T
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     shapes = batch_shapes()
-    t0 = time.time()
-    scenes = [T.Scene(**sh) for sh in shapes]
-    gen_s = time.time() - t0
     pin = [(torch.from_numpy(S.slc[0]).pin_memory(), torch.from_numpy(S.slc[1]).pin_memory())
            for S in scenes]
     slc = [(a.numpy(), b.numpy()) for a, b in pin]
@@ -407,7 +411,7 @@ def run_serve(args, rank, world):
                               "p99": float(np.percentile(queue, 99))},
                     hbm_peak_gb=st.hbm_peak / 1e9)
 
-    jobs = serve_jobs(args.jobs, shapes)
+    jobs = serve_jobs(n_jobs, shapes)
     one_pass(jobs[:4], True)                        # warm-up: LUTs, kernel attributes
     with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
         open_loop = one_pass(jobs, False)
@@ -422,7 +426,7 @@ def run_serve(args, rank, world):
         "steps": 1, "warmup": 1, "ms_per_step": closed["span_s"] * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 (f64 geometry)", "data": "synthetic (seeded)",
-        "config": {"workload": f"serve: {args.jobs} Poisson jobs ({SERVE_RATE:.0f}/s), 1-9 bursts "
+        "config": {"workload": f"serve: {n_jobs} Poisson jobs ({SERVE_RATE:.0f}/s), 1-9 bursts "
                                "of 3 uneven sub-swaths",
                    "budget_gb": SERVE_BUDGET / 2**30, "slots": SERVE_SLOTS,
                    "window": f"{WIN_RG}x{WIN_AZ}"},
@@ -430,21 +434,29 @@ def run_serve(args, rank, world):
         "plain": {"value": plain, "unit": UNIT, "job": f"{S.cfg.n_bursts} bursts of "
                   f"{S.cfg.lines_per_burst}x{S.cfg.samples_per_burst}"},
         "served_over_plain": closed["pairs_per_s"] / plain,
-        "clocks": clk.summary(), "scene_gen_s": gen_s,
+        "clocks": clk.summary(),
     }
+    return line
+
+
+def run_serve(args, rank, world):
+    import torch
+    import topsb200 as T
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    scenes, gen_s = batch_scenes(T)
+    line = serve_result(T, torch, scenes, args.jobs, world)
+    line["scene_gen_s"] = gen_s
     print(json.dumps(line), flush=True)
 
 
-def run_precision(args, rank, world):
+def precision_result(T, torch, steps, warmup, world=1):
     """Precision variant on the small workload's inputs (2 bursts of 1500 x
-    4096): the pipeline with the split-precision deramp (default) and with the
-    all-FP64 deramp, each timed on the device and each output compared with
+    4096): the pipeline with the split-precision deramp (default), with the
+    all-FP64 deramp, and with the split deramp plus compensated ESD and
+    coherence sums, each timed on the device and each output compared with
     the FP64 host oracle run on the same inputs."""
-    import torch
-    import topsb200 as T
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     cfg = CONFIGS["small"]
     S = build_scene(T, cfg, 0)
     nb, L, W = cfg["n_bursts"], cfg["lines_per_burst"], cfg["samples_per_burst"]
@@ -495,22 +507,24 @@ def run_precision(args, rank, world):
     sp = stream.cuda_stream
     modes = {}
     di = S.dem_info
-    for name, prec in (("split", T.PREC_SPLIT), ("fp64", T.PREC_FP64)):
+    for name, prec, comp in (("split", T.PREC_SPLIT, 0), ("fp64", T.PREC_FP64, 0),
+                             ("split_compensated", T.PREC_SPLIT, 1)):
         P = T.Pair(S.swath[0], S.swath[1], S.dem.shape,
-                   T.pair_opts(win_rg=WIN_RG, win_az=WIN_AZ, precision=prec))
+                   T.pair_opts(win_rg=WIN_RG, win_az=WIN_AZ, precision=prec, compensated=comp))
         P.set_dem(np.rint(S.dem), di.lat0, di.lon0, di.dlat, di.dlon, T.scene_windows(S), sp)
         P.upload(S.slc[0], S.slc[1], sp)
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             P.run(sp, graph=True)
         stream.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for _ in range(args.steps):
+        for _ in range(steps):
             P.run(sp, graph=True)
         e1.record(stream)
         stream.synchronize()
-        ms = e0.elapsed_time(e1) / args.steps
+        ms = e0.elapsed_time(e1) / steps
+        stage = P.stage_times(sp)
         out = P.download(stream=sp)
         stream.synchronize()
         P.close()
@@ -540,10 +554,12 @@ def run_precision(args, rank, world):
         ats = np.unravel_index(int(np.argmax(ds)), ds.shape)
         err["reslave_esd_max_abs_over_rms"] = float(ds.max())
         err["reslave_esd_max_at"] = {"line": int(ats[0]), "sample": int(ats[1])}
-        modes[name] = {"ms_per_step": ms, "pairs_per_s": nb * 1e3 / ms, "error_vs_fp64_oracle": err}
+        modes[name] = {"ms_per_step": ms, "pairs_per_s": nb * 1e3 / ms,
+                       "esd_ms": stage["esd"], "coherence_ms": stage["coherence"],
+                       "error_vs_fp64_oracle": err}
     line = {
         "metric": METRIC, "value": modes["split"]["pairs_per_s"], "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": modes["split"]["ms_per_step"],
+        "steps": steps, "warmup": warmup, "ms_per_step": modes["split"]["ms_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 split / f64", "data": "synthetic (seeded)",
         "config": {"workload": workload_name("precision (small inputs)", cfg),
@@ -552,7 +568,14 @@ def run_precision(args, rank, world):
         "tolerances": {"offsets_px": 1e-4, "reslave_rel_rms": 1e-4, "esd_shift_px": 1e-5,
                        "coherence_max_abs": 1e-5},
     }
-    print(json.dumps(line), flush=True)
+    return line
+
+
+def run_precision(args, rank, world):
+    import torch
+    import topsb200 as T
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    print(json.dumps(precision_result(T, torch, args.steps, args.warmup, world)), flush=True)
 
 
 def workload_name(name, cfg):
@@ -573,6 +596,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=6)
     ap.add_argument("--plain-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="default run: skip the precision, batch and serving measurements")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -757,11 +782,50 @@ def main():
         v, nthreads, sample = cpu_baseline(S)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port",
                                 "sample": sample}
+    P.close()
+    if not args.no_extras and rank == 0 and world == 1 and args.config == "subswath":
+        # the other workloads, measured in the same run: precision variant
+        # (small inputs against the FP64 oracle), batched uneven sub-swaths
+        # and the serving loop (the 150 GB serving budget last: the other
+        # plans are released by then)
+        t0 = time.time()
+        line["precision"] = compact_precision(
+            precision_result(T, torch, max(3, args.steps // 2), 3))
+        scenes, _ = batch_scenes(T)
+        line["batch"] = compact_batch(batch_result(T, torch, scenes, max(3, args.steps // 2), 3))
+        line["serve"] = compact_serve(serve_result(T, torch, scenes, args.jobs))
+        line["extras_s"] = time.time() - t0
     if rank == 0:
         print(json.dumps(line), flush=True)
-    P.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+def compact_precision(p):
+    return {"workload": p["config"]["workload"], "tolerances": p["tolerances"],
+            "modes": {k: {"pairs_per_s": v["pairs_per_s"], "ms_per_step": v["ms_per_step"],
+                          "esd_ms": v["esd_ms"], "coherence_ms": v["coherence_ms"],
+                          "error_vs_fp64_oracle": {
+                              e: v["error_vs_fp64_oracle"][e]
+                              for e in ("offsets_px", "offsets_rg_px", "reslave_rel_rms",
+                                        "reslave_esd_rel_rms", "esd_shift_px",
+                                        "coherence_max_abs", "coherence_p99_99_abs",
+                                        "coherence_px_above_1e-5")}}
+                      for k, v in p["modes"].items()}}
+
+
+def compact_batch(b):
+    return {"workload": b["config"]["workload"], "value": b["value"], "unit": b["unit"],
+            "ms_per_step": b["ms_per_step"], "per_burst_loop": b["per_burst_loop"],
+            "tune": b["tune"], "resample_roofline": b["resample_roofline"],
+            "gpu_launches_per_step": b["gpu_launches_per_step"], "clocks": b["clocks"]}
+
+
+def compact_serve(v):
+    return {"workload": v["config"]["workload"], "budget_gb": v["config"]["budget_gb"],
+            "slots": v["config"]["slots"], "closed_loop": v["closed_loop"],
+            "open_loop": v["open_loop"], "plain": v["plain"],
+            "served_over_plain": v["served_over_plain"], "clocks": v["clocks"]}
 
 
 STITCH_MARGIN = 20   # invalid lines at each burst edge of the synthetic bursts

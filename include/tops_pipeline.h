@@ -150,7 +150,8 @@ int tops_pair_run_per_burst(tops_pair *p, void *stream);
  * config (npoints other than 12, empty ranges) or missing product files. */
 typedef struct {
   int subswaths, burst_pairs;   /* processed */
-  double seconds;               /* processing and writing, without scene generation */
+  double seconds;               /* wall time of the run: loading, processing and writing,
+                                   overlapped across sub-swaths */
   double shifts[TOPS_MAX_BURSTS];   /* ESD shifts of the last sub-swath */
 } tops_run_stats;
 

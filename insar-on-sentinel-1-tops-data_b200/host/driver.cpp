@@ -26,6 +26,8 @@
 #include <sys/stat.h>
 
 #include <chrono>
+#include <future>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -98,9 +100,20 @@ struct PairInputs {
   std::vector<int> first_valid, last_valid;
 };
 
-int process_pair(const tops_config &c, int nsub, tops_run_stats *st, const PairInputs &in);
+struct Product;
 
-int run_subswath(const tops_config &c, int nsub, tops_run_stats *st) {
+// One sub-swath's inputs and the storage they point into (a generated scene,
+// or two products and the DEM).  Loaded on a host thread while the GPU works
+// on the previous sub-swath.
+struct Loaded {
+  int status = TOPS_OK;
+  PairInputs in;
+  Scene scene;
+  std::unique_ptr<Product> M, S;
+  std::vector<float> dem;
+};
+
+int load_synthetic(const tops_config &c, int nsub, Loaded &out) {
   tops_synth_cfg sc;
   D_TRY(tops_synth_defaults(&sc));
   sc.seed = c.seed + 1000l * (nsub - 1);
@@ -114,18 +127,17 @@ int run_subswath(const tops_config &c, int nsub, tops_run_stats *st) {
   sc.az_shift_true = c.az_shift_true;
   const int b0 = c.burst0 - 1, k = c.burstN - c.burst0 + 1;
   if (b0 < 0 || k < 1 || b0 + k > c.n_bursts) return TOPS_E_INVALID;
-  Scene scene;
-  D_TRY(tops_synth_create(&sc, &scene.s));
+  D_TRY(tops_synth_create(&sc, &out.scene.s));
   tops_swath_info mi, si;
-  D_TRY(tops_synth_swath(scene.s, 0, &mi));
-  D_TRY(tops_synth_swath(scene.s, 1, &si));
-  PairInputs in;
+  D_TRY(tops_synth_swath(out.scene.s, 0, &mi));
+  D_TRY(tops_synth_swath(out.scene.s, 1, &si));
+  PairInputs &in = out.in;
   in.m = sub_swath(mi, b0, k);
   in.s = sub_swath(si, b0, k);
   in.k = k;
   const int L = in.m.lines_per_burst, W = in.m.samples_per_burst;
   tops_dem_info di;
-  in.dem = tops_synth_dem(scene.s, &di);
+  in.dem = tops_synth_dem(out.scene.s, &di);
   in.dem_lines = di.lines;
   in.dem_pixels = di.pixels;
   in.lat0 = di.lat0;
@@ -134,15 +146,15 @@ int run_subswath(const tops_config &c, int nsub, tops_run_stats *st) {
   in.dlon = di.dlon;
   in.win.resize(k);
   for (int i = 0; i < k; i++)
-    D_TRY(tops_synth_burst_dem_window(scene.s, b0 + i, 24, &in.win[i].row0, &in.win[i].col0,
+    D_TRY(tops_synth_burst_dem_window(out.scene.s, b0 + i, 24, &in.win[i].row0, &in.win[i].col0,
                                       &in.win[i].rows, &in.win[i].cols));
   const size_t burst_elems = (size_t)L * W * 2;   // int16 per burst
-  in.ms = tops_synth_slc(scene.s, 0) + (size_t)b0 * burst_elems;
-  in.ss = tops_synth_slc(scene.s, 1) + (size_t)b0 * burst_elems;
+  in.ms = tops_synth_slc(out.scene.s, 0) + (size_t)b0 * burst_elems;
+  in.ss = tops_synth_slc(out.scene.s, 1) + (size_t)b0 * burst_elems;
   // every line of the synthetic bursts is valid
   in.first_valid.assign(k, 0);
   in.last_valid.assign(k, L - 1);
-  return process_pair(c, nsub, st, in);
+  return TOPS_OK;
 }
 
 // ------------------------------------------------------------ products
@@ -248,8 +260,10 @@ tops_dem_window dem_window(const tops_s1_annotation &a, int b, double lat_max, d
   return w;
 }
 
-int run_subswath_product(const tops_config &c, int nsub, tops_run_stats *st) {
-  Product M, S;
+int load_products(const tops_config &c, int nsub, Loaded &out) {
+  out.M.reset(new Product());
+  out.S.reset(new Product());
+  Product &M = *out.M, &S = *out.S;
   D_TRY(load_product(c.masterpath, nsub, c.polarisation, c.preciseOrbitMaster, M));
   D_TRY(load_product(c.slavepath, nsub, c.polarisation, c.preciseOrbitSlave, S));
   const tops_s1_geogrid mg = {M.geo_lines, M.geo_points, M.az.data(), M.rg.data(), M.lat.data(),
@@ -270,7 +284,8 @@ int run_subswath_product(const tops_config &c, int nsub, tops_run_stats *st) {
   if (type != TOPS_TIFF_INT16 && type != TOPS_TIFF_FLOAT32) return TOPS_E_CONFIG;
   double gt[6];
   D_TRY(tops_tiff_georef(c.SpecificDemPath, gt));
-  std::vector<float> dem((size_t)w * h);
+  std::vector<float> &dem = out.dem;
+  dem.resize((size_t)w * h);
   if (type == TOPS_TIFF_INT16) {
     std::vector<int16_t> raw((size_t)w * h);
     D_TRY(tops_tiff_read(c.SpecificDemPath, &type, &w, &h, raw.data(), raw.size() * 2));
@@ -280,7 +295,7 @@ int run_subswath_product(const tops_config &c, int nsub, tops_run_stats *st) {
   }
   // RefDem::Init (DataTypes.cpp:200-222): upper-left corner and spacings
   const double lat_max = gt[3], lon_min = gt[0], dlat = fabs(gt[5]), dlon = fabs(gt[1]);
-  PairInputs in;
+  PairInputs &in = out.in;
   in.m = sub_swath(M.info, mb0, k);
   in.s = sub_swath(S.info, sb0, k);
   in.k = k;
@@ -299,13 +314,78 @@ int run_subswath_product(const tops_config &c, int nsub, tops_run_stats *st) {
   }
   in.ms = M.slc.data() + (size_t)mb0 * L * W * 2;
   in.ss = S.slc.data() + (size_t)sb0 * L * W * 2;
-  return process_pair(c, nsub, st, in);
+  return TOPS_OK;
 }
 
-int process_pair(const tops_config &c, int nsub, tops_run_stats *st, const PairInputs &in) {
+std::unique_ptr<Loaded> load_subswath(const tops_config &c, int nsub, bool products) {
+  std::unique_ptr<Loaded> L(new Loaded());
+  L->status = products ? load_products(c, nsub, *L) : load_synthetic(c, nsub, *L);
+  return L;
+}
+
+// Grow-only page-locked host buffer (pageable if the host cannot pin it):
+// the plan's pipelined host-to-host call overlaps its per-burst copies with
+// the kernels only on page-locked memory.
+struct HostBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  bool pinned = false;
+  HostBuf() = default;
+  HostBuf(const HostBuf &) = delete;
+  HostBuf &operator=(const HostBuf &) = delete;
+  ~HostBuf() { release(); }
+  void release() {
+    if (p) {
+      if (pinned)
+        cudaFreeHost(p);
+      else
+        free(p);
+    }
+    p = nullptr;
+    cap = 0;
+  }
+  void *get(size_t n) {
+    if (n > cap) {
+      release();
+      if (cudaHostAlloc(&p, n, cudaHostAllocDefault) == cudaSuccess) {
+        pinned = true;
+      } else {
+        (void)cudaGetLastError();
+        p = malloc(n);
+        pinned = false;
+      }
+      cap = p ? n : 0;
+    }
+    return p;
+  }
+};
+
+// One sub-swath's results, written by the writer thread.
+struct Outputs {
+  HostBuf reslave, reslave_esd, coh, stitched;
+  int k = 0, W = 0, L = 0, stitch_lines = 0, nsub = 0;
+  std::vector<double> shifts;
+};
+
+void copy_parallel(void *dst, const void *src, size_t bytes) {
+  const size_t chunk = 8u << 20;
+  const long n = (long)((bytes + chunk - 1) / chunk);
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < n; i++) {
+    const size_t o = (size_t)i * chunk;
+    memcpy(static_cast<char *>(dst) + o, static_cast<const char *>(src) + o,
+           std::min(chunk, bytes - o));
+  }
+}
+
+// The GPU stage of one sub-swath: the SLCs are copied into page-locked
+// staging and run through the plan's pipelined host-to-host call (per-burst
+// uploads, kernels and downloads overlapped on three streams), then the
+// coherence is debursted on the device.
+int process_pair(const tops_config &c, const PairInputs &in, HostBuf &stage_m, HostBuf &stage_s,
+                 Outputs &out) {
   const tops_swath_info &m = in.m, &s = in.s;
   const int k = in.k, L = m.lines_per_burst, W = m.samples_per_burst;
-  auto t0 = std::chrono::steady_clock::now();
   tops_pair_opts o;
   D_TRY(tops_pair_opts_default(&o));
   o.win_rg = c.coh_win_rg;
@@ -316,23 +396,21 @@ int process_pair(const tops_config &c, int nsub, tops_run_stats *st, const PairI
   D_TRY(tops_pair_create(&m, &s, &o, in.dem_lines, in.dem_pixels, &plan.p));
   D_TRY(tops_pair_set_dem(plan.p, in.dem, in.lat0, in.lon0, in.dlat, in.dlon, in.win.data(),
                           nullptr));
-  D_TRY(tops_pair_upload(plan.p, in.ms, in.ss, nullptr));
-  D_TRY(tops_pair_run(plan.p, nullptr));
   const size_t n = (size_t)k * L * W;
-  std::vector<float> reslave(2 * n), reslave_esd(2 * n), coh(n);
-  std::vector<double> cpm(12 * k), shifts(k > 1 ? k - 1 : 1);
-  D_TRY(tops_pair_download(plan.p, reslave.data(), reslave_esd.data(), coh.data(), cpm.data(),
-                           shifts.data(), nullptr));
-  if (cudaStreamSynchronize(nullptr) != cudaSuccess) return TOPS_E_CUDA;
-
-  // the reference's file names: <process_dir>/ReSlave-N.tif, ... (Main.cpp:98-101)
-  const std::string dir = c.process_dir, tag = "-" + std::to_string(nsub) + ".tif";
-  D_TRY(tops_tiff_write((dir + "/ReSlave" + tag).c_str(), TOPS_TIFF_CFLOAT32, W, k * L,
-                        reslave.data(), (size_t)W * 8));
-  D_TRY(tops_tiff_write((dir + "/ReSlaveESD" + tag).c_str(), TOPS_TIFF_CFLOAT32, W, k * L,
-                        reslave_esd.data(), (size_t)W * 8));
-  D_TRY(tops_tiff_write((dir + "/Coh" + tag).c_str(), TOPS_TIFF_FLOAT32, W, k * L, coh.data(),
-                        (size_t)W * 4));
+  void *ms = stage_m.get(n * 4), *ss = stage_s.get(n * 4);
+  float *rs = static_cast<float *>(out.reslave.get(n * 8));
+  float *re = static_cast<float *>(out.reslave_esd.get(n * 8));
+  float *coh = static_cast<float *>(out.coh.get(n * 4));
+  if (!ms || !ss || !rs || !re || !coh) return TOPS_E_NOMEM;
+  copy_parallel(ms, in.ms, n * 4);
+  copy_parallel(ss, in.ss, n * 4);
+  std::vector<double> cpm(12 * k);
+  out.shifts.assign(k > 1 ? k - 1 : 1, 0.0);
+  D_TRY(tops_pair_process(plan.p, ms, ss, rs, re, coh, cpm.data(), out.shifts.data(), nullptr));
+  out.k = k;
+  out.W = W;
+  out.L = L;
+  out.stitch_lines = 0;
   if (c.stitch) {
     const int *fv = in.first_valid.data(), *lv = in.last_valid.data();
     int h = 0;
@@ -343,34 +421,51 @@ int process_pair(const tops_config &c, int nsub, tops_run_stats *st, const PairI
     D_TRY(tops_pair_buffers_get(plan.p, &b));
     int *d_map = nullptr;
     float *d_out = nullptr;
-    int r = TOPS_OK;
-    if (cudaMalloc(&d_map, sizeof(int) * h) != cudaSuccess ||
-        cudaMalloc(&d_out, sizeof(float) * (size_t)h * W) != cudaSuccess)
+    float *host = static_cast<float *>(out.stitched.get(sizeof(float) * (size_t)h * W));
+    int r = host ? TOPS_OK : TOPS_E_NOMEM;
+    if (r == TOPS_OK && (cudaMalloc(&d_map, sizeof(int) * h) != cudaSuccess ||
+                         cudaMalloc(&d_out, sizeof(float) * (size_t)h * W) != cudaSuccess))
       r = TOPS_E_NOMEM;
-    std::vector<float> out((size_t)h * W);
     if (r == TOPS_OK && cudaMemcpy(d_map, map.data(), sizeof(int) * h,
                                    cudaMemcpyHostToDevice) != cudaSuccess)
       r = TOPS_E_CUDA;
     if (r == TOPS_OK)
       r = tops_stitch(b.coh, b.coh_pitch, d_out, (size_t)W * 4, d_map, h, (size_t)W * 4, nullptr);
-    if (r == TOPS_OK && cudaMemcpy(out.data(), d_out, sizeof(float) * out.size(),
+    if (r == TOPS_OK && cudaMemcpy(host, d_out, sizeof(float) * (size_t)h * W,
                                    cudaMemcpyDeviceToHost) != cudaSuccess)
       r = TOPS_E_CUDA;
     cudaFree(d_map);
     cudaFree(d_out);
+    (void)cudaGetLastError();
     D_TRY(r);
-    D_TRY(tops_tiff_write((dir + "/CohStitch" + tag).c_str(), TOPS_TIFF_FLOAT32, W, h,
-                          out.data(), (size_t)W * 4));
+    out.stitch_lines = h;
   }
-  st->seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-  st->subswaths++;
-  st->burst_pairs += k;
-  for (int i = 0; i + 1 < k && i < TOPS_MAX_BURSTS; i++) st->shifts[i] = shifts[i];
+  return TOPS_OK;
+}
+
+// The writer stage: the reference's file names, <process_dir>/ReSlave-N.tif,
+// ReSlaveESD-N.tif, Coh-N.tif (Main.cpp:98-101) and CohStitch-N.tif.
+int write_outputs(const tops_config &c, const Outputs &o) {
+  const std::string dir = c.process_dir, tag = "-" + std::to_string(o.nsub) + ".tif";
+  const int W = o.W, rows = o.k * o.L;
+  D_TRY(tops_tiff_write((dir + "/ReSlave" + tag).c_str(), TOPS_TIFF_CFLOAT32, W, rows,
+                        o.reslave.p, (size_t)W * 8));
+  D_TRY(tops_tiff_write((dir + "/ReSlaveESD" + tag).c_str(), TOPS_TIFF_CFLOAT32, W, rows,
+                        o.reslave_esd.p, (size_t)W * 8));
+  D_TRY(tops_tiff_write((dir + "/Coh" + tag).c_str(), TOPS_TIFF_FLOAT32, W, rows, o.coh.p,
+                        (size_t)W * 4));
+  if (o.stitch_lines > 0)
+    D_TRY(tops_tiff_write((dir + "/CohStitch" + tag).c_str(), TOPS_TIFF_FLOAT32, W,
+                          o.stitch_lines, o.stitched.p, (size_t)W * 4));
   return TOPS_OK;
 }
 
 }  // namespace
 
+// The sub-swaths run as a three-stage pipeline: a host thread loads
+// sub-swath n + 1 (product files or the generator) and another writes
+// sub-swath n - 1's rasters while the GPU processes sub-swath n.  The
+// results are the same as processing the sub-swaths one after another.
 extern "C" int tops_run_config(const char *config_path, tops_run_stats *stats) {
   if (!config_path || !stats) return TOPS_E_INVALID;
   memset(stats, 0, sizeof(*stats));
@@ -384,7 +479,38 @@ extern "C" int tops_run_config(const char *config_path, tops_run_stats *stats) {
   D_TRY(make_dir(c.process_dir));   // CheckDir (Main.cpp:26)
   // products unless masterpath is empty or "(synthetic)"
   const bool products = c.masterpath[0] != '\0' && strcmp(c.masterpath, "(synthetic)") != 0;
-  for (int nsub = c.firstsubswath; nsub <= c.lastsubswath; nsub++)
-    D_TRY(products ? run_subswath_product(c, nsub, stats) : run_subswath(c, nsub, stats));
-  return TOPS_OK;
+  const auto t0 = std::chrono::steady_clock::now();
+  HostBuf stage_m, stage_s;
+  Outputs outs[2];
+  std::future<std::unique_ptr<Loaded>> next =
+      std::async(std::launch::async, load_subswath, std::cref(c), c.firstsubswath, products);
+  std::future<int> writing;
+  int status = TOPS_OK;
+  for (int nsub = c.firstsubswath; nsub <= c.lastsubswath && status == TOPS_OK; nsub++) {
+    std::unique_ptr<Loaded> cur = next.get();
+    if (nsub < c.lastsubswath)
+      next = std::async(std::launch::async, load_subswath, std::cref(c), nsub + 1, products);
+    status = cur->status;
+    if (status != TOPS_OK) break;
+    // the slot written two sub-swaths ago is free once that write is done
+    Outputs &o = outs[nsub & 1];
+    status = process_pair(c, cur->in, stage_m, stage_s, o);
+    if (writing.valid()) {
+      const int w = writing.get();
+      if (status == TOPS_OK) status = w;
+    }
+    if (status != TOPS_OK) break;
+    o.nsub = nsub;
+    stats->subswaths++;
+    stats->burst_pairs += o.k;
+    for (int i = 0; i + 1 < o.k && i < TOPS_MAX_BURSTS; i++) stats->shifts[i] = o.shifts[i];
+    writing = std::async(std::launch::async, write_outputs, std::cref(c), std::cref(o));
+  }
+  if (writing.valid()) {
+    const int w = writing.get();
+    if (status == TOPS_OK) status = w;
+  }
+  if (next.valid()) next.wait();   // a load still running when an error ended the loop
+  stats->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return status;
 }
