@@ -48,6 +48,13 @@ const char *tops_status_string(int status);
 int tops_last_cuda_error(void);
 /* Library version string. */
 const char *tops_version(void);
+
+/* Measured FP64 fused-multiply-add throughput of the current device in
+ * TFLOP/s (2 flops per FMA), timed with CUDA events on `stream` under the
+ * clocks the device runs at.  No counterpart in the reference: it is the
+ * denominator of the geometric coregistration's roofline, a stage bound by
+ * FP64 arithmetic rather than by memory. */
+int tops_fp64_peak(double *tflops, void *stream);
 /* Waits for the work enqueued on `stream` (NULL: the legacy stream). */
 int tops_stream_synchronize(void *stream);
 

@@ -203,9 +203,14 @@ __global__ void __launch_bounds__(GC_NT, 2) geocoreg_kernel(const __grid_constan
   const int tiles = tiles_x * ((J.lines + GC_TR - 1) / GC_TR);
   const double ymid = 0.5 * ((double)J.ymin + (double)J.ymax);
   const double xmid = 0.5 * ((double)J.xmin + (double)J.xmax);
-  double acc[GC_NSUM];
+  // sums of the monomials L^i P^j (i + j <= 4) of the design row a = (1, L,
+  // P, L^2, LP, P^2) -- its 21 distinct products a_i a_j are 15 monomials --
+  // and of a_i times the slave line and pixel: 27 accumulators, expanded to
+  // the 33 normal-equation sums after the loop
+  constexpr int GC_NMOM = 27;
+  double acc[GC_NMOM];
 #pragma unroll
-  for (int q = 0; q < GC_NSUM; q++) acc[q] = 0.0;
+  for (int q = 0; q < GC_NMOM; q++) acc[q] = 0.0;
 
   for (int tile = lblk; tile < tiles; tile += J.blocks) {
     const int row0 = (tile / tiles_x) * GC_TR;
@@ -262,23 +267,33 @@ __global__ void __launch_bounds__(GC_NT, 2) geocoreg_kernel(const __grid_constan
       }
       const double L = (ml - ymid) * J.inv_yq;
       const double P = (mp - xmid) * J.inv_xq;
-      const double a[6] = {1.0, L, P, L * L, L * P, P * P};
-      int q = 0;
+      const double L2 = L * L, LP = L * P, P2 = P * P;
+      const double a[6] = {1.0, L, P, L2, LP, P2};
+      // monomials in the order M00 M10 M01 M20 M11 M02 M30 M21 M12 M03 M40
+      // M31 M22 M13 M04
+      const double m[15] = {1.0, L, P, L2, LP, P2, L2 * L, L2 * P, L * P2, P2 * P,
+                            L2 * L2, L2 * LP, L2 * P2, LP * P2, P2 * P2};
 #pragma unroll
-      for (int i = 0; i < 6; i++)
-#pragma unroll
-        for (int j = i; j < 6; j++) acc[q++] += a[i] * a[j];
+      for (int q = 0; q < 15; q++) acc[q] += m[q];
 #pragma unroll
       for (int i = 0; i < 6; i++) {
-        acc[21 + i] += a[i] * sl;
-        acc[27 + i] += a[i] * sp;
+        acc[15 + i] = fma(a[i], sl, acc[15 + i]);
+        acc[21 + i] = fma(a[i], sp, acc[21 + i]);
       }
     }
   }
+  // the 33 sums: a_i a_j (i <= j, row-major) from the monomials, then the
+  // slave-line and slave-pixel sums
+  constexpr int kMono[21] = {0, 1, 2, 3, 4, 5,     // 1 x (1 L P L2 LP P2)
+                             3, 4, 6, 7, 8,        // L x (L P L2 LP P2)
+                             5, 7, 8, 9,           // P x (P L2 LP P2)
+                             10, 11, 12,           // L2 x (L2 LP P2)
+                             12, 13,               // LP x (LP P2)
+                             14};                  // P2 x P2
   // fixed-order block reduction
 #pragma unroll
   for (int q = 0; q < GC_NSUM; q++) {
-    double v = acc[q];
+    double v = q < 21 ? acc[kMono[q]] : acc[q - 6];
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5][q] = v;
   }

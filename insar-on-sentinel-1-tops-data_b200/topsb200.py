@@ -208,6 +208,7 @@ _proto("tops_synth_burst_dem_window", C.c_int, [_vp, C.c_int, C.c_int, _ip, _ip,
 _proto("tops_synth_truth", C.c_int, [_vp, C.c_int, C.POINTER(C.c_long), C.POINTER(_dp)])
 _proto("tops_synth_timing", C.c_int, [_vp, _dp])
 # reference-compatible ABI (host buffers)
+_proto("tops_fp64_peak", C.c_int, [_dp, _vp])
 _proto("GeoCoreg_warp_cuda", C.c_int,
        [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int,
         C.c_int, _dp, _dp, C.c_double, C.c_double, C.c_int, C.c_double, C.c_double, C.c_double,
@@ -238,6 +239,13 @@ _proto("tops_esd_static", C.c_int, [C.POINTER(EsdOverlap), C.c_int, C.c_int, C.c
                                     _vp, _vp, _vp])
 _proto("tops_geocoreg_scratch_bytes", C.c_size_t, [C.POINTER(GeoJob), C.c_int])
 _proto("tops_geocoreg", C.c_int, [C.POINTER(GeoJob), C.c_int, _vp, C.c_size_t, _vp])
+
+
+def fp64_peak(stream=0) -> float:
+    """Measured FP64 FMA throughput of the device, TFLOP/s."""
+    v = C.c_double(0.0)
+    check(lib.tops_fp64_peak(C.byref(v), C.c_void_p(stream)), "tops_fp64_peak")
+    return v.value
 
 
 def ptr(a: np.ndarray, ctype):
