@@ -301,7 +301,7 @@ constexpr int CT_TW = 240;                 // output columns per strip
 constexpr int CT_CPI = 4;                  // outputs per horizontal item
 constexpr int CT_SEG = 256;                // rows per work item
 constexpr int CT_MAXJOBS = 16;
-constexpr long CT_WAIT_LIMIT = 1L << 26;   // mbarrier polls before a chunk is given up
+constexpr unsigned long long CT_WAIT_NS = 2000000000ull;   // a chunk is given up after 2 s
 static_assert(CT_XOFF % 4 == 0 && CT_XOFF == CT_DX, "box x coordinates stay 16-byte aligned");
 static_assert(CT_XOFF + CT_TW + CT_WRG - 1 - CT_DX <= CT_LW, "the strip's boxes cover its windows");
 static_assert(CT_TW % CT_CPI == 0 && CT_CH * (CT_TW / CT_CPI) <= CT_NT, "one horizontal item per thread");
@@ -357,11 +357,20 @@ __device__ __forceinline__ void ct_tma_2d(void *dst, const CUtensorMap *tm, int 
       "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(ct_smem(bar))
       : "memory");
 }
-// Waits for the slot's chunk with a bounded number of polls; false if it
-// never arrived (recorded in g_coh_wait_faults).
+__device__ __forceinline__ unsigned long long ct_now_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Waits for the slot's chunk for at most CT_WAIT_NS of wall time (the
+// bound is on time, not on polls: a poll may suspend the thread); false if
+// it never arrived (recorded in g_coh_wait_faults).
 __device__ __forceinline__ bool ct_wait(unsigned long long *bar, unsigned parity) {
-  for (long it = 0; it < CT_WAIT_LIMIT; it++)
+  if (ct_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = ct_now_ns();
+  do {
     if (ct_try_wait(bar, parity)) return true;
+  } while (ct_now_ns() - t0 < CT_WAIT_NS);
   return false;
 }
 

@@ -50,10 +50,17 @@
 //        (row; M0..M2 the azimuth taps' moments, tc0 = tc(L0)),
 // equal to the reference's sum in exact arithmetic.
 //
-// Rows or pixels outside these cases (several keys in a row, edge and
-// outside pixels, range supports beyond the ring window, columns with more
-// than RS_MAXRUN key runs) take a per-pixel path that computes the same
-// formula from the slave in HBM.
+// Every row whose strip maps to one azimuth key takes the shared pass: from
+// the register window when its line is the window's, else (the row-to-line
+// map skipped a line inside a group) by the same 12-line sum over lines
+// deramped anew.  A column with more than RS_MAXRUN key runs in the item
+// finds each pixel's key and run terms with the functions that build the
+// run tables.  Rows with several azimuth keys, and pixels whose range
+// support leaves the ring window, take a per-pixel path that computes the
+// reference's formula from the slave in HBM; edge and outside pixels take
+// the nearest sample and 0.  Which path a pixel takes depends on its row,
+// its column and its strip only, never on the work item, so a job that
+// produces a subset of the rows gives those rows bit for bit.
 //
 // Precision modes: TOPS_PREC_SPLIT (default) forms each sample's deramp
 // phase in FP32 as rho(y) + G(y, x), rho the FP64 reference phase reduced
@@ -140,7 +147,9 @@ struct __align__(16) RsShared {
                                       // rows without a shared azimuth pass (bit mask)
   int2 grange[RS_NGRP];               // per group: lines its window pushes need
   int gen_n[RS_NGRP];                 // per group: pixels deferred to the per-pixel pass
-  unsigned short gen[RS_GR * RS_TW];  // their (row in group) * 128 + column
+  int gen_d[RS_NGRP];                 // per group: pixels of columns without a run table
+  unsigned short gen[RS_GR * RS_TW];  // their (row in group) * 128 + column: the first
+                                      // from the bottom, the second from the top
   int scan[RS_NT / 32];               // per-warp totals of the bin-change scan
   double caz[6], crg[6], shift;
   double ref_a0, ref_a1, ref_a2, tm;
@@ -481,12 +490,22 @@ __device__ __forceinline__ void stage_rows(RsShared &S, const ResampleJob &J, in
                                            bool xin, int lo, int hi) {
   const short2 *const sl = J.slave;
   const long pitch = J.slave_pitch;
-  const unsigned rows_in = (unsigned)(J.sy1 - J.sy0);
-  long off = (long)(lo - J.sy0) * pitch + (xa - J.sx0);
+  const unsigned base = smem_u32(&S.stage[0][x]);
+  constexpr unsigned kRow = RS_FW * sizeof(short2);
+  if (xin && lo >= J.sy0 && hi <= J.sy1) {
+    // every line inside the slave box (the usual case): no per-line checks
+    const short2 *src = sl + (long)(lo - J.sy0) * pitch + (xa - J.sx0);
 #pragma unroll 4
-  for (int y = lo; y <= hi; y++, off += pitch) {
-    const bool in = xin && (unsigned)(y - J.sy0) <= rows_in;
-    cp_async_4s(smem_u32(&S.stage[y & (RS_SR - 1)][x]), sl + (in ? off : 0), in ? 4 : 0);
+    for (int y = lo; y <= hi; y++, src += pitch)
+      cp_async_4s(base + (unsigned)(y & (RS_SR - 1)) * kRow, src, 4);
+  } else {
+    const unsigned rows_in = (unsigned)(J.sy1 - J.sy0);
+    long off = (long)(lo - J.sy0) * pitch + (xa - J.sx0);
+#pragma unroll 1
+    for (int y = lo; y <= hi; y++, off += pitch) {
+      const bool in = xin && (unsigned)(y - J.sy0) <= rows_in;
+      cp_async_4s(base + (unsigned)(y & (RS_SR - 1)) * kRow, sl + (in ? off : 0), in ? 4 : 0);
+    }
   }
   cp_async_commit();
 }
@@ -514,6 +533,34 @@ __device__ __forceinline__ float4 run_terms(const RsShared &S, const RsLut &lut,
     gg.w = G0;
   }
   return gg;
+}
+
+// A pixel of a shared row (its azimuth-interpolated row in vrow) whose
+// column has no run table: its range key and the key's run terms are found
+// here, by the same functions the run tables are built with, so the result
+// is the one the run path gives.
+__device__ __forceinline__ float2 pixel_keyed(const RsShared &S, const ResampleJob &J,
+                                           const RsRow &R, const float2 *vrow, int r, int c) {
+  ColRun cr;
+  cr.key = rg_key(S, J, r, c);
+  const float4 g = run_terms(S, J.lut, S.xw, cr.key);
+  cr.sp = g.x;
+  cr.G2 = g.y;
+  cr.G1 = g.z;
+  cr.G0 = g.w;
+  const int p0 = cr.key >> 12;
+  const int xb = p0 - 5 - S.xw;
+  cr.ok = p0 >= J.sx0 + 5 && p0 <= J.sx1 - 7 && xb >= 0 && xb + 13 < RS_FW;
+  if (cr.ok) {
+    run_weights(cr, J);
+    return cmul_conj_phase(range_single(vrow, xb, cr), run_phase(R, cr));
+  }
+  if (p0 < J.sx0 || p0 > J.sx1) return make_float2(0.f, 0.f);
+  if (p0 < J.sx0 + 5 || p0 > J.sx1 - 7) {
+    const short2 sv = J.slave[(long)(R.L0 - J.sy0) * J.slave_pitch + (p0 - J.sx0)];
+    return make_float2((float)sv.x, (float)sv.y);
+  }
+  return pixel_generic(S, J, r, c);
 }
 
 // One work item (strip x segment of one job); all threads of the CTA call it
@@ -658,28 +705,48 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
   }
   __syncthreads();
 
-  // ---- [P5] thread 0: the window of the azimuth pass over the groups.
-  // The window advances one line per row; it is (re)filled at the start of
-  // a group whose first row takes a shared pass on a line the window does
-  // not expect.  A row takes the shared pass when its line is the window's.
+  // ---- [P5] the window of the azimuth pass over the groups.  The window
+  // advances one line per row; a group whose first row with a single key
+  // finds another line than the window expects (or no window yet) fills it
+  // anew at the group's start, with the line of that row extrapolated back
+  // one line per row.  A row takes the shared pass when it has a single key
+  // and its line is the window's.  Thread g finds group g's first
+  // single-key row; thread 0 then chains the groups.
+  {
+    const int ngrp = (nr + RS_GR - 1) / RS_GR;
+    if (tid < ngrp) {
+      int k1 = -1, l1 = 0;
+      for (int k = 0; k < RS_GR && tid * RS_GR + k < nr; k++) {
+        const RsRow &R = S.rows[tid * RS_GR + k];
+        if (R.mode) {
+          k1 = k;
+          l1 = R.L0;
+          break;
+        }
+      }
+      S.grange[tid] = make_int2(k1, l1);
+    }
+  }
+  __syncthreads();
   if (tid == 0) {
     const int ngrp = (nr + RS_GR - 1) / RS_GR;
     bool on = false;
     int base_row = 0, base_L0 = 0;
     for (int g = 0; g < ngrp; g++) {
       const int p = g * RS_GR;
-      const RsRow &R = S.rows[p];
+      const int2 f = S.grange[g];   // first single-key row of the group, its line
       bool fill = false;
-      if (R.mode && (!on || R.L0 != base_L0 + (p - base_row))) {
+      if (f.x >= 0 && (!on || f.y != base_L0 + (p + f.x - base_row))) {
         fill = true;
         on = true;
-        base_row = p;
-        base_L0 = R.L0;
+        base_row = p + f.x;
+        base_L0 = f.y;
       }
       // (window on, bit 0: filled here | bit 1: check-free loop, line of
       // row 0, per-pixel rows)
       S.gwin[g] = make_int4(on ? 1 : 0, fill ? 1 : 0, on ? base_L0 + (p - base_row) : 0, 0);
       S.gen_n[g] = 0;
+      S.gen_d[g] = 0;
     }
     S.ngrp = ngrp;
   }
@@ -692,12 +759,7 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
   {
     const int lane = tid & 31, warp = tid >> 5;
     const int r0 = 2 * tid, r1 = r0 + 1;
-    auto shared_row = [&](int ri) -> bool {
-      if (ri >= nr) return false;
-      const RsRow &R = S.rows[ri];
-      const int4 gw = S.gwin[ri / RS_GR];
-      return R.mode && gw.x && R.L0 == gw.z + ri % RS_GR;
-    };
+    auto shared_row = [&](int ri) -> bool { return ri < nr && S.rows[ri].mode; };
     const bool h0 = shared_row(r0), h1 = shared_row(r1);
     const bool p0 = r0 > 0 && shared_row(r0 - 1);
     auto bin_of = [&](int ri) { return S.rows[ri].bin & 0xffff; };
@@ -716,9 +778,16 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
       const int4 gw = S.gwin[tid];
       const int gr = min(RS_GR, nr - tid * RS_GR);
       if (gw.x) ymin = gw.z - (gw.y ? 5 : -6);
+      // rows without a shared pass (bits 0..11) and shared rows whose line
+      // is not the window's, summed directly (bits 16..27)
       int mask = 0;
-      for (int k = 0; k < gr; k++)
-        if (!shared_row(tid * RS_GR + k)) mask |= 1 << k;
+      for (int k = 0; k < gr; k++) {
+        const int ri = tid * RS_GR + k;
+        if (!shared_row(ri))
+          mask |= 1 << k;
+        else if (!gw.x || S.rows[ri].L0 != gw.z + k)
+          mask |= 1 << (16 + k);
+      }
       S.grange[tid] = gw.x ? make_int2(gw.y ? gw.z - 5 : gw.z + 6, gw.z + gr - 1 + 6)
                            : make_int2(1, 0);
       S.gwin[tid].w = mask;
@@ -911,7 +980,8 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
     const int gr = min(RS_GR, nr - rg0);
     const int4 plan = S.gplan[g];
     const int4 gw = S.gwin[g];
-    const int pixmask = gw.w;
+    const int pixmask = gw.w & 0xfff;     // rows without a shared pass
+    const int dirmask = gw.w >> 16;       // shared rows off the window's line
     cp_async_wait_all();                  // this thread's staged lines of the group
     // ---- [A] azimuth pass of the group's rows (the taps are loaded anew per
     // group, so they hold no registers during [B] and [C])
@@ -956,7 +1026,7 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
         if (k < gr) {
           w[(k + 11) % RS_GR] = deramp_at<kSplit>(S, J, x, xa, xin, wl0 + k + 6, plan.z, plan.w,
                                                   g2c, g1c, g0c, cq);
-          if (!((pixmask >> k) & 1)) {
+          if (!(((pixmask | dirmask) >> k) & 1)) {
             const int bin = S.rows[rg0 + k].bin;
             if (bin != wz_bin) {
               load_az_taps(S, lut, bin, wz);
@@ -972,6 +1042,29 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
             S.vd[k][x] = __fadd2_rn(a, b);
           }
         }
+      }
+    }
+    if (dirmask) {
+      // shared rows whose line is not the window's (the row-to-line map
+      // skipped a line inside the group): the same sum, in the same order,
+      // over lines deramped anew
+#pragma unroll 1
+      for (int m = dirmask; m; m &= m - 1) {
+        const int k = __ffs(m) - 1;
+        const RsRow &R = S.rows[rg0 + k];
+        const float *kl = lut.kaz + (R.bin & 0xffff) * kTaps;
+        float2 a = make_float2(0.f, 0.f), b = a;
+#pragma unroll 1
+        for (int j = 0; j < RS_GR; j += 2) {
+          const float wa = __ldg(kl + j), wb = __ldg(kl + j + 1);
+          const float2 d0 = deramp_at<kSplit>(S, J, x, xa, xin, R.L0 - 5 + j, plan.z, plan.w,
+                                              g2c, g1c, g0c, cq);
+          const float2 d1 = deramp_at<kSplit>(S, J, x, xa, xin, R.L0 - 4 + j, plan.z, plan.w,
+                                              g2c, g1c, g0c, cq);
+          a = __ffma2_rn(make_float2(wa, wa), d0, a);
+          b = __ffma2_rn(make_float2(wb, wb), d1, b);
+        }
+        S.vd[k][x] = __fadd2_rn(a, b);
       }
     }
     // stage the next group's new lines; they land while [B] runs
@@ -1037,7 +1130,10 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
             const ColRun &cr = cc ? cr1 : cr0;
             const bool dense = cc ? dense1 : dense0;
             const int p0 = cr.key >> 12;
-            if (dense || (p0 >= J.sx0 + 5 && p0 <= J.sx1 - 7 && !cr.ok)) {
+            if (dense) {
+              const int e = atomicAdd(&S.gen_d[g], 1);
+              S.gen[RS_GR * RS_TW - 1 - e] = (unsigned short)(k * 128 + dc + cc);
+            } else if (p0 >= J.sx0 + 5 && p0 <= J.sx1 - 7 && !cr.ok) {
               const int e = atomicAdd(&S.gen_n[g], 1);
               S.gen[e] = (unsigned short)(k * 128 + dc + cc);
             } else if (cr.ok) {
@@ -1053,6 +1149,23 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
       }
     }
     __syncthreads();
+
+    // ---- [C1] pixels of shared rows in columns without a run table, all
+    // threads: the range key and its run terms per pixel, then the range
+    // pass over the tile as in [B]
+    {
+      const int nd = S.gen_d[g];
+      if (nd > 0) {
+        for (int u = tid; u < nd; u += RS_NT) {
+          const int code = S.gen[RS_GR * RS_TW - 1 - u];
+          const int k = code >> 7, c = code & 127;
+          const int r = r_begin + rg0 + k;
+          J.out[(long)(r - J.row0) * J.out_pitch + c0 + c] =
+              pixel_keyed(S, J, S.rows[rg0 + k], &S.vd[k][0], r, c);
+        }
+        __syncthreads();
+      }
+    }
 
     // ---- [C] per-pixel path, all threads: the rows without a shared pass,
     // then the listed pixels

@@ -96,9 +96,10 @@ def test_resample_steep_polynomial(T, O, scene_small):
     assert rel_rms(gpu, ref) < RS_TOL
 
 
-def _resample_device(T, kw, precision, out_offset=0, slave_offset=0):
+def _resample_device(T, kw, precision, out_offset=0, slave_offset=0, rows=None):
     """tops_resample_ex on device buffers; out_offset / slave_offset (bytes)
-    misalign the output and slave bases to force the scalar-access paths."""
+    misalign the output and slave bases to force the scalar-access paths;
+    rows = (row0, n) produces only master rows row0 .. row0 + n - 1."""
     import ctypes as C
     import torch
     slave = np.ascontiguousarray(kw["slave"], np.int16)
@@ -125,14 +126,15 @@ def _resample_device(T, kw, precision, out_offset=0, slave_offset=0):
     j.az_shift = kw["az_shift"]
     j.s_first_line = kw["s_burst_idx"] * kw["lines_per_burst"]
     j.dt = kw["dt"]
-    j.out_row0, j.out_rows = 0, -1
+    j.out_row0, j.out_rows = (0, -1) if rows is None else rows
     stream = torch.cuda.current_stream().cuda_stream
     T.check(T.lib.tops_resample_ex(lut, C.byref(j), 1, precision, C.c_void_p(stream)),
             "tops_resample_ex")
     torch.cuda.synchronize()
     T.lib.tops_lut_destroy(lut)
     out = o_dev[out_offset:out_offset + L * W * 8].cpu().numpy().view(np.complex64)
-    return out.reshape(L, W)
+    out = out.reshape(L, W)
+    return out if rows is None else out[:rows[1]]
 
 
 @pytest.mark.parametrize("prec", ["split", "fp64"])
@@ -287,3 +289,21 @@ def test_geocoreg_not_positive_definite(T, scene_small):
                         (np.array(m.sv_t[:m.n_sv]), np.array(s.sv_t[:s.n_sv])), g["coefs"],
                         g["azi_init"], S.cfg.samples_per_burst)
     assert ei.value.status == T.TOPS_E_NOT_PD
+
+
+@pytest.mark.parametrize("prec", ["split", "fp64"])
+def test_resample_row_subset_bit_exact(T, O, scene_esd, prec):
+    """A job that produces a subset of the master rows (the overlap bands of
+    the band-only dataflow, or any other range) gives those rows bit for bit
+    as the job over the whole burst: the kernel's choices (ring window,
+    phase reference column, work items) do not depend on the row range."""
+    S = scene_esd
+    cpm = oracle_cpm(O, S, 1)
+    kw = rs_inputs(S, 1, cpm, 0.0123)
+    mode = T.PREC_SPLIT if prec == "split" else T.PREC_FP64
+    full = _resample_device(T, kw, mode)
+    L, ov = S.cfg.lines_per_burst, S.cfg.overlap_lines
+    for r0, n in ((L - ov, ov), (0, ov), (123, 54), (7, 1)):
+        part = _resample_device(T, kw, mode, rows=(r0, n))
+        bad = np.argwhere(part != full[r0:r0 + n])
+        assert bad.size == 0, (r0, n, bad[:8].tolist(), bad.shape[0])
