@@ -578,6 +578,41 @@ def run_precision(args, rank, world):
     print(json.dumps(precision_result(T, torch, args.steps, args.warmup, world)), flush=True)
 
 
+def run_product(args, rank, world):
+    """The config.txt-driven run (tops_run_config) over 3 synthetic sub-swaths
+    of 3 bursts of 1500 x 21000, writing ReSlave, ReSlaveESD and Coh TIFFs:
+    its wall time against the summed load (synthetic generation), pair-run
+    and write times, which the run overlaps across sub-swaths."""
+    import shutil
+    import tempfile
+    import topsb200 as T
+    if rank != 0:
+        return
+    d = tempfile.mkdtemp(prefix="tops_run_")
+    try:
+        keys = dict(process_dir=os.path.join(d, "out"), masterpath="(synthetic)",
+                    slavepath="(synthetic)", firstsubswath=1, lastsubswath=3, burst0=1, burstN=3,
+                    stitch=0, **CONFIGS["subswath3"])
+        cfg = os.path.join(d, "config.txt")
+        with open(cfg, "w") as f:
+            f.write("".join(f"{k}={v}\n" for k, v in keys.items()))
+        st = T.run_config(cfg)
+        written = sum(os.path.getsize(os.path.join(d, "out", n)) for n in os.listdir(os.path.join(d, "out")))
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    serial = st.load_seconds + st.process_seconds + st.write_seconds
+    print(json.dumps({
+        "metric": "burst-pairs/s (config run: synthetic inputs, TIFF outputs)",
+        "value": st.burst_pairs / st.seconds, "unit": UNIT, "n_gpus": 1,
+        "higher_is_better": True,
+        "config": {"workload": "3 sub-swaths x 3 bursts of 1500x21000, DEM 3600x3600",
+                   "window": f"{WIN_RG}x{WIN_AZ}"},
+        "seconds": st.seconds, "load_seconds": st.load_seconds,
+        "process_seconds": st.process_seconds, "write_seconds": st.write_seconds,
+        "serial_sum_seconds": serial, "overlap_saved_seconds": serial - st.seconds,
+        "bytes_written": written}), flush=True)
+
+
 def workload_name(name, cfg):
     return (f"{name}: {cfg['n_bursts']} burst pairs of {cfg['lines_per_burst']}x"
             f"{cfg['samples_per_burst']} CInt16, {cfg['overlap_lines']}-line overlaps, DEM "
@@ -591,7 +626,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="subswath",
-                    choices=sorted(CONFIGS) + ["batch", "serve", "precision"])
+                    choices=sorted(CONFIGS) + ["batch", "serve", "precision", "product"])
     ap.add_argument("--jobs", type=int, default=40, help="serve: number of arriving jobs")
     ap.add_argument("--e2e-steps", type=int, default=6)
     ap.add_argument("--plain-steps", type=int, default=2)
@@ -610,6 +645,8 @@ def main():
         return run_serve(args, rank, world)
     if args.config == "precision":
         return run_precision(args, rank, world)
+    if args.config == "product":
+        return run_product(args, rank, world)
 
     import torch
     import torch.distributed as dist
@@ -681,6 +718,8 @@ def main():
         dist.barrier()
     ms = e0.elapsed_time(e1) / args.steps
     launches_per_step = P.buffers().n_launches   # counted by the runs above
+    overlap = overlap_report(T, torch, S, windows, stream, h_m, h_s, args.steps, args.warmup,
+                             dist, world, nb)
     ms_max = max_over_ranks(ms, dist, world, "cuda")
     value = whole_job_value(world, nb, ms_max)
 
@@ -774,6 +813,7 @@ def main():
                      "algorithmic_bytes_per_launch": rs_bytes, "launch_ms": rs_ms,
                      "peak_kind": peak_kind},
         "stages": stages,
+        "coh_overlap": overlap,
         "hbm_ceilings": ceilings,
         "clocks": clk.summary(),
         "scene_gen_s": gen_s,
@@ -866,6 +906,39 @@ def stitch_report(T, P, S, torch, stream, steps):
     return out
 
 
+def overlap_report(T, torch, S, windows, stream, h_m, h_s, steps, warmup, dist, world, nb):
+    """The same graph step with tops_pair_opts.coh_overlap = 1: each burst's
+    coherence on a second stream right after its ReSlaveESD resample."""
+    import ctypes as C
+    sp = stream.cuda_stream
+    di = S.dem_info
+    Q = T.Pair(S.swath[0], S.swath[1], S.dem.shape,
+               T.pair_opts(win_rg=WIN_RG, win_az=WIN_AZ, coh_overlap=1))
+    Q.set_dem(S.dem, di.lat0, di.lon0, di.dlat, di.dlon, windows, sp)
+    T.check(T.lib.tops_pair_upload(Q._h, C.c_void_p(h_m.data_ptr()), C.c_void_p(h_s.data_ptr()),
+                                   C.c_void_p(sp)), "upload")
+    step = lambda: T.check(T.lib.tops_pair_run_graph(Q._h, C.c_void_p(sp)), "run_graph")
+    for _ in range(warmup):
+        step()
+    stream.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    stream.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1) / steps, dist, world, "cuda")
+    launches = Q.buffers().n_launches
+    Q.close()
+    return {"value": whole_job_value(world, nb, ms), "ms_per_step": ms,
+            "launches_per_step": launches,
+            "form": "graph step, coherence of each burst on a second stream after its "
+                    "ReSlaveESD resample (same outputs bit for bit)"}
+
+
 def stage_report(T, P, S, windows, sp, steps):
     """Per-stage device time of the pair (tops_pair_stage_times, averaged
     over `steps` eager runs), with each stage's algorithmic bytes, achieved
@@ -892,6 +965,19 @@ def stage_report(T, P, S, windows, sp, steps):
     out["geocoreg"]["dem_px"] = dem_px
     out["geocoreg"]["dem_mpx_per_s"] = dem_px / (ms["geocoreg"] * 1e-3) / 1e6
     out["geocoreg"]["bound"] = "fp64"
+    # FP64 roofline: FP64 operations per DEM pixel from an ncu count of the
+    # kernel on this workload (DFMA counted twice), over the FP64 FMA rate
+    # measured on this device now
+    gf = os.path.join(ROOT, "profiles", "geocoreg_fp64.json")
+    if os.path.exists(gf):
+        per_px = json.load(open(gf)).get("fp64_flops_per_dem_px")
+        if per_px:
+            pk = T.fp64_peak(sp)
+            tf = per_px * dem_px / (ms["geocoreg"] * 1e-3) / 1e12
+            out["geocoreg"].update({"fp64_tflops": tf, "fp64_peak_tflops": pk,
+                                    "frac_fp64": tf / pk if pk > 0 else None,
+                                    "fp64_flops_per_dem_px": per_px,
+                                    "fp64_peak_kind": "measured (tops_fp64_peak)"})
     return out
 
 

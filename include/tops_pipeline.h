@@ -44,6 +44,11 @@ typedef struct {
                                coherence window sums without the sliding
                                update (pairwise per output); 0 (default): the
                                plain fixed-order FP32 sums */
+  int coh_overlap;          /* 1: the coherence of each ReSlaveESD burst runs
+                               on a second stream as soon as that burst is
+                               resampled, overlapping the resampling of the
+                               next ones (same kernels, same outputs);
+                               0 (default): after the whole ReSlaveESD launch */
 } tops_pair_opts;
 
 int tops_pair_opts_default(tops_pair_opts *o);
@@ -153,6 +158,11 @@ typedef struct {
   double seconds;               /* wall time of the run: loading, processing and writing,
                                    overlapped across sub-swaths */
   double shifts[TOPS_MAX_BURSTS];   /* ESD shifts of the last sub-swath */
+  double load_seconds;          /* summed wall times of the sub-swath loads (reader thread) */
+  double process_seconds;       /* summed wall times of the sub-swath pair runs, staging
+                                   copies and device work included (main thread) */
+  double write_seconds;         /* summed wall times of the output writes (writer thread);
+                                   seconds < load + process + write shows the overlap */
 } tops_run_stats;
 
 int tops_run_config(const char *config_path, tops_run_stats *stats);

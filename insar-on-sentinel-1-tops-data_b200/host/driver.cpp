@@ -107,6 +107,7 @@ struct Product;
 // on the previous sub-swath.
 struct Loaded {
   int status = TOPS_OK;
+  double seconds = 0;   // wall time of the load
   PairInputs in;
   Scene scene;
   std::unique_ptr<Product> M, S;
@@ -317,7 +318,16 @@ int load_products(const tops_config &c, int nsub, Loaded &out) {
   return TOPS_OK;
 }
 
+std::unique_ptr<Loaded> load_subswath_untimed(const tops_config &c, int nsub, bool products);
+
 std::unique_ptr<Loaded> load_subswath(const tops_config &c, int nsub, bool products) {
+  const auto t0 = std::chrono::steady_clock::now();
+  std::unique_ptr<Loaded> L = load_subswath_untimed(c, nsub, products);
+  L->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return L;
+}
+
+std::unique_ptr<Loaded> load_subswath_untimed(const tops_config &c, int nsub, bool products) {
   std::unique_ptr<Loaded> L(new Loaded());
   L->status = products ? load_products(c, nsub, *L) : load_synthetic(c, nsub, *L);
   return L;
@@ -363,6 +373,7 @@ struct HostBuf {
 // One sub-swath's results, written by the writer thread.
 struct Outputs {
   HostBuf reslave, reslave_esd, coh, stitched;
+  double write_seconds = 0;   // wall time of write_outputs
   int k = 0, W = 0, L = 0, stitch_lines = 0, nsub = 0;
   std::vector<double> shifts;
 };
@@ -445,7 +456,16 @@ int process_pair(const tops_config &c, const PairInputs &in, HostBuf &stage_m, H
 
 // The writer stage: the reference's file names, <process_dir>/ReSlave-N.tif,
 // ReSlaveESD-N.tif, Coh-N.tif (Main.cpp:98-101) and CohStitch-N.tif.
-int write_outputs(const tops_config &c, const Outputs &o) {
+int write_outputs_untimed(const tops_config &c, const Outputs &o);
+
+int write_outputs(const tops_config &c, Outputs &o) {
+  const auto t0 = std::chrono::steady_clock::now();
+  const int r = write_outputs_untimed(c, o);
+  o.write_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return r;
+}
+
+int write_outputs_untimed(const tops_config &c, const Outputs &o) {
   const std::string dir = c.process_dir, tag = "-" + std::to_string(o.nsub) + ".tif";
   const int W = o.W, rows = o.k * o.L;
   D_TRY(tops_tiff_write((dir + "/ReSlave" + tag).c_str(), TOPS_TIFF_CFLOAT32, W, rows,
@@ -485,18 +505,24 @@ extern "C" int tops_run_config(const char *config_path, tops_run_stats *stats) {
   std::future<std::unique_ptr<Loaded>> next =
       std::async(std::launch::async, load_subswath, std::cref(c), c.firstsubswath, products);
   std::future<int> writing;
+  Outputs *pending = nullptr;   // the outputs `writing` writes
   int status = TOPS_OK;
   for (int nsub = c.firstsubswath; nsub <= c.lastsubswath && status == TOPS_OK; nsub++) {
     std::unique_ptr<Loaded> cur = next.get();
     if (nsub < c.lastsubswath)
       next = std::async(std::launch::async, load_subswath, std::cref(c), nsub + 1, products);
     status = cur->status;
+    stats->load_seconds += cur->seconds;
     if (status != TOPS_OK) break;
     // the slot written two sub-swaths ago is free once that write is done
     Outputs &o = outs[nsub & 1];
+    const auto tp = std::chrono::steady_clock::now();
     status = process_pair(c, cur->in, stage_m, stage_s, o);
+    stats->process_seconds +=
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - tp).count();
     if (writing.valid()) {
       const int w = writing.get();
+      stats->write_seconds += pending->write_seconds;
       if (status == TOPS_OK) status = w;
     }
     if (status != TOPS_OK) break;
@@ -504,10 +530,12 @@ extern "C" int tops_run_config(const char *config_path, tops_run_stats *stats) {
     stats->subswaths++;
     stats->burst_pairs += o.k;
     for (int i = 0; i + 1 < o.k && i < TOPS_MAX_BURSTS; i++) stats->shifts[i] = o.shifts[i];
-    writing = std::async(std::launch::async, write_outputs, std::cref(c), std::cref(o));
+    pending = &o;
+    writing = std::async(std::launch::async, write_outputs, std::cref(c), std::ref(o));
   }
   if (writing.valid()) {
     const int w = writing.get();
+    stats->write_seconds += pending->write_seconds;
     if (status == TOPS_OK) status = w;
   }
   if (next.valid()) next.wait();   // a load still running when an error ended the loop

@@ -59,6 +59,9 @@ struct tops_pair {
   // copy streams and per-burst events of the pipelined host-to-host run
   cudaStream_t s_up = nullptr, s_down = nullptr;
   std::vector<cudaEvent_t> pev;
+  // coherence stream and per-burst events of the overlapped ReSlaveESD tail
+  cudaStream_t s_coh = nullptr;
+  std::vector<cudaEvent_t> cev;
   std::vector<void *> allocs;
   int n_launches = 0;
   Arena *arena = nullptr;      // if set, device buffers come from it (no cudaMalloc)
@@ -82,7 +85,9 @@ struct tops_pair {
     if (capture_stream) cudaStreamDestroy(capture_stream);
     if (s_up) cudaStreamDestroy(s_up);
     if (s_down) cudaStreamDestroy(s_down);
+    if (s_coh) cudaStreamDestroy(s_coh);
     for (cudaEvent_t e : pev) cudaEventDestroy(e);
+    for (cudaEvent_t e : cev) cudaEventDestroy(e);
     for (void *p : allocs) {
       if (arena)
         arena->release(reinterpret_cast<uintptr_t>(p));

@@ -83,6 +83,7 @@ int tops_pair_opts_default(tops_pair_opts *o) {
   o->burst0_deramp_rows = 1;
   o->precision = TOPS_PREC_SPLIT;
   o->compensated = 0;
+  o->coh_overlap = 0;
   return TOPS_OK;
 }
 
@@ -464,6 +465,46 @@ void pair_coh_jobs(const tops_pair *P, std::vector<tops_coh_job> &cj) {
   }
 }
 
+// The ReSlaveESD resample burst by burst on `st`, and each burst's coherence
+// on a second stream as soon as the burst is resampled, so the coherence of
+// burst b (HBM-bound) overlaps the resample of burst b + 1 (issue-bound).
+// The kernels and their inputs are those of the one-launch form, so the
+// outputs are the same bit for bit.  The coherence stream has the highest
+// priority: its CTAs are dispatched ahead of the resample's pending ones.
+static int pair_tail_overlapped(tops_pair *P, const std::vector<tops_resample_job> &rs2,
+                                const std::vector<tops_coh_job> &cj, int skip,
+                                const tops::RowCopy &first, cudaStream_t st, int &launches) {
+  const int nb = P->nb;
+  if (!P->s_coh) {
+    int lo = 0, hi = 0;
+    P_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    P_CUDA(cudaStreamCreateWithPriority(&P->s_coh, cudaStreamNonBlocking, hi));
+  }
+  while ((int)P->cev.size() < nb + 1) {
+    cudaEvent_t e;
+    P_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    P->cev.push_back(e);
+  }
+  cudaStream_t cs = P->s_coh;
+  for (int b = 0; b < nb; b++) {
+    if (b == 0 && skip) {
+      tops::RowCopy c = first;
+      P_TRY(tops::row_copy(&c, 1, st, &launches));
+    } else {
+      P_TRY(tops_resample_ex(P->lut, &rs2[b], 1, P->o.precision, st));
+      launches += 1;
+    }
+    P_CUDA(cudaEventRecord(P->cev[b], st));
+    P_CUDA(cudaStreamWaitEvent(cs, P->cev[b], 0));
+    P_TRY(tops::coherence_launch(&cj[b], 1, P->o.win_rg, P->o.win_az, coh_cfg(P->o), cs));
+    launches += 1;
+  }
+  // `st` completes when the last coherence has
+  P_CUDA(cudaEventRecord(P->cev[nb], cs));
+  P_CUDA(cudaStreamWaitEvent(st, P->cev[nb], 0));
+  return TOPS_OK;
+}
+
 extern "C" {
 
 int tops_pair_run(tops_pair *P, void *stream) {
@@ -492,6 +533,17 @@ int tops_pair_run(tops_pair *P, void *stream) {
   //    uncorrected, Func.cpp:2653-2702)
   jobs.clear();
   pair_rs2_jobs(P, P->d_shift, jobs);
+  if (P->o.coh_overlap && nb > 1) {
+    // 4 + 5 overlapped: each burst's coherence as soon as it is resampled
+    tops::RowCopy c;
+    const int skip = pair_first_burst_copy(P, &c);
+    std::vector<tops_coh_job> cj;
+    pair_coh_jobs(P, cj);
+    P_TRY(pair_tail_overlapped(P, jobs, cj, skip, c, static_cast<cudaStream_t>(stream),
+                               launches));
+    P->n_launches = launches;
+    return TOPS_OK;
+  }
   {
     tops::RowCopy c;
     const int skip = pair_first_burst_copy(P, &c);

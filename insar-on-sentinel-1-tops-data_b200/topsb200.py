@@ -324,7 +324,8 @@ def swath_deramp_params(info: SwathInfo, orbit_coefs, ncoef: int):
 
 class RunStats(C.Structure):
     _fields_ = [("subswaths", C.c_int), ("burst_pairs", C.c_int), ("seconds", C.c_double),
-                ("shifts", C.c_double * MAX_BURSTS)]
+                ("shifts", C.c_double * MAX_BURSTS), ("load_seconds", C.c_double),
+                ("process_seconds", C.c_double), ("write_seconds", C.c_double)]
 
 
 _proto("tops_run_config", C.c_int, [C.c_char_p, C.POINTER(RunStats)])
@@ -543,7 +544,8 @@ def geocoreg_warp(dem_int, lat0, lon0, dlat, dlon, xmin, xmax, ymin, ymax, m_bur
 class PairOpts(C.Structure):
     _fields_ = [("win_rg", C.c_int), ("win_az", C.c_int), ("esd_threshold", C.c_float),
                 ("reslave_full", C.c_int), ("burst0_deramp_rows", C.c_int),
-                ("precision", C.c_int), ("compensated", C.c_int)]
+                ("precision", C.c_int), ("compensated", C.c_int),
+                ("coh_overlap", C.c_int)]
 
 
 class DemWindow(C.Structure):

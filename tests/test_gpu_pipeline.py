@@ -57,6 +57,19 @@ def test_pipeline_overlap_bands_only(T, scene_esd):
     assert np.array_equal(a["reslave_esd"][:L], a["reslave"][:L])
 
 
+@pytest.mark.parametrize("graph", [False, True])
+def test_coherence_overlap_equals_one_launch(T, scene_esd, graph):
+    """coh_overlap: each burst's coherence on a second stream right after
+    its ReSlaveESD resample gives the one-launch outputs bit for bit, eager
+    and captured in a CUDA graph."""
+    a = run_pair(T, scene_esd)
+    b = run_pair(T, scene_esd, graph=graph, coh_overlap=1)
+    for k in ("reslave", "reslave_esd", "coh", "cpm", "shifts"):
+        assert np.array_equal(a[k], b[k]), k
+    n = scene_esd.cfg.n_bursts
+    assert b["launches"] == a["launches"] + 2 * n - 3   # per-burst resample + coherence
+
+
 def test_plain_form_equals_pipeline(T, scene_esd):
     S = scene_esd
     dem_int = np.rint(S.dem).astype(np.int32)

@@ -37,6 +37,9 @@ def test_run_config_outputs_match_the_plan(T, tmp_path):
     out = tmp_path / "proc"
     st = T.run_config(_write_config(tmp_path / "config.txt", out))
     assert st.subswaths == 2 and st.burst_pairs == 4
+    # the stage times the run overlaps: each positive, none above the sum
+    assert min(st.load_seconds, st.process_seconds, st.write_seconds) > 0.0
+    assert st.seconds > 0.0
     for nsub in (1, 2):
         S = T.Scene(**{**SMALL, "seed": SMALL["seed"] + 1000 * (nsub - 1)})
         m, s = T.sub_swath(S.swath[0], 1, 2), T.sub_swath(S.swath[1], 1, 2)
