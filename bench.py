@@ -907,7 +907,7 @@ def stitch_report(T, P, S, torch, stream, steps):
 
 
 def overlap_report(T, torch, S, windows, stream, h_m, h_s, steps, warmup, dist, world, nb):
-    """The same graph step with tops_pair_opts.coh_overlap = 1: each burst's
+    """The same graph step with tops_pair_opts.coh_overlap = 1: each chunk's
     coherence on a second stream right after its ReSlaveESD resample."""
     import ctypes as C
     sp = stream.cuda_stream
@@ -935,8 +935,8 @@ def overlap_report(T, torch, S, windows, stream, h_m, h_s, steps, warmup, dist, 
     Q.close()
     return {"value": whole_job_value(world, nb, ms), "ms_per_step": ms,
             "launches_per_step": launches,
-            "form": "graph step, coherence of each burst on a second stream after its "
-                    "ReSlaveESD resample (same outputs bit for bit)"}
+            "form": "graph step, ReSlaveESD in up to 3 chunks of bursts, each chunk's coherence "
+                    "on a second stream after its resample (same outputs bit for bit)"}
 
 
 def stage_report(T, P, S, windows, sp, steps):

@@ -44,10 +44,11 @@ typedef struct {
                                coherence window sums without the sliding
                                update (pairwise per output); 0 (default): the
                                plain fixed-order FP32 sums */
-  int coh_overlap;          /* 1: the coherence of each ReSlaveESD burst runs
-                               on a second stream as soon as that burst is
-                               resampled, overlapping the resampling of the
-                               next ones (same kernels, same outputs);
+  int coh_overlap;          /* 1: the ReSlaveESD resample in up to 3 chunks of
+                               bursts, the coherence of each chunk on a second
+                               stream as soon as it is resampled, overlapping
+                               the resampling of the next chunk (same kernels,
+                               same outputs);
                                0 (default): after the whole ReSlaveESD launch */
 } tops_pair_opts;
 

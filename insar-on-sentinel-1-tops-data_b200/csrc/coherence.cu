@@ -298,13 +298,15 @@ constexpr int CT_WRG = 10;                 // range window of this variant
 constexpr int CT_DX = (CT_WRG - 1) / 2;    // 4
 constexpr int CT_XOFF = CT_DX;             // box start left of the strip
 constexpr int CT_TW = 240;                 // output columns per strip
-constexpr int CT_CPI = 4;                  // outputs per horizontal item
+constexpr int CT_CPI = 8;                  // outputs per horizontal item (= CO_CPI)
 constexpr int CT_SEG = 256;                // rows per work item
 constexpr int CT_MAXJOBS = 16;
 constexpr unsigned long long CT_WAIT_NS = 2000000000ull;   // a chunk is given up after 2 s
 static_assert(CT_XOFF % 4 == 0 && CT_XOFF == CT_DX, "box x coordinates stay 16-byte aligned");
 static_assert(CT_XOFF + CT_TW + CT_WRG - 1 - CT_DX <= CT_LW, "the strip's boxes cover its windows");
 static_assert(CT_TW % CT_CPI == 0 && CT_CH * (CT_TW / CT_CPI) <= CT_NT, "one horizontal item per thread");
+static_assert(CT_CPI == CO_CPI && CT_TW % CO_CPI == 0 && CO_TW % CO_CPI == 0,
+              "items start at the same columns as coherence_item's: same sums, same order");
 
 __host__ __device__ constexpr int pad4(int x) { return x + (x >> 2); }
 
@@ -465,7 +467,7 @@ __device__ __forceinline__ bool coh_tma_item(CtShared &S, const CtBatch &B, int 
     }
     __syncthreads();
     // horizontal box: CT_CPI consecutive outputs per item; an item starts at
-    // a multiple of 4 columns, so every padded offset below is a constant
+    // a multiple of 8 columns, so every padded offset below is a constant
     {
       constexpr int NG = CT_TW / CT_CPI;
       const int k = tid / NG;
@@ -501,7 +503,10 @@ __device__ __forceinline__ bool coh_tma_item(CtShared &S, const CtBatch &B, int 
         }
         float *orow = J.coh + (long)o * J.coh_pitch + c0 + cg;
         if (cg + CT_CPI <= cN && ((reinterpret_cast<uintptr_t>(orow) & 15) == 0)) {
-          *reinterpret_cast<float4 *>(orow) = make_float4(out[0], out[1], out[2], out[3]);
+#pragma unroll
+          for (int v = 0; v < CT_CPI; v += 4)
+            *reinterpret_cast<float4 *>(orow + v) =
+                make_float4(out[v], out[v + 1], out[v + 2], out[v + 3]);
         } else {
 #pragma unroll
           for (int uu = 0; uu < CT_CPI; uu++)

@@ -465,12 +465,14 @@ void pair_coh_jobs(const tops_pair *P, std::vector<tops_coh_job> &cj) {
   }
 }
 
-// The ReSlaveESD resample burst by burst on `st`, and each burst's coherence
-// on a second stream as soon as the burst is resampled, so the coherence of
-// burst b (HBM-bound) overlaps the resample of burst b + 1 (issue-bound).
-// The kernels and their inputs are those of the one-launch form, so the
-// outputs are the same bit for bit.  The coherence stream has the highest
-// priority: its CTAs are dispatched ahead of the resample's pending ones.
+// The ReSlaveESD resample in up to three chunks of bursts on `st`, and each
+// chunk's coherence on a second stream as soon as the chunk is resampled, so
+// the coherence of one chunk (L1- and HBM-bound) overlaps the resample of the
+// next (issue-bound).  Chunks rather than single bursts keep each launch
+// several waves long.  The kernels and their inputs are those of the
+// one-launch form, so the outputs are the same bit for bit.  The coherence
+// stream has the highest priority: its CTAs are dispatched ahead of the
+// resample's pending ones.
 static int pair_tail_overlapped(tops_pair *P, const std::vector<tops_resample_job> &rs2,
                                 const std::vector<tops_coh_job> &cj, int skip,
                                 const tops::RowCopy &first, cudaStream_t st, int &launches) {
@@ -486,22 +488,29 @@ static int pair_tail_overlapped(tops_pair *P, const std::vector<tops_resample_jo
     P->cev.push_back(e);
   }
   cudaStream_t cs = P->s_coh;
-  for (int b = 0; b < nb; b++) {
-    if (b == 0 && skip) {
+  const int per = (nb + 2) / 3;   // bursts per chunk
+  int e = 0;
+  for (int b0 = 0; b0 < nb; b0 += per) {
+    const int b1 = std::min(nb, b0 + per);
+    int r0 = b0;
+    if (b0 == 0 && skip) {
       tops::RowCopy c = first;
       P_TRY(tops::row_copy(&c, 1, st, &launches));
-    } else {
-      P_TRY(tops_resample_ex(P->lut, &rs2[b], 1, P->o.precision, st));
+      r0 = 1;
+    }
+    if (b1 > r0) {
+      P_TRY(tops_resample_ex(P->lut, &rs2[r0], b1 - r0, P->o.precision, st));
       launches += 1;
     }
-    P_CUDA(cudaEventRecord(P->cev[b], st));
-    P_CUDA(cudaStreamWaitEvent(cs, P->cev[b], 0));
-    P_TRY(tops::coherence_launch(&cj[b], 1, P->o.win_rg, P->o.win_az, coh_cfg(P->o), cs));
+    P_CUDA(cudaEventRecord(P->cev[e], st));
+    P_CUDA(cudaStreamWaitEvent(cs, P->cev[e], 0));
+    e++;
+    P_TRY(tops::coherence_launch(&cj[b0], b1 - b0, P->o.win_rg, P->o.win_az, coh_cfg(P->o), cs));
     launches += 1;
   }
   // `st` completes when the last coherence has
-  P_CUDA(cudaEventRecord(P->cev[nb], cs));
-  P_CUDA(cudaStreamWaitEvent(st, P->cev[nb], 0));
+  P_CUDA(cudaEventRecord(P->cev[e], cs));
+  P_CUDA(cudaStreamWaitEvent(st, P->cev[e], 0));
   return TOPS_OK;
 }
 

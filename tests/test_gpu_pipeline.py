@@ -59,15 +59,20 @@ def test_pipeline_overlap_bands_only(T, scene_esd):
 
 @pytest.mark.parametrize("graph", [False, True])
 def test_coherence_overlap_equals_one_launch(T, scene_esd, graph):
-    """coh_overlap: each burst's coherence on a second stream right after
-    its ReSlaveESD resample gives the one-launch outputs bit for bit, eager
-    and captured in a CUDA graph."""
+    """coh_overlap: each chunk's coherence on a second stream right after its
+    ReSlaveESD resample gives the one-launch outputs bit for bit, eager and
+    captured in a CUDA graph."""
     a = run_pair(T, scene_esd)
     b = run_pair(T, scene_esd, graph=graph, coh_overlap=1)
     for k in ("reslave", "reslave_esd", "coh", "cpm", "shifts"):
         assert np.array_equal(a[k], b[k]), k
+    # up to 3 chunks of bursts, each a resample launch (none for a chunk that
+    # holds only the copied first burst) and a coherence launch
     n = scene_esd.cfg.n_bursts
-    assert b["launches"] == a["launches"] + 2 * n - 3   # per-burst resample + coherence
+    per = (n + 2) // 3
+    chunks = -(-n // per)
+    extra = (chunks - (1 if per == 1 else 0)) + chunks - 2
+    assert b["launches"] == a["launches"] + extra
 
 
 def test_plain_form_equals_pipeline(T, scene_esd):
