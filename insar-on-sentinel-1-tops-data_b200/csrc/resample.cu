@@ -99,7 +99,7 @@ static_assert(RS_DT <= RS_NT && RS_GR == 12 && RS_HR * 2 == RS_GR,
               "thread mappings assume these sizes");
 
 enum : int { REG_OUT = 0, REG_EDGE = 1, REG_IN = 2 };
-enum : int { RM_PIXEL = 0, RM_SHARED = 1 };
+enum : int { RM_PIXEL = 0, RM_SHARED = 1, RM_TWO = 2 };
 
 using RsLut = LutPtrs;
 
@@ -117,6 +117,8 @@ struct __align__(16) RsRow {
   int L0;                    // azimuth line of the shared azimuth pass
   int bin;                   // its LUT bin | bin-table slot << 16
   int mode;                  // RM_SHARED: the row takes the shared azimuth pass;
+                             // RM_TWO | lo << 8 | hi << 16: the same, but columns
+                             // [lo, hi) have the next LUT bin of the same line;
                              // RM_PIXEL: its pixels take the per-pixel path
 };
 
@@ -146,6 +148,7 @@ struct __align__(16) RsShared {
   int4 gwin[RS_NGRP];                 // per group: window on, filled at its start, line of row 0,
                                       // rows without a shared azimuth pass (bit mask)
   int2 grange[RS_NGRP];               // per group: lines its window pushes need
+  RsRow r2[RS_GR];                    // row terms of the second bin of the group's two-bin rows
   int gen_n[RS_NGRP];                 // per group: pixels deferred to the per-pixel pass
   int gen_d[RS_NGRP];                 // per group: pixels of columns without a run table
   unsigned short gen[RS_GR * RS_TW];  // their (row in group) * 128 + column: the first
@@ -563,6 +566,55 @@ __device__ __forceinline__ float2 pixel_keyed(const RsShared &S, const ResampleJ
   return pixel_generic(S, J, r, c);
 }
 
+// Azimuth sum of this thread's ring column for the key (L0, bin) over
+// lines deramped anew (staged lines in [win_lo, win_hi] from shared memory,
+// others from HBM), in the order of the register-window sum.
+template <bool kSplit>
+__device__ __forceinline__ float2 az_direct(const RsShared &S, const ResampleJob &J,
+                                            const RsLut &lut, int x, int xa, bool xin, int L0,
+                                            int bin, int win_lo, int win_hi, float g2c,
+                                            float g1c, float g0c, const DerampQuad &cq) {
+  const float *kl = lut.kaz + bin * kTaps;
+  float2 a = make_float2(0.f, 0.f), b = a;
+#pragma unroll 1
+  for (int j = 0; j < RS_GR; j += 2) {
+    const float wa = __ldg(kl + j), wb = __ldg(kl + j + 1);
+    const float2 d0 =
+        deramp_at<kSplit>(S, J, x, xa, xin, L0 - 5 + j, win_lo, win_hi, g2c, g1c, g0c, cq);
+    const float2 d1 =
+        deramp_at<kSplit>(S, J, x, xa, xin, L0 - 4 + j, win_lo, win_hi, g2c, g1c, g0c, cq);
+    a = __ffma2_rn(make_float2(wa, wa), d0, a);
+    b = __ffma2_rn(make_float2(wb, wb), d1, b);
+  }
+  return __fadd2_rn(a, b);
+}
+
+// Reramp row terms of the azimuth key (L0, bin): Psi = sum_j kAz[j]
+// phi_ref(L0 - 5 + j) (FP64) and the taps' moments about the burst centre
+// time.
+__device__ __forceinline__ void row_terms(const RsShared &S, const ResampleJob &J,
+                                          const RsLut &lut, int L0, int bin, RsRow &R) {
+  const DerampQuad refq = {S.ref_a0, S.ref_a1, S.ref_a2};
+  const float *kl = lut.kaz + bin * kTaps;
+  double psi = 0.0, m0 = 0.0, m1 = 0.0, m2 = 0.0;
+#pragma unroll 4
+  for (int j = 0; j < kTaps; j++) {
+    const double w = (double)__ldg(kl + j), u = (double)(j - 5);
+    const double ta = (double)(L0 - 5 + j - J.s_first_line) * J.dt;
+    psi = fma(w, quad_eval(refq, ta), psi);
+    m0 += w;
+    m1 = fma(w, u, m1);
+    m2 = fma(w, u * u, m2);
+  }
+  const double tc0 = (double)(L0 - J.s_first_line) * J.dt - S.tm;
+  const double dt = J.dt;
+  R.rho = reduce_2pi(psi);
+  R.psif = (float)psi;
+  R.R2 = (float)(m0 * tc0 * tc0 + 2.0 * tc0 * dt * m1 + dt * dt * m2);
+  R.R1 = (float)(m0 * tc0 + dt * m1);
+  R.R0 = (float)m0;
+}
+
 // One work item (strip x segment of one job); all threads of the CTA call it
 // with the same item.
 template <bool kSplit>
@@ -664,7 +716,10 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
   S.ring_gc[x] = make_float4(g2c, g1c, g0c, 0.f);
 
   // ---- [P4] per-row statistics: one shared azimuth pass where the whole
-  // strip maps to one (line, bin) key inside the slave box's interior
+  // strip maps to one (line, bin) key inside the slave box's interior; where
+  // it maps to two adjacent bins of one line and the position is monotone
+  // along the strip, the columns of the second bin are found by bisection of
+  // the exact per-pixel key
   for (int ri = tid; ri < nr; ri += RS_NT) {
     const double L = row_L(J, r_begin + ri);
     const double Aaz = row_a(S.caz, L) + S.shift, Baz = row_b(S.caz, L);
@@ -673,34 +728,41 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
     int l0lo, blo, l0hi, bhi;
     split_pos(ylo, l0lo, blo);
     split_pos(yhi, l0hi, bhi);
-    const bool fast = (l0lo == l0hi) && (blo == bhi) && l0lo >= J.sy0 + 5 && l0hi <= J.sy1 - 7;
+    const bool inter = l0lo >= J.sy0 + 5 && l0hi <= J.sy1 - 7;
+    const bool fast = (l0lo == l0hi) && (blo == bhi) && inter;
+    int mode = fast ? RM_SHARED : RM_PIXEL;
+    if (!fast && inter && l0lo == l0hi && bhi == blo + 1) {
+      const double c2 = 2.0 * S.caz[5];
+      const double s0 = fma(c2, S.col_phat[0], Baz), s1 = fma(c2, S.col_phat[cN - 1], Baz);
+      if ((s0 < 0.0) == (s1 < 0.0)) {
+        auto is_hi = [&](int c) {
+          int l, b;
+          split_pos(pix_pos(Aaz, Baz, S.col_phat[c], S.col_qaz[c]), l, b);
+          return b == bhi;
+        };
+        const bool f0 = is_hi(0);
+        int t = cN;   // first column whose bin differs from column 0's
+        if (is_hi(cN - 1) != f0) {
+          int lo = 0, hi = cN - 1;
+          while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (is_hi(mid) == f0)
+              lo = mid;
+            else
+              hi = mid;
+          }
+          t = hi;
+        }
+        const int c_lo = f0 ? 0 : t, c_hi = f0 ? t : cN;
+        mode = RM_TWO | (c_lo << 8) | (c_hi << 16);
+      }
+    }
     RsRow R;
     R.L0 = l0lo;
     R.bin = blo | (RS_NOSLOT << 16);
-    R.mode = fast ? 1 : 0;
     R.rho = R.psif = R.R2 = R.R1 = R.R0 = 0.f;
-    if (fast) {
-      // Psi = sum_j kAz[j] phi_ref(L0 - 5 + j) (FP64) and the taps' moments
-      const DerampQuad refq = {S.ref_a0, S.ref_a1, S.ref_a2};
-      const float *kl = lut.kaz + blo * kTaps;
-      double psi = 0.0, m0 = 0.0, m1 = 0.0, m2 = 0.0;
-#pragma unroll 4
-      for (int j = 0; j < kTaps; j++) {
-        const double w = (double)__ldg(kl + j), u = (double)(j - 5);
-        const double ta = (double)(l0lo - 5 + j - J.s_first_line) * J.dt;
-        psi = fma(w, quad_eval(refq, ta), psi);
-        m0 += w;
-        m1 = fma(w, u, m1);
-        m2 = fma(w, u * u, m2);
-      }
-      const double tc0 = (double)(l0lo - J.s_first_line) * J.dt - tm;
-      const double dt = J.dt;
-      R.rho = reduce_2pi(psi);
-      R.psif = (float)psi;
-      R.R2 = (float)(m0 * tc0 * tc0 + 2.0 * tc0 * dt * m1 + dt * dt * m2);
-      R.R1 = (float)(m0 * tc0 + dt * m1);
-      R.R0 = (float)m0;
-    }
+    if (mode != RM_PIXEL) row_terms(S, J, lut, l0lo, blo, R);
+    R.mode = mode;
     S.rows[ri] = R;
   }
   __syncthreads();
@@ -780,14 +842,17 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
       if (gw.x) ymin = gw.z - (gw.y ? 5 : -6);
       // rows without a shared pass (bits 0..11) and shared rows whose line
       // is not the window's, summed directly (bits 16..27)
-      int mask = 0;
+      int mask = 0, two = 0;
       for (int k = 0; k < gr; k++) {
         const int ri = tid * RS_GR + k;
         if (!shared_row(ri))
           mask |= 1 << k;
         else if (!gw.x || S.rows[ri].L0 != gw.z + k)
           mask |= 1 << (16 + k);
+        if (shared_row(ri) && (S.rows[ri].mode & 0xff) == RM_TWO) two |= 1 << k;
       }
+      // rows with a second bin (bits 4..15 of the flags)
+      S.gwin[tid].y = gw.y | (two << 4);
       S.grange[tid] = gw.x ? make_int2(gw.y ? gw.z - 5 : gw.z + 6, gw.z + gr - 1 + 6)
                            : make_int2(1, 0);
       S.gwin[tid].w = mask;
@@ -814,7 +879,6 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
       const int b = R.bin & 0xffff;
       const int slot = incl - 1 < RS_MAXBIN ? incl - 1 : RS_NOSLOT;
       R.bin = b | (slot << 16);
-      R.mode = RM_SHARED;
       if (f && slot < RS_MAXBIN) S.bin_id[slot] = b;
     };
     set_row(r0, h0, incl0, f0);
@@ -980,7 +1044,7 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
     const int gr = min(RS_GR, nr - rg0);
     const int4 plan = S.gplan[g];
     const int4 gw = S.gwin[g];
-    const int pixmask = gw.w & 0xfff;     // rows without a shared pass
+    const int pixmask = gw.w & 0xfff;     // rows without a shared pass ([A] only)
     const int dirmask = gw.w >> 16;       // shared rows off the window's line
     cp_async_wait_all();                  // this thread's staged lines of the group
     // ---- [A] azimuth pass of the group's rows (the taps are loaded anew per
@@ -1052,19 +1116,8 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
       for (int m = dirmask; m; m &= m - 1) {
         const int k = __ffs(m) - 1;
         const RsRow &R = S.rows[rg0 + k];
-        const float *kl = lut.kaz + (R.bin & 0xffff) * kTaps;
-        float2 a = make_float2(0.f, 0.f), b = a;
-#pragma unroll 1
-        for (int j = 0; j < RS_GR; j += 2) {
-          const float wa = __ldg(kl + j), wb = __ldg(kl + j + 1);
-          const float2 d0 = deramp_at<kSplit>(S, J, x, xa, xin, R.L0 - 5 + j, plan.z, plan.w,
-                                              g2c, g1c, g0c, cq);
-          const float2 d1 = deramp_at<kSplit>(S, J, x, xa, xin, R.L0 - 4 + j, plan.z, plan.w,
-                                              g2c, g1c, g0c, cq);
-          a = __ffma2_rn(make_float2(wa, wa), d0, a);
-          b = __ffma2_rn(make_float2(wb, wb), d1, b);
-        }
-        S.vd[k][x] = __fadd2_rn(a, b);
+        S.vd[k][x] = az_direct<kSplit>(S, J, lut, x, xa, xin, R.L0, R.bin & 0xffff, plan.z,
+                                       plan.w, g2c, g1c, g0c, cq);
       }
     }
     // stage the next group's new lines; they land while [B] runs
@@ -1076,6 +1129,9 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
 
     // ---- [B] range pass, reramp, store: 2 columns x 6 rows per thread;
     // pixels the shared passes do not cover are listed for [C]
+    // rows without a shared pass and two-bin rows (read again here, so the
+    // group's flags hold no registers during [B])
+    const int bskip = (S.gwin[g].w & 0xfff) | ((S.gwin[g].y >> 4) & 0xfff);
     if (dval0) {
       run_weights(cr0, J);
       run_weights(cr1, J);
@@ -1083,7 +1139,7 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
       for (int kk = 0; kk < RS_HR; kk++) {
         const int k = dh * RS_HR + kk;
         if (k >= gr) break;
-        if ((pixmask >> k) & 1) continue;   // the whole row is done in [C]
+        if ((bskip >> k) & 1) continue;     // the whole row is done in [C2] or [C]
         const int ri = rg0 + k;
         if (ri >= cr0.next) {
           while (ri >= cr0.next) run_load(cr0, S, J, dc, cr0.m + 1);
@@ -1167,9 +1223,57 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
       }
     }
 
+    // ---- [C2] two-bin rows, all threads, by the keyed path: the columns of
+    // the first bin from the tile; then the rows' azimuth sums with the
+    // second bin, over lines deramped anew from HBM (the line ring already
+    // holds the next group's lines), into their tile rows, and the row terms
+    // of that key; then the columns of the second bin
+    {
+      const int two = (S.gwin[g].y >> 4) & 0xfff;
+      if (two) {
+#pragma unroll 1
+        for (int m = two; m; m &= m - 1) {
+          const int k = __ffs(m) - 1;
+          const int md = S.rows[rg0 + k].mode;
+          const int lo = (md >> 8) & 0xff, hi = (md >> 16) & 0xff;
+          const int r = r_begin + rg0 + k;
+          for (int c = tid; c < cN; c += RS_NT)
+            if (c < lo || c >= hi)
+              J.out[(long)(r - J.row0) * J.out_pitch + c0 + c] =
+                  pixel_keyed(S, J, S.rows[rg0 + k], &S.vd[k][0], r, c);
+        }
+        __syncthreads();
+#pragma unroll 1
+        for (int m = two; m; m &= m - 1) {
+          const int k = __ffs(m) - 1;
+          const RsRow &R = S.rows[rg0 + k];
+          S.vd[k][x] = az_direct<kSplit>(S, J, lut, x, xa, xin, R.L0, (R.bin & 0xffff) + 1, 1,
+                                         0, g2c, g1c, g0c, cq);
+        }
+        if (tid < RS_GR && ((two >> tid) & 1)) {
+          const RsRow &R = S.rows[rg0 + tid];
+          RsRow R2 = R;
+          row_terms(S, J, lut, R.L0, (R.bin & 0xffff) + 1, R2);
+          S.r2[tid] = R2;
+        }
+        __syncthreads();
+#pragma unroll 1
+        for (int m = two; m; m &= m - 1) {
+          const int k = __ffs(m) - 1;
+          const int md = S.rows[rg0 + k].mode;
+          const int r = r_begin + rg0 + k;
+          for (int c = ((md >> 8) & 0xff) + tid; c < ((md >> 16) & 0xff); c += RS_NT)
+            J.out[(long)(r - J.row0) * J.out_pitch + c0 + c] =
+                pixel_keyed(S, J, S.r2[k], &S.vd[k][0], r, c);
+        }
+        __syncthreads();
+      }
+    }
+
     // ---- [C] per-pixel path, all threads: the rows without a shared pass,
     // then the listed pixels
     {
+      const int pixmask = S.gwin[g].w & 0xfff;
       const int npr = __popc(pixmask);
       const int nrow_units = npr * cN;
       const int total = nrow_units + S.gen_n[g];

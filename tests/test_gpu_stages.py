@@ -153,6 +153,45 @@ def test_resample_precision_modes(T, O, scene_small, prec):
         assert err < 1e-5, err
 
 
+def _two_bin_share(cpm_az, mbox, shift, strip=112):
+    """Share of (row, 112-column strip) pieces whose azimuth keys are two
+    adjacent LUT bins of one line."""
+    from chain import positions
+    y = positions(np.asarray(cpm_az), mbox, shift)
+    line = np.trunc(y)
+    b = np.clip(np.trunc((y - line) * 2047.0 + 0.5), 0, 2047)
+    n = two = 0
+    for c in range(0, y.shape[1], strip):
+        bb, ll = b[:, c:c + strip], line[:, c:c + strip]
+        one_line = ll.min(1) == ll.max(1)
+        two += int(np.sum(one_line & (bb.max(1) - bb.min(1) == 1)))
+        n += y.shape[0]
+    return two / n
+
+
+@pytest.mark.parametrize("prec", ["split", "fp64"])
+def test_resample_two_bin_rows(T, O, scene_small, prec):
+    """Rows whose strip spans two adjacent azimuth bins (here most rows: an
+    azimuth offset that changes by ~1/3 of a bin per strip) take the shared
+    pass with the second bin summed after the range pass: against the FP64
+    oracle, and a row subset bit for bit as the whole job."""
+    S = scene_small
+    az, rg = oracle_cpm(O, S, 1)
+    az = np.array(az, np.float64)
+    az[2] += 3e-3 * S.cfg.samples_per_burst / 4096.0
+    kw = rs_inputs(S, 1, (az, rg), 0.0123)
+    assert _two_bin_share(az, kw["mbox"], 0.0123) > 0.3
+    mode = T.PREC_SPLIT if prec == "split" else T.PREC_FP64
+    gpu = _resample_device(T, kw, mode)
+    ref, _ = O.resample(**kw)
+    err = rel_rms(gpu, ref)
+    assert err < RS_TOL, err
+    for r0, n in ((123, 54), (7, 1), (250, 13)):
+        part = _resample_device(T, kw, mode, rows=(r0, n))
+        bad = np.argwhere(part != gpu[r0:r0 + n])
+        assert bad.size == 0, (r0, n, bad[:8].tolist(), bad.shape[0])
+
+
 def test_resample_unaligned_buffers(T, O, scene_small):
     """Misaligned slave / output bases take the scalar-access paths."""
     S = scene_small
