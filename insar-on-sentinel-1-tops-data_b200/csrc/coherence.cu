@@ -288,8 +288,10 @@ __global__ void __launch_bounds__(CO_NT, 3) coherence_kernel(const __grid_consta
 // starts CT_XOFF = dx columns left of the strip, a multiple of 4, so every
 // box's x coordinate is 16-byte aligned in both images; the copy engine
 // fills rows and columns outside the image with zeros -- the zero pad.  The
-// sums are those of coherence_item, in the same order, so the two kernels
-// agree bit for bit.
+// vertical sums are those of coherence_item; the horizontal sliding sum
+// restarts every CT_CPI = 4 outputs instead of every CO_CPI = 8 (measured
+// faster: 0.398 against 0.490 ms for 3 bursts of 1500 x 21000), so the two
+// kernels agree to FP32 rounding of the window sums (a few 1e-7).
 constexpr int CT_NT = 256;
 constexpr int CT_LW = 256;                 // loaded columns (box width)
 constexpr int CT_CH = 4;                   // rows per chunk (box height)
@@ -298,15 +300,13 @@ constexpr int CT_WRG = 10;                 // range window of this variant
 constexpr int CT_DX = (CT_WRG - 1) / 2;    // 4
 constexpr int CT_XOFF = CT_DX;             // box start left of the strip
 constexpr int CT_TW = 240;                 // output columns per strip
-constexpr int CT_CPI = 8;                  // outputs per horizontal item (= CO_CPI)
+constexpr int CT_CPI = 4;                  // outputs per horizontal item
 constexpr int CT_SEG = 256;                // rows per work item
 constexpr int CT_MAXJOBS = 16;
 constexpr unsigned long long CT_WAIT_NS = 2000000000ull;   // a chunk is given up after 2 s
 static_assert(CT_XOFF % 4 == 0 && CT_XOFF == CT_DX, "box x coordinates stay 16-byte aligned");
 static_assert(CT_XOFF + CT_TW + CT_WRG - 1 - CT_DX <= CT_LW, "the strip's boxes cover its windows");
 static_assert(CT_TW % CT_CPI == 0 && CT_CH * (CT_TW / CT_CPI) <= CT_NT, "one horizontal item per thread");
-static_assert(CT_CPI == CO_CPI && CT_TW % CO_CPI == 0 && CO_TW % CO_CPI == 0,
-              "items start at the same columns as coherence_item's: same sums, same order");
 
 __host__ __device__ constexpr int pad4(int x) { return x + (x >> 2); }
 
@@ -467,7 +467,7 @@ __device__ __forceinline__ bool coh_tma_item(CtShared &S, const CtBatch &B, int 
     }
     __syncthreads();
     // horizontal box: CT_CPI consecutive outputs per item; an item starts at
-    // a multiple of 8 columns, so every padded offset below is a constant
+    // a multiple of 4 columns, so every padded offset below is a constant
     {
       constexpr int NG = CT_TW / CT_CPI;
       const int k = tid / NG;

@@ -244,8 +244,10 @@ def test_coherence_slave_equals_master(T, O, scene_small):
 @pytest.mark.parametrize("win_az", [3, 6])
 def test_coherence_tma_equals_generic(T, scene_small, win_az):
     """The TMA-staged coherence kernel (10-sample range window, 16-byte
-    aligned rows) gives the generic kernel's outputs bit for bit: the slave
-    placed 8 bytes off a 16-byte boundary takes the generic kernel."""
+    aligned rows) against the generic kernel (the slave placed 8 bytes off a
+    16-byte boundary takes it): the same vertical sums, the horizontal
+    sliding sum restarted every 4 instead of every 8 outputs, so the two
+    agree to FP32 rounding of the window sums."""
     import ctypes as C
     import torch
     S = scene_small
@@ -267,7 +269,7 @@ def test_coherence_tma_equals_generic(T, scene_small, win_az):
         T.check(T.lib.tops_coherence(C.byref(job), 1, 10, win_az, None), "tops_coherence")
         torch.cuda.synchronize()
         out.append(coh.cpu().numpy())
-    assert np.array_equal(out[0], out[1])
+    assert np.abs(out[0] - out[1]).max() < 2e-6
     assert np.all(np.isfinite(out[0])) and out[0].min() >= 0.0 and out[0].max() <= 1.0 + 1e-6
 
 
