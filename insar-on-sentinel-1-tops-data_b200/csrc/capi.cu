@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "device_slots.h"
 #include "launch.h"
 
 namespace tops {
@@ -69,15 +70,15 @@ struct Workspace {
     return TOPS_OK;
   }
 };
-static thread_local Workspace g_ws_dev[kMaxDevices];
+static thread_local DeviceSlots<Workspace, kMaxDevices> g_ws;
 
 // The workspace of the calling thread on its current device.
 static int workspace(Workspace **out) {
   int dev = -1;
   TOPS_CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kMaxDevices) return TOPS_E_INVALID;
-  g_ws_dev[dev].dev = dev;
-  *out = &g_ws_dev[dev];
+  Workspace *w = g_ws.at(dev);
+  if (!w) return TOPS_E_INVALID;
+  *out = w;
   return TOPS_OK;
 }
 
@@ -101,7 +102,7 @@ struct LutScratch {
     if (have_cur) cudaSetDevice(cur);
   }
 };
-static thread_local LutScratch g_lut_dev[kMaxDevices];
+static thread_local DeviceSlots<LutScratch, kMaxDevices> g_lut;
 
 // The reference passes its host LUT on every call; keep one device copy per
 // (thread, device) and refresh it when the caller's table changes.
@@ -109,9 +110,9 @@ static int lut_for(const float *kaz, const float *krg, int npoints, tops_lut_dev
   if (npoints != kTaps) return TOPS_E_INVALID;
   int dev = -1;
   TOPS_CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kMaxDevices) return TOPS_E_INVALID;
-  LutScratch &g = g_lut_dev[dev];
-  g.dev = dev;
+  LutScratch *gp = g_lut.at(dev);
+  if (!gp) return TOPS_E_INVALID;
+  LutScratch &g = *gp;
   const size_t n = (size_t)kLutBins * kTaps;
   if (!g.lut || memcmp(g.kaz.data(), kaz, n * sizeof(float)) ||
       memcmp(g.krg.data(), krg, n * sizeof(float))) {

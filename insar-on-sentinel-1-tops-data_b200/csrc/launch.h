@@ -2,8 +2,9 @@
 // kernels, used by the batched plans (host/pipeline.cpp): the work-item tile
 // (rows per item) and the scheduling mode.
 //
-//   seg_rows  output rows per work item (0: the kernel's default); the
-//             resample kernel takes 12..252, the coherence kernel 8..512
+//   seg_rows  output rows per work item; the resample kernel takes 12..252
+//             (0: the longest of 252, 168, 120, 84 that gives two waves of
+//             items), the coherence kernel 8..512 (0: its default)
 //   counters  if non-null: persistent launch.  `grid` CTAs (0: as many as
 //             fit on the device at once) pull work items from a queue -- the
 //             device int counters[k], set to 0 on the stream before the k-th

@@ -1472,6 +1472,20 @@ static int launch_resample_t(const ResampleJob *jobs, int njobs, const TileCfg &
   if (s0 != TOPS_OK) return s0;
   if (cfg.seg_rows < 0 || cfg.seg_rows > RS_MAXSEG || (cfg.seg_rows && cfg.seg_rows < RS_GR))
     return TOPS_E_INVALID;
+  // default segment rows: the longest (least prologue per output row) that
+  // still gives every SM two waves of items; small launches (a narrow burst,
+  // a single burst) take shorter segments.  Outputs do not depend on it.
+  int seg_rows = cfg.seg_rows;
+  if (!seg_rows) {
+    static const int kSegs[] = {RS_SEG, 168, 120, 84};
+    for (int sr : kSegs) {
+      long items = 0;
+      for (int j = 0; j < njobs; j++)
+        items += (long)jobs[j].strips * ((jobs[j].nrows + sr - 1) / sr);
+      seg_rows = sr;
+      if (items >= 2L * resident) break;
+    }
+  }
   for (int j0 = 0, k = 0; j0 < njobs; j0 += RS_MAXJOBS, k++) {
     RsBatch B;
     B.njobs = 0;
@@ -1480,10 +1494,8 @@ static int launch_resample_t(const ResampleJob *jobs, int njobs, const TileCfg &
     for (int j = j0; j < njobs && j < j0 + RS_MAXJOBS; j++) {
       ResampleJob &J = B.jobs[B.njobs];
       J = jobs[j];
-      if (cfg.seg_rows) {
-        J.seg_rows = cfg.seg_rows;
-        J.segs = (J.nrows + cfg.seg_rows - 1) / cfg.seg_rows;
-      }
+      J.seg_rows = seg_rows;
+      J.segs = (J.nrows + seg_rows - 1) / seg_rows;
       J.item_begin = items;
       items += J.strips * J.segs;
       B.njobs++;

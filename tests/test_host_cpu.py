@@ -7,7 +7,7 @@ import re
 import numpy as np
 import pytest
 
-from conftest import ROOT, c64, rel_rms
+from conftest import PKG, ROOT, c64, rel_rms
 
 
 # ------------------------------------------------------------ C ABI exports
@@ -224,3 +224,36 @@ def test_synth_invalid_config(T):
         T.Scene(n_bursts=0)
     with pytest.raises(T.TopsError):
         T.Scene(overlap_lines=2000)
+
+
+def test_device_slots_keep_devices_apart(tmp_path):
+    """The reference-compatible wrappers' per-thread caches (workspace, LUT
+    copy) hold one slot per device index, tagged with its device
+    (csrc/device_slots.h): a call after a device change gets another slot,
+    never the buffers of the previous device; indexes outside the table are
+    refused."""
+    import subprocess
+    src = tmp_path / "slots.cpp"
+    src.write_text(r"""
+#include "device_slots.h"
+#include <cstdio>
+struct Cache { int dev = -1; int buffers = 0; };
+int main() {
+  static tops::DeviceSlots<Cache, 8> c;
+  Cache *a = c.at(0);
+  a->buffers = 7;                      // allocated on device 0
+  Cache *b = c.at(1);                  // the thread switched to device 1
+  if (b == a || b->dev != 1 || b->buffers != 0) return 1;
+  if (c.at(0) != a || a->dev != 0 || a->buffers != 7) return 2;
+  if (c.at(-1) || c.at(8)) return 3;
+  std::puts("ok");
+  return 0;
+}
+""")
+    exe = tmp_path / "slots"
+    inc = os.path.join(PKG, "csrc")
+    r = subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", "-I" + inc, str(src), "-o",
+                        str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", (r.returncode, r.stdout)
