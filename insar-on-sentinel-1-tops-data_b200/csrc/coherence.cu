@@ -330,16 +330,6 @@ struct __align__(128) CtShared {
 
 __device__ int g_coh_wait_faults;       // chunks whose wait ran out (0 normally)
 
-// Loaded column of each lane in the vertical pass, a permutation of the
-// warp's 32 columns: every 8 consecutive lanes store their 16-byte vertical
-// sums V[k][pad4(col)] to 8 different 16-byte bank groups, and every 16
-// consecutive lanes load their 8-byte slave samples from 16 different 8-byte
-// bank pairs (col mod 16 distinct), so neither access has bank conflicts;
-// the 4-byte master loads stay within one 128-byte row.
-__constant__ int c_coh_lane_col[32] = {0,  20, 2,  22, 23, 17, 24, 19, 26, 27, 21,
-                                       28, 29, 30, 31, 25, 7,  1,  8,  3,  16, 4,
-                                       18, 6,  13, 14, 15, 9,  10, 11, 5,  12};
-
 __device__ __forceinline__ unsigned ct_smem(const void *p) {
   return static_cast<unsigned>(__cvta_generic_to_shared(p));
 }
@@ -424,7 +414,7 @@ __device__ __forceinline__ bool coh_tma_item(CtShared &S, const CtBatch &B, int 
   float4 q[NQ > 0 ? NQ : 1];
 #pragma unroll
   for (int j = 0; j < NQ; j++) q[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-  const int t = (tid & ~31) + c_coh_lane_col[tid & 31];   // loaded column
+  const int t = tid;                       // loaded column
   bool ok = true;
   for (int u = 0; u < T; u++) {
     const unsigned slot = (seq + u) % CT_NST;
