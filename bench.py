@@ -752,6 +752,13 @@ def main():
 
     e2e_ms = timed(process, args.e2e_steps)
     serial_ms = timed(serial, max(1, args.e2e_steps // 2))
+    # the same call without the ReSlave download (the reference writes ReSlave
+    # only as an intermediate raster): ReSlaveESD, coherence, offsets, shifts
+    process_no_rs = lambda: T.check(T.lib.tops_pair_process(
+        P._h, C.c_void_p(h_m.data_ptr()), C.c_void_p(h_s.data_ptr()), None,
+        C.c_void_p(h_re.data_ptr()), C.cast(C.c_void_p(h_coh.data_ptr()), C.POINTER(C.c_float)),
+        T.ptr(h_cpm, C.c_double), T.ptr(h_sh, C.c_double), C.c_void_p(sp)), "process")
+    no_rs_ms = timed(process_no_rs, max(1, args.e2e_steps // 2))
     e2e_step_ms = float(np.mean(e2e_ms))
     e2e_value = whole_job_value(world, nb, max_over_ranks(e2e_step_ms, dist, world, "cuda"))
     h2d = 2 * n * W * 4
@@ -800,6 +807,11 @@ def main():
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_step_ms,
                 "form": "tops_pair_process (per-burst copy/compute pipeline)",
                 "serial_ms_per_step": float(np.mean(serial_ms)),
+                "without_reslave_download": {
+                    "value": whole_job_value(world, nb, max_over_ranks(float(np.mean(no_rs_ms)),
+                                                                       dist, world, "cuda")),
+                    "ms_per_step": float(np.mean(no_rs_ms)),
+                    "d2h_bytes_per_step": d2h - n * W * 8},
                 "latency_ms": {"p50": float(np.percentile(e2e_ms, 50)),
                                "p99": float(np.percentile(e2e_ms, 99))}},
         "plain": {"value": plain_value, "unit": UNIT,
