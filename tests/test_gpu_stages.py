@@ -378,3 +378,13 @@ def test_resample_row_subset_bit_exact(T, O, scene_esd, prec):
         part = _resample_device(T, kw, mode, rows=(r0, n))
         bad = np.argwhere(part != full[r0:r0 + n])
         assert bad.size == 0, (r0, n, bad[:8].tolist(), bad.shape[0])
+
+
+def test_fp64_peak_measurement(T):
+    """tops_fp64_peak: the device's FP64 FMA rate under the current clocks,
+    the denominator of the geometric coregistration's roofline.  A B200 runs
+    FP64 FMAs at tens of TFLOP/s; two measurements agree to a few percent."""
+    a = T.fp64_peak()
+    b = T.fp64_peak()
+    assert 5.0 < a < 200.0 and 5.0 < b < 200.0, (a, b)
+    assert abs(a - b) / max(a, b) < 0.1, (a, b)
