@@ -44,11 +44,17 @@ struct EsBatch {
   EsdOverlap ov[ES_MAXOV];
 };
 
+// Shared rows are padded by one slot every 4 (pad4): a horizontal item
+// starts at a multiple of 4 columns, so its 16-byte sum loads and 8-byte
+// centre loads fall in distinct banks across the warp, and the padded
+// offsets of an item are constants when the window width is.
+__host__ __device__ constexpr int es_pad(int x) { return x + (x >> 2); }
+
 struct EsShared {
-  float4 VF[ES_GR][ES_NT];
-  float4 VB[ES_GR][ES_NT];
-  float2 IF[ES_GR][ES_NT];   // centre mF * conj(sF)
-  float2 IB[ES_GR][ES_NT];   // centre mB * conj(sB)
+  float4 VF[ES_GR][es_pad(ES_NT)];
+  float4 VB[ES_GR][es_pad(ES_NT)];
+  float2 IF[ES_GR][es_pad(ES_NT)];   // centre mF * conj(sF)
+  float2 IB[ES_GR][es_pad(ES_NT)];   // centre mB * conj(sB)
   float2 red[ES_NT / 32];
 };
 
@@ -68,8 +74,9 @@ __device__ __forceinline__ float gamma_of(float4 w) {
 }
 
 // WAZ > 0: the azimuth window height at compile time, so the input rows of a
-// group are loaded together (their latencies overlap); 0: any height.
-template <int WAZ>
+// group are loaded together (their latencies overlap); 0: any height.  WRG >
+// 0: the range window width at compile time (the horizontal box unrolls).
+template <int WAZ, int WRG>
 __global__ void __launch_bounds__(ES_NT, 2) esd_kernel(const __grid_constant__ EsBatch B,
                                                         double2 *partials) {
   extern __shared__ __align__(16) unsigned char es_smem[];
@@ -82,7 +89,7 @@ __global__ void __launch_bounds__(ES_NT, 2) esd_kernel(const __grid_constant__ E
   const EsdOverlap &O = B.ov[ob];
   const int local = item - O.item_begin;
   const int strip = local % O.strips, seg = local / O.strips;
-  const int win_rg = B.win_rg, win_az = WAZ > 0 ? WAZ : B.win_az;
+  const int win_rg = WRG > 0 ? WRG : B.win_rg, win_az = WAZ > 0 ? WAZ : B.win_az;
   const int dw = (win_rg - 1) / 2, dh = (win_az - 1) / 2;
   const int c0 = strip * ES_TW;
   const int cN = min(ES_TW, O.pixels - c0);
@@ -117,24 +124,27 @@ __global__ void __launch_bounds__(ES_NT, 2) esd_kernel(const __grid_constant__ E
       const int k = it / ngrp;
       const int cg = (it - k * ngrp) << 2;
       float4 wF = make_float4(0.f, 0.f, 0.f, 0.f), wB = wF;
+      const float4 *VF = &S.VF[k][es_pad(cg)], *VB = &S.VB[k][es_pad(cg)];
+#pragma unroll
       for (int i = 0; i < win_rg; i++) {
-        const float4 a = S.VF[k][cg + i], b = S.VB[k][cg + i];
+        const float4 a = VF[es_pad(i)], b = VB[es_pad(i)];
         wF.x += a.x; wF.y += a.y; wF.z += a.z; wF.w += a.w;
         wB.x += b.x; wB.y += b.y; wB.z += b.z; wB.w += b.w;
       }
 #pragma unroll
       for (int u = 0; u < 4; u++) {
         if (u > 0) {
-          const int ia = cg + u - 1 + win_rg, ib = cg + u - 1;
-          const float4 a = S.VF[k][ia], b = S.VF[k][ib];
+          const int ia = es_pad(u - 1 + win_rg), ib = es_pad(u - 1);
+          const float4 a = VF[ia], b = VF[ib];
           wF.x += a.x - b.x; wF.y += a.y - b.y; wF.z += a.z - b.z; wF.w += a.w - b.w;
-          const float4 c = S.VB[k][ia], d = S.VB[k][ib];
+          const float4 c = VB[ia], d = VB[ib];
           wB.x += c.x - d.x; wB.y += c.y - d.y; wB.z += c.z - d.z; wB.w += c.w - d.w;
         }
         if (cg + u >= cN) continue;
         const float g = (gamma_of(wF) + gamma_of(wB)) * 0.5f;
         if (g < B.thr || g >= 1.f) continue;
-        const float2 f = S.IF[k][cg + u + dw], b = S.IB[k][cg + u + dw];
+        const float2 f = S.IF[k][es_pad(cg) + es_pad(u + dw)];
+        const float2 b = S.IB[k][es_pad(cg) + es_pad(u + dw)];
         // (mF sF*) * conj(mB sB*)
         const float dre = f.x * b.x + f.y * b.y;
         const float dim = f.y * b.x - f.x * b.y;
@@ -213,10 +223,10 @@ __global__ void __launch_bounds__(ES_NT, 2) esd_kernel(const __grid_constant__ E
           aF.x += pF[k + j].x; aF.y += pF[k + j].y; aF.z += pF[k + j].z; aF.w += pF[k + j].w;
           aB.x += pB[k + j].x; aB.y += pB[k + j].y; aB.z += pB[k + j].z; aB.w += pB[k + j].w;
         }
-        S.VF[k][tid] = aF;
-        S.VB[k][tid] = aB;
-        S.IF[k][tid] = make_float2(pF[k + dh].x, pF[k + dh].y);
-        S.IB[k][tid] = make_float2(pB[k + dh].x, pB[k + dh].y);
+        S.VF[k][es_pad(tid)] = aF;
+        S.VB[k][es_pad(tid)] = aB;
+        S.IF[k][es_pad(tid)] = make_float2(pF[k + dh].x, pF[k + dh].y);
+        S.IB[k][es_pad(tid)] = make_float2(pB[k + dh].x, pB[k + dh].y);
       }
 #pragma unroll
       for (int j = 0; j < WAZ - 1; j++) {
@@ -265,10 +275,10 @@ __global__ void __launch_bounds__(ES_NT, 2) esd_kernel(const __grid_constant__ E
     }
 #pragma unroll
     for (int k = 0; k < ES_GR; k++) {
-      S.VF[k][tid] = aF[k];
-      S.VB[k][tid] = aB[k];
-      S.IF[k][tid] = cF[k];
-      S.IB[k][tid] = cB[k];
+      S.VF[k][es_pad(tid)] = aF[k];
+      S.VB[k][es_pad(tid)] = aB[k];
+      S.IF[k][es_pad(tid)] = cF[k];
+      S.IB[k][es_pad(tid)] = cB[k];
     }
     __syncthreads();
     horizontal(gr);
@@ -369,7 +379,8 @@ int launch_esd(const EsdOverlap *ovs, int n_ov, int win_az, int win_rg, float th
   const int s0 = once_per_device(
       setup, dev,
       [&](int &) -> int {
-        for (auto fn : {esd_kernel<3>, esd_kernel<6>, esd_kernel<0>})
+        for (auto fn : {esd_kernel<3, 10>, esd_kernel<3, 0>, esd_kernel<6, 24>, esd_kernel<6, 0>,
+                        esd_kernel<0, 0>})
           TOPS_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)sizeof(EsShared)));
         return TOPS_OK;
@@ -392,12 +403,16 @@ int launch_esd(const EsdOverlap *ovs, int n_ov, int win_az, int win_rg, float th
       B.n_ov++;
     }
     B.total_items = items;
-    if (win_az == 3)
-      esd_kernel<3><<<items, ES_NT, sizeof(EsShared), st>>>(B, part);
+    if (win_az == 3 && win_rg == 10)
+      esd_kernel<3, 10><<<items, ES_NT, sizeof(EsShared), st>>>(B, part);
+    else if (win_az == 3)
+      esd_kernel<3, 0><<<items, ES_NT, sizeof(EsShared), st>>>(B, part);
+    else if (win_az == 6 && win_rg == 24)
+      esd_kernel<6, 24><<<items, ES_NT, sizeof(EsShared), st>>>(B, part);
     else if (win_az == 6)
-      esd_kernel<6><<<items, ES_NT, sizeof(EsShared), st>>>(B, part);
+      esd_kernel<6, 0><<<items, ES_NT, sizeof(EsShared), st>>>(B, part);
     else
-      esd_kernel<0><<<items, ES_NT, sizeof(EsShared), st>>>(B, part);
+      esd_kernel<0, 0><<<items, ES_NT, sizeof(EsShared), st>>>(B, part);
     TOPS_CUDA_TRY(cudaGetLastError());
     esd_finalize_kernel<<<B.n_ov, 256, 0, st>>>(B, part, shifts, sums, o0);
     TOPS_CUDA_TRY(cudaGetLastError());
