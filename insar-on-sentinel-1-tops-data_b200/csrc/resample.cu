@@ -30,14 +30,16 @@
 //       during the previous group; each new line is deramped in registers
 //       and pushed into a 12-line register window (the window's slots rotate
 //       with the row index, so a steady row costs one deramp and no moves);
-//       v = sum_j kAz[j] d(L0-5+j) is 12 packed FP32x2 FMAs, written to a
-//       double-buffered tile.
+//       v = sum_j kAz[j] d(L0-5+j) is 12 packed FP32x2 FMAs, written to the
+//       group's 12 x 128 tile; then the next group's raw lines are staged,
+//       so their copies land while [B] runs.
 //   [B] range pass, thread = 2 adjacent output columns x 6 rows: the 14
 //       tile samples of the pair are 7 16-byte loads, the 12 range weights
 //       of each column stay in registers for its key run, and the reramp
 //       phase is a dot product of row terms and column-run terms (below).
-// One barrier per group separates [A] and [B]; the tile is double-buffered,
-// so [A] of the next group never waits for [B].
+// A barrier separates [A] and [B]; the deferred passes [C1] (columns
+// without run tables), [C2] (the second bin of two-bin rows) and [C] (the
+// per-pixel path) follow [B] when the group has such pixels.
 //
 // The phase.  The reference reramps with the 144-tap FP64 sum
 // Phi = sum_j sum_i kAz[j] kRg[i] phi(y_j, x_i).  With phi = phi_ref(y) +
@@ -53,12 +55,15 @@
 // Every row whose strip maps to one azimuth key takes the shared pass: from
 // the register window when its line is the window's, else (the row-to-line
 // map skipped a line inside a group) by the same 12-line sum over lines
-// deramped anew.  A column with more than RS_MAXRUN key runs in the item
-// finds each pixel's key and run terms with the functions that build the
-// run tables.  Rows with several azimuth keys, and pixels whose range
-// support leaves the ring window, take a per-pixel path that computes the
-// reference's formula from the slave in HBM; edge and outside pixels take
-// the nearest sample and 0.  Which path a pixel takes depends on its row,
+// deramped anew.  A row whose strip spans two adjacent bins of one line
+// takes it for the first bin; the second bin's sums follow the range pass
+// over the freed tile rows, and its columns (found by bisection in the
+// prologue) go through the keyed path.  A column with more than RS_MAXRUN
+// key runs in the item finds each pixel's key and run terms with the
+// functions that build the run tables.  Rows with more azimuth keys, and
+// pixels whose range support leaves the ring window, take a per-pixel path
+// that computes the reference's formula from the slave in HBM; edge and
+// outside pixels take the nearest sample and 0.  Which path a pixel takes depends on its row,
 // its column and its strip only, never on the work item, so a job that
 // produces a subset of the rows gives those rows bit for bit.
 //
