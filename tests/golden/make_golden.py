@@ -11,6 +11,13 @@ stores every input they saw and what they returned:
     python tests/golden/make_golden.py front           -> tests/golden/ref_front.npz
     python tests/golden/make_golden.py stages [--scene 2] [--out D]
                                                    -> D/ref_stages[2].npz (needs a GPU)
+    python tests/golden/make_golden.py timing --scene subswath [--out D]
+                                                   -> D/ref_timing_subswath.json (needs a GPU)
+
+``timing`` is not a fixture: it times the reference's own CUDA stages, called
+per burst as its drivers call them (each call copying its inputs to the device
+and its outputs back), on the benchmark's full sub-swath pair, for context
+beside the rebuild's numbers.
 
 The scene comes from the product's seeded generator (tops_synth_*), but the
 fixtures hold the generated arrays themselves, so the tests replay them
@@ -60,6 +67,9 @@ SCENES = {
               dem_lines=128, dem_pixels=128, seed=23, az_shift_true=0.03),
     "2": dict(n_bursts=4, lines_per_burst=160, samples_per_burst=300, overlap_lines=30,
               dem_lines=160, dem_pixels=160, seed=29, az_shift_true=-0.04),
+    # the benchmark's sub-swath pair (timing only)
+    "subswath": dict(n_bursts=9, lines_per_burst=1500, samples_per_burst=21000,
+                     overlap_lines=100, dem_lines=3600, dem_pixels=3600, seed=2),
 }
 SCENE = SCENES["1"]
 DEM_MARGIN = 24
@@ -544,9 +554,90 @@ def stages(out_path, host_path):
     print(f"wrote {out_path}: {len(res)} arrays")
 
 
+def timing(out_path, host_path, win=(10, 3), passes=2):
+    """Wall time of the reference's stage calls on one sub-swath pair, per
+    stage, in the order of its drivers (Func.cpp:2215-2763): geocoreg and
+    resample per burst, ESD over the overlaps, then per burst the corrected
+    resample kept on the device and its coherence.  The first pass warms the
+    context; the last one is reported."""
+    import json
+    import time
+    F = make_scene()
+    H = dict(np.load(host_path))
+    R, Co, E, G = _stage_libs()
+    nb, L, W, _ = (int(v) for v in F["m_ints"])
+    kaz, krg = iso(H["lut_kaz"]), iso(H["lut_krg"])
+    s_dt, m_dt = F["s_reals"][0], F["m_reals"][0]
+    wr, wa = win
+    ov = iso(H["m_ov"], np.int32)
+    mslc = F["master_slc"]
+    spec = float(H["m_spec_sep"])
+    for p in range(passes):
+        t = dict(geocoreg=0.0, resample=0.0, esd=0.0, resample_esd=0.0, coherence=0.0)
+        cpm = []
+        for b in range(nb):
+            t0 = time.perf_counter()
+            cpm.append(ref_geocoreg(G, F, H, b))
+            t["geocoreg"] += time.perf_counter() - t0
+        reslave = np.zeros((nb, L, W), np.complex64)
+        for b in range(nb):
+            out = iso(np.zeros((L, W), np.complex64))
+            args, keep = _rs_args(F, H, b, cpm[b][0], cpm[b][1], 0.0, s_dt, out, kaz, krg)
+            t0 = time.perf_counter()
+            R.DerampDemodResample(*args)
+            t["resample"] += time.perf_counter() - t0
+            reslave[b] = out
+        mF = iso(np.concatenate([mslc[(i + 1) * L - ov[i]:(i + 1) * L] for i in range(nb - 1)]))
+        mB = iso(np.concatenate([mslc[(i + 1) * L:(i + 1) * L + ov[i]] for i in range(nb - 1)]))
+        sF = iso(np.concatenate([reslave[i][L - ov[i]:] for i in range(nb - 1)]))
+        sB = iso(np.concatenate([reslave[i + 1][:ov[i]] for i in range(nb - 1)]))
+        shift = iso(np.full(nb - 1, np.nan))
+        t0 = time.perf_counter()
+        E.EstESDShifts(mF.ctypes.data, mB.ctypes.data, sF.ctypes.data, sB.ctypes.data,
+                       _ptr(ov, C.c_int), _ptr(shift, C.c_double), nb - 1, mF.shape[0], W, wa, wr,
+                       int(ov.max()), ESD_THRESHOLD, spec, m_dt)
+        t["esd"] += time.perf_counter() - t0
+        shifts = np.array(shift)
+        shifts[np.abs(shifts) > 100] = 0.0       # Func.cpp:2612-2621
+        coh_mean = []
+        for b in range(nb):
+            master = iso(mslc[b * L:(b + 1) * L])
+            c = iso(np.zeros((L, W), np.float32))
+            if b == 0:
+                first = iso(reslave[0])
+                t0 = time.perf_counter()
+                d = R.ResampleFirstBurst(first.ctypes.data, W, L)
+                t1 = time.perf_counter()
+                Co.CoherenceEst_ESD(0, 0, W, L, (wr - 1) // 2, (wa - 1) // 2, wr, wa,
+                                    master.ctypes.data, d, _ptr(c, C.c_float))
+            else:
+                out = iso(np.zeros((L, W), np.complex64))
+                args, keep = _rs_args(F, H, b, cpm[b][0], cpm[b][1], float(shifts[b - 1]), m_dt,
+                                      out, kaz, krg)
+                t0 = time.perf_counter()
+                d = R.DerampDemodResample_ESD(*args)
+                t1 = time.perf_counter()
+                Co.CoherenceEst(0, b * L, W, L, (wr - 1) // 2, (wa - 1) // 2, wr, wa,
+                                master.ctypes.data, d, _ptr(c, C.c_float))
+            t2 = time.perf_counter()
+            t["resample_esd"] += t1 - t0
+            t["coherence"] += t2 - t1
+            coh_mean.append(float(np.nanmean(c[20:-20, 20:-20])))
+        total = sum(t.values())
+        _say(f"pass {p}: {total:.3f} s, " + ", ".join(f"{k} {v:.3f} s" for k, v in t.items()))
+    res = {"workload": f"{nb} burst pairs of {L}x{W} CInt16, DEM {SCENE['dem_lines']}x"
+                       f"{SCENE['dem_pixels']}, window {wr}x{wa}",
+           "form": "the reference's CUDA stages (oracle/_ref), per burst, host buffers",
+           "seconds": total, "burst_pairs_per_s": nb / total,
+           "stage_seconds": t, "esd_shifts": shifts.tolist(), "mean_coherence": coh_mean}
+    with open(out_path, "w") as f:
+        json.dump(res, f, indent=1)
+    print(json.dumps(res), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
-    ap.add_argument("part", choices=("host", "stitch", "stages", "front"))
+    ap.add_argument("part", choices=("host", "stitch", "stages", "front", "timing"))
     ap.add_argument("--out", default=HERE)
     ap.add_argument("--scene", default="1", choices=sorted(SCENES))
     a = ap.parse_args()
@@ -560,6 +651,11 @@ def main():
         stitch(os.path.join(a.out, "ref_stitch.npz"))
     elif a.part == "front":
         front(os.path.join(a.out, "ref_front.npz"))
+    elif a.part == "timing":
+        hp = os.path.join(a.out, f"ref_host_{a.scene}.npz")
+        if not os.path.exists(hp):
+            host(hp)
+        timing(os.path.join(a.out, f"ref_timing_{a.scene}.json"), hp)
     else:
         stages(os.path.join(a.out, f"ref_stages{sfx}.npz"), os.path.join(HERE, f"ref_host{sfx}.npz"))
 
