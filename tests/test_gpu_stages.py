@@ -96,6 +96,28 @@ def test_resample_steep_polynomial(T, O, scene_small):
     assert rel_rms(gpu, ref) < RS_TOL
 
 
+@pytest.mark.parametrize("prec", ["split", "fp64"])
+def test_resample_azimuth_scale(T, O, scene_small, prec):
+    """An azimuth scale of 1.01 lines per row: the row-to-line map skips a
+    line every ~100 rows, so rows inside a group leave the register window's
+    line (their sums are formed directly from the staged lines), and the LUT
+    bin changes every row (more bins per item than the tap table holds).
+    Against the FP64 oracle, and row subsets bit for bit."""
+    S = scene_small
+    az, rg = oracle_cpm(O, S, 1)
+    az = np.array(az, np.float64)
+    az[1] *= 1.01
+    kw = rs_inputs(S, 1, (az, rg), 0.02)
+    mode = T.PREC_SPLIT if prec == "split" else T.PREC_FP64
+    gpu = _resample_device(T, kw, mode)
+    ref, _ = O.resample(**kw)
+    assert rel_rms(gpu, ref) < RS_TOL
+    for r0, n in ((95, 30), (13, 250)):
+        part = _resample_device(T, kw, mode, rows=(r0, n))
+        bad = np.argwhere(part != gpu[r0:r0 + n])
+        assert bad.size == 0, (r0, n, bad[:8].tolist(), bad.shape[0])
+
+
 def _resample_device(T, kw, precision, out_offset=0, slave_offset=0, rows=None):
     """tops_resample_ex on device buffers; out_offset / slave_offset (bytes)
     misalign the output and slave bases to force the scalar-access paths;
