@@ -39,6 +39,22 @@ def test_pipeline_vs_oracle(T, O, scene_esd):
     assert np.all(np.abs(gpu["shifts"] - expect) < 0.01)
 
 
+def test_compensated_sums_vs_oracle(T, O, scene_esd):
+    """tops_pair_opts.compensated: Kahan-compensated ESD phasor sums and
+    pairwise coherence window sums, at the same tolerances against the FP64
+    oracle chain; the option changes no resampling before ESD (ReSlave equal
+    to the default plan's bit for bit)."""
+    S = scene_esd
+    gpu = run_pair(T, S, compensated=1)
+    ref = oracle_chain(O, S, coherence=True)
+    assert np.abs(gpu["shifts"] - ref["shifts"]).max() < TOL_ESD_PX
+    for b in range(S.cfg.n_bursts):
+        check_burst_parity(S, gpu, ref, b)
+    plain = run_pair(T, S)
+    assert np.array_equal(gpu["reslave"], plain["reslave"])
+    assert np.abs(gpu["shifts"] - plain["shifts"]).max() < 1e-9
+
+
 def test_pipeline_graph_equals_eager(T, scene_small):
     a = run_pair(T, scene_small)
     b = run_pair(T, scene_small, graph=True)
