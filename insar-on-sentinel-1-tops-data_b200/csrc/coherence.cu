@@ -87,10 +87,10 @@ __device__ __forceinline__ float4 window_pairwise(const float4 *V, int n, Idx id
 // evaluated as |s|^2 < 1e-6.  WRG > 0: range window known at compile time;
 // an item starts at a multiple of 8 columns, so pad8(cg + i) = pad8(cg) +
 // pad8(i) and every shared-memory offset below is a constant.
-template <int WRG>
+template <int WRG, bool COMP>
 __device__ __forceinline__ void coh_horizontal(const CoShared &S, const CohJob &J, int tid,
                                                int rg, int gr, int c0, int cN, int win_rg_rt,
-                                               int dx_rt, bool comp) {
+                                               int dx_rt) {
   constexpr int NG = CO_TW / CO_CPI;
   static_assert(CO_CPI % 8 == 0, "items must start at multiples of 8 columns");
   const int win_rg = WRG > 0 ? WRG : win_rg_rt;
@@ -111,7 +111,7 @@ __device__ __forceinline__ void coh_horizontal(const CoShared &S, const CohJob &
     float out[CO_CPI];
 #pragma unroll
     for (int u = 0; u < CO_CPI; u++) {
-      if (comp) {
+      if (COMP) {
         w = window_pairwise(V, win_rg, [&](int i) { return pad8(u + i); });
       } else if (u > 0) {
         const float4 a = V[pad8(u - 1 + win_rg)];
@@ -148,7 +148,7 @@ __device__ __forceinline__ void coh_horizontal(const CoShared &S, const CohJob &
 
 // One work item (strip x segment of one job); all threads of the CTA call it
 // with the same item.
-template <int WAZ, int WRG>
+template <int WAZ, int WRG, bool COMP>
 __device__ __forceinline__ void coherence_item(CoShared &S, const CoBatch &B, int item) {
   const int tid = threadIdx.x;
   int jb = 0;
@@ -218,7 +218,7 @@ __device__ __forceinline__ void coherence_item(CoShared &S, const CoBatch &B, in
 #pragma unroll
       for (int j = 0; j < NQ; j++) q[j] = p[CO_GR + j];
       __syncthreads();
-      coh_horizontal<WRG>(S, J, tid, rg, gr, c0, cN, win_rg, dx, B.compensated != 0);
+      coh_horizontal<WRG, COMP>(S, J, tid, rg, gr, c0, cN, win_rg, dx);
       __syncthreads();
     }
   } else {
@@ -251,13 +251,15 @@ __device__ __forceinline__ void coherence_item(CoShared &S, const CoBatch &B, in
         S.spow[k][pad8(tid)] = spow[k];
       }
       __syncthreads();
-      coh_horizontal<WRG>(S, J, tid, rg, gr, c0, cN, win_rg, dx, B.compensated != 0);
+      coh_horizontal<WRG, COMP>(S, J, tid, rg, gr, c0, cN, win_rg, dx);
       __syncthreads();
     }
   }
 }
 
-template <int WAZ, int WRG>
+// COMP: the compensated window sums (a separate instantiation, so the plain
+// kernels carry none of its code or registers)
+template <int WAZ, int WRG, bool COMP>
 __global__ void __launch_bounds__(CO_NT, 3) coherence_kernel(const __grid_constant__ CoBatch B) {
   __shared__ CoShared S;
   // one work item per CTA, or (persistent) items from the queue until it
@@ -270,7 +272,7 @@ __global__ void __launch_bounds__(CO_NT, 3) coherence_kernel(const __grid_consta
     __syncthreads();
   }
   while (item < B.total_items) {
-    coherence_item<WAZ, WRG>(S, B, item);
+    coherence_item<WAZ, WRG, COMP>(S, B, item);
     if (!B.counter) break;
     if (threadIdx.x == 0) S.next_item = atomicAdd(B.counter, 1);
     __syncthreads();
@@ -378,7 +380,7 @@ __device__ __forceinline__ bool ct_wait(unsigned long long *bar, unsigned parity
 
 // One work item; returns false (all threads) when a chunk never arrived.
 // `seq` counts the chunks this CTA has consumed (slot and mbarrier phase).
-template <int WAZ>
+template <int WAZ, bool COMP>
 __device__ __forceinline__ bool coh_tma_item(CtShared &S, const CtBatch &B, int item,
                                              unsigned &seq) {
   constexpr int DY = (WAZ - 1) / 2;
@@ -480,10 +482,9 @@ __device__ __forceinline__ bool coh_tma_item(CtShared &S, const CtBatch &B, int 
 #pragma unroll
         for (int i = 0; i < CT_WRG; i++) add4(w, V[pad4(i)]);
         float out[CT_CPI];
-        const bool comp = B.compensated != 0;
 #pragma unroll
         for (int uu = 0; uu < CT_CPI; uu++) {
-          if (comp) {
+          if (COMP) {
             w = window_pairwise(V, CT_WRG, [&](int i) { return pad4(uu + i); });
           } else if (uu > 0) {
             const float4 a = V[pad4(uu - 1 + CT_WRG)];
@@ -520,7 +521,7 @@ __device__ __forceinline__ bool coh_tma_item(CtShared &S, const CtBatch &B, int 
   return ok;
 }
 
-template <int WAZ>
+template <int WAZ, bool COMP>
 __global__ void __launch_bounds__(CT_NT, 3) coh_tma_kernel(const __grid_constant__ CtBatch B) {
   extern __shared__ __align__(128) unsigned char ct_smem_raw[];
   CtShared &S = *reinterpret_cast<CtShared *>(ct_smem_raw);
@@ -538,7 +539,7 @@ __global__ void __launch_bounds__(CT_NT, 3) coh_tma_kernel(const __grid_constant
     __syncthreads();
   }
   while (item < B.total_items) {
-    if (!coh_tma_item<WAZ>(S, B, item, seq)) break;
+    if (!coh_tma_item<WAZ, COMP>(S, B, item, seq)) break;
     if (!B.counter) break;
     if (threadIdx.x == 0) S.next_item = atomicAdd(B.counter, 1);
     __syncthreads();
@@ -598,12 +599,12 @@ static int launch_coh_tma(const CohJob *jobs, int njobs, const TileCfg &cfg, int
   const int s0 = once_per_device(
       setup, dev,
       [&](int &v) -> int {
-        TOPS_CUDA_TRY(cudaFuncSetAttribute(coh_tma_kernel<WAZ>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)sizeof(CtShared)));
+        for (auto fn : {coh_tma_kernel<WAZ, false>, coh_tma_kernel<WAZ, true>})
+          TOPS_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)sizeof(CtShared)));
         int per_sm = 0, sms = 0;
         TOPS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &per_sm, coh_tma_kernel<WAZ>, CT_NT, sizeof(CtShared)));
+            &per_sm, coh_tma_kernel<WAZ, false>, CT_NT, sizeof(CtShared)));
         TOPS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         v = per_sm * sms;
         return TOPS_OK;
@@ -635,7 +636,10 @@ static int launch_coh_tma(const CohJob *jobs, int njobs, const TileCfg &cfg, int
       TOPS_CUDA_TRY(cudaMemsetAsync(B.counter, 0, sizeof(int), st));
       grid = min(items, cfg.grid > 0 ? cfg.grid : resident);
     }
-    coh_tma_kernel<WAZ><<<grid, CT_NT, sizeof(CtShared), st>>>(B);
+    if (B.compensated)
+      coh_tma_kernel<WAZ, true><<<grid, CT_NT, sizeof(CtShared), st>>>(B);
+    else
+      coh_tma_kernel<WAZ, false><<<grid, CT_NT, sizeof(CtShared), st>>>(B);
     TOPS_CUDA_TRY(cudaGetLastError());
   }
   return TOPS_OK;
@@ -643,7 +647,10 @@ static int launch_coh_tma(const CohJob *jobs, int njobs, const TileCfg &cfg, int
 
 template <int WAZ, int WRG>
 static int launch_coh_t(const CoBatch &B, int grid, cudaStream_t st) {
-  coherence_kernel<WAZ, WRG><<<grid, CO_NT, 0, st>>>(B);
+  if (B.compensated)
+    coherence_kernel<WAZ, WRG, true><<<grid, CO_NT, 0, st>>>(B);
+  else
+    coherence_kernel<WAZ, WRG, false><<<grid, CO_NT, 0, st>>>(B);
   TOPS_CUDA_TRY(cudaGetLastError());
   return TOPS_OK;
 }
@@ -657,7 +664,7 @@ static int coh_resident(int dev) {
       [&](int &v) -> int {
         int per_sm = 0, sms = 0;
         TOPS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &per_sm, coherence_kernel<WAZ, WRG>, CO_NT, 0));
+            &per_sm, coherence_kernel<WAZ, WRG, false>, CO_NT, 0));
         TOPS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         v = per_sm * sms;
         return TOPS_OK;
