@@ -282,14 +282,15 @@ __global__ void __launch_bounds__(CO_NT, 3) coherence_kernel(const __grid_consta
 }
 
 // ------------------------------------------------ TMA-staged variant
-// For the pipeline's 10-sample range window.  A CTA of CT_NT threads owns a
-// strip of CT_TW output columns and a segment of rows; its input rows come
-// in chunks of CT_CH rows x CT_LW columns (master as 32-bit, slave as 64-bit
-// elements), each chunk one cp.async.bulk.tensor box per image on an
-// mbarrier, CT_NST - 1 chunks ahead of the one being summed.  The box
-// starts CT_XOFF = dx columns left of the strip, a multiple of 4, so every
-// box's x coordinate is 16-byte aligned in both images; the copy engine
-// fills rows and columns outside the image with zeros -- the zero pad.  The
+// For the pipeline's 10-sample and the reference driver's 24-sample range
+// windows.  A CTA of CT_NT threads owns a strip of TW output columns and a
+// segment of rows; its input rows come in chunks of CT_CH rows x CT_LW
+// columns (master as 32-bit, slave as 64-bit elements), each chunk one
+// cp.async.bulk.tensor box per image on an mbarrier, CT_NST - 1 chunks ahead
+// of the one being summed.  The box starts XOFF columns left of the strip:
+// dx rounded up to a multiple of 4, so every box's x coordinate is 16-byte
+// aligned in both images; the copy engine fills rows and columns outside the
+// image with zeros -- the zero pad.  The
 // vertical sums are those of coherence_item; the horizontal sliding sum
 // restarts every CT_CPI = 4 outputs instead of every CO_CPI = 8 (measured
 // faster: 0.398 against 0.490 ms for 3 bursts of 1500 x 21000), so the two
@@ -298,17 +299,23 @@ constexpr int CT_NT = 256;
 constexpr int CT_LW = 256;                 // loaded columns (box width)
 constexpr int CT_CH = 4;                   // rows per chunk (box height)
 constexpr int CT_NST = 4;                  // chunk slots
-constexpr int CT_WRG = 10;                 // range window of this variant
-constexpr int CT_DX = (CT_WRG - 1) / 2;    // 4
-constexpr int CT_XOFF = CT_DX;             // box start left of the strip
-constexpr int CT_TW = 240;                 // output columns per strip
 constexpr int CT_CPI = 4;                  // outputs per horizontal item
 constexpr int CT_SEG = 256;                // rows per work item
 constexpr int CT_MAXJOBS = 16;
 constexpr unsigned long long CT_WAIT_NS = 2000000000ull;   // a chunk is given up after 2 s
-static_assert(CT_XOFF % 4 == 0 && CT_XOFF == CT_DX, "box x coordinates stay 16-byte aligned");
-static_assert(CT_XOFF + CT_TW + CT_WRG - 1 - CT_DX <= CT_LW, "the strip's boxes cover its windows");
-static_assert(CT_TW % CT_CPI == 0 && CT_CH * (CT_TW / CT_CPI) <= CT_NT, "one horizontal item per thread");
+// Geometry of a range window of WRG samples: the box starts XOFF columns
+// left of the strip, the window of the strip's first output starts B0
+// columns into the box, and a strip has TW outputs.
+template <int WRG>
+struct CtWin {
+  static constexpr int DX = (WRG - 1) / 2;
+  static constexpr int XOFF = (DX + 3) & ~3;
+  static constexpr int B0 = XOFF - DX;
+  static constexpr int TW = WRG == 10 ? 240 : ((CT_LW - XOFF - (WRG - 1 - DX)) & ~(CT_CPI - 1));
+  static_assert(XOFF % 4 == 0, "box x coordinates stay 16-byte aligned");
+  static_assert(XOFF + TW + WRG - 1 - DX <= CT_LW, "the strip's boxes cover its windows");
+  static_assert(TW % CT_CPI == 0 && CT_CH * (TW / CT_CPI) <= CT_NT, "one horizontal item per thread");
+};
 
 __host__ __device__ constexpr int pad4(int x) { return x + (x >> 2); }
 
@@ -380,9 +387,10 @@ __device__ __forceinline__ bool ct_wait(unsigned long long *bar, unsigned parity
 
 // One work item; returns false (all threads) when a chunk never arrived.
 // `seq` counts the chunks this CTA has consumed (slot and mbarrier phase).
-template <int WAZ, bool COMP>
+template <int WAZ, int WRG, bool COMP>
 __device__ __forceinline__ bool coh_tma_item(CtShared &S, const CtBatch &B, int item,
                                              unsigned &seq) {
+  using Win = CtWin<WRG>;
   constexpr int DY = (WAZ - 1) / 2;
   constexpr int NQ = WAZ - 1;
   constexpr int H = (NQ + CT_CH - 1) / CT_CH;   // chunks holding the first halo rows
@@ -393,13 +401,13 @@ __device__ __forceinline__ bool coh_tma_item(CtShared &S, const CtBatch &B, int 
   const CohJob &J = B.jobs[jb];
   const int local = item - J.item_begin;
   const int strip = local % J.strips, seg = local / J.strips;
-  const int c0 = strip * CT_TW;
-  const int cN = min(CT_TW, J.pixels - c0);
+  const int c0 = strip * Win::TW;
+  const int cN = min(Win::TW, J.pixels - c0);
   const int r_begin = seg * J.seg_rows;
   const int r_end = min(r_begin + J.seg_rows, J.lines);
   const int nout = (r_end - r_begin + CT_CH - 1) / CT_CH;
   const int T = H + nout;
-  const int x0 = c0 - CT_XOFF;
+  const int x0 = c0 - Win::XOFF;
   // chunk u holds input rows base(u) .. base(u) + CT_CH - 1: output chunk
   // u - H's new rows, the halo rows r_begin - DY .. r_begin - DY + NQ - 1
   // at the end of the first H chunks
@@ -471,7 +479,8 @@ __device__ __forceinline__ bool coh_tma_item(CtShared &S, const CtBatch &B, int 
     // horizontal box: CT_CPI consecutive outputs per item; an item starts at
     // a multiple of 4 columns, so every padded offset below is a constant
     {
-      constexpr int NG = CT_TW / CT_CPI;
+      constexpr int NG = Win::TW / CT_CPI;
+      constexpr int B0 = Win::B0;
       const int k = tid / NG;
       const int cg = (tid - k * NG) * CT_CPI;
       const int o = r_begin + CT_CH * (u - H) + k;   // output row
@@ -480,15 +489,15 @@ __device__ __forceinline__ bool coh_tma_item(CtShared &S, const CtBatch &B, int 
         const float *Jd = &S.spow[k][pad4(cg)];
         float4 w = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-        for (int i = 0; i < CT_WRG; i++) add4(w, V[pad4(i)]);
+        for (int i = 0; i < WRG; i++) add4(w, V[pad4(B0 + i)]);
         float out[CT_CPI];
 #pragma unroll
         for (int uu = 0; uu < CT_CPI; uu++) {
           if (COMP) {
-            w = window_pairwise(V, CT_WRG, [&](int i) { return pad4(uu + i); });
+            w = window_pairwise(V, WRG, [&](int i) { return pad4(B0 + uu + i); });
           } else if (uu > 0) {
-            const float4 a = V[pad4(uu - 1 + CT_WRG)];
-            const float4 b = V[pad4(uu - 1)];
+            const float4 a = V[pad4(B0 + uu - 1 + WRG)];
+            const float4 b = V[pad4(B0 + uu - 1)];
             const float2 m1 = make_float2(-1.f, -1.f);
             const float2 wc = __fadd2_rn(make_float2(w.x, w.y),
                                          __ffma2_rn(make_float2(b.x, b.y), m1, make_float2(a.x, a.y)));
@@ -499,7 +508,7 @@ __device__ __forceinline__ bool coh_tma_item(CtShared &S, const CtBatch &B, int 
           const float pp = w.z * w.w;
           const float num = fmaf(w.x, w.x, w.y * w.y);
           float g = (pp > 0.f && num > 0.f) ? num * rsqrtf(num) * rsqrtf(pp) : 0.f;
-          if (Jd[pad4(uu + CT_XOFF)] < 1e-6f) g = 0.f;
+          if (Jd[pad4(uu + Win::XOFF)] < 1e-6f) g = 0.f;
           out[uu] = g;
         }
         float *orow = J.coh + (long)o * J.coh_pitch + c0 + cg;
@@ -521,7 +530,7 @@ __device__ __forceinline__ bool coh_tma_item(CtShared &S, const CtBatch &B, int 
   return ok;
 }
 
-template <int WAZ, bool COMP>
+template <int WAZ, int WRG, bool COMP>
 __global__ void __launch_bounds__(CT_NT, 3) coh_tma_kernel(const __grid_constant__ CtBatch B) {
   extern __shared__ __align__(128) unsigned char ct_smem_raw[];
   CtShared &S = *reinterpret_cast<CtShared *>(ct_smem_raw);
@@ -539,7 +548,7 @@ __global__ void __launch_bounds__(CT_NT, 3) coh_tma_kernel(const __grid_constant
     __syncthreads();
   }
   while (item < B.total_items) {
-    if (!coh_tma_item<WAZ, COMP>(S, B, item, seq)) break;
+    if (!coh_tma_item<WAZ, WRG, COMP>(S, B, item, seq)) break;
     if (!B.counter) break;
     if (threadIdx.x == 0) S.next_item = atomicAdd(B.counter, 1);
     __syncthreads();
@@ -591,7 +600,7 @@ static int encode_maps(const CohJob &J, CUtensorMap *tm_m, CUtensorMap *tm_s) {
   return r == CUDA_SUCCESS ? TOPS_OK : TOPS_E_INVALID;
 }
 
-template <int WAZ>
+template <int WAZ, int WRG>
 static int launch_coh_tma(const CohJob *jobs, int njobs, const TileCfg &cfg, int dev,
                           cudaStream_t st) {
   static PerDeviceOnce setup;
@@ -599,12 +608,12 @@ static int launch_coh_tma(const CohJob *jobs, int njobs, const TileCfg &cfg, int
   const int s0 = once_per_device(
       setup, dev,
       [&](int &v) -> int {
-        for (auto fn : {coh_tma_kernel<WAZ, false>, coh_tma_kernel<WAZ, true>})
+        for (auto fn : {coh_tma_kernel<WAZ, WRG, false>, coh_tma_kernel<WAZ, WRG, true>})
           TOPS_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)sizeof(CtShared)));
         int per_sm = 0, sms = 0;
         TOPS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &per_sm, coh_tma_kernel<WAZ, false>, CT_NT, sizeof(CtShared)));
+            &per_sm, coh_tma_kernel<WAZ, WRG, false>, CT_NT, sizeof(CtShared)));
         TOPS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         v = per_sm * sms;
         return TOPS_OK;
@@ -622,7 +631,7 @@ static int launch_coh_tma(const CohJob *jobs, int njobs, const TileCfg &cfg, int
       J = jobs[j];
       J.seg_rows = cfg.seg_rows ? cfg.seg_rows : CT_SEG;
       J.segs = (J.lines + J.seg_rows - 1) / J.seg_rows;
-      J.strips = (J.pixels + CT_TW - 1) / CT_TW;
+      J.strips = (J.pixels + CtWin<WRG>::TW - 1) / CtWin<WRG>::TW;
       J.item_begin = items;
       items += J.strips * J.segs;
       const int s = encode_maps(J, &B.tm_m[B.njobs], &B.tm_s[B.njobs]);
@@ -637,9 +646,9 @@ static int launch_coh_tma(const CohJob *jobs, int njobs, const TileCfg &cfg, int
       grid = min(items, cfg.grid > 0 ? cfg.grid : resident);
     }
     if (B.compensated)
-      coh_tma_kernel<WAZ, true><<<grid, CT_NT, sizeof(CtShared), st>>>(B);
+      coh_tma_kernel<WAZ, WRG, true><<<grid, CT_NT, sizeof(CtShared), st>>>(B);
     else
-      coh_tma_kernel<WAZ, false><<<grid, CT_NT, sizeof(CtShared), st>>>(B);
+      coh_tma_kernel<WAZ, WRG, false><<<grid, CT_NT, sizeof(CtShared), st>>>(B);
     TOPS_CUDA_TRY(cudaGetLastError());
   }
   return TOPS_OK;
@@ -699,13 +708,18 @@ int launch_coherence(const CohJob *jobs, int njobs, int win_rg, int win_az, cons
   int dev = 0;
   TOPS_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDevices) return TOPS_E_INVALID;
-  // the TMA-staged kernel for the pipeline's 10-sample range window
-  if (win_rg == CT_WRG && (win_az == 3 || win_az == 6) && tensor_map_encoder()) {
+  // the TMA-staged kernel for the pipeline's 10 x 3 and the reference
+  // driver's 24 x 6 windows (and 10 x 6, 24 x 3)
+  if ((win_rg == 10 || win_rg == 24) && (win_az == 3 || win_az == 6) && tensor_map_encoder()) {
     bool all = true;
     for (int j = 0; j < njobs; j++) all = all && tma_eligible(jobs[j]);
-    if (all)
-      return win_az == 3 ? launch_coh_tma<3>(jobs, njobs, cfg, dev, st)
-                         : launch_coh_tma<6>(jobs, njobs, cfg, dev, st);
+    if (all) {
+      if (win_rg == 10)
+        return win_az == 3 ? launch_coh_tma<3, 10>(jobs, njobs, cfg, dev, st)
+                           : launch_coh_tma<6, 10>(jobs, njobs, cfg, dev, st);
+      return win_az == 3 ? launch_coh_tma<3, 24>(jobs, njobs, cfg, dev, st)
+                         : launch_coh_tma<6, 24>(jobs, njobs, cfg, dev, st);
+    }
   }
   for (int j0 = 0, k = 0; j0 < njobs; j0 += CO_MAXJOBS, k++) {
     CoBatch B;

@@ -263,10 +263,10 @@ def test_coherence_slave_equals_master(T, O, scene_small):
     assert np.all(gpu[~live] == 0)
 
 
-@pytest.mark.parametrize("win_az", [3, 6])
-def test_coherence_tma_equals_generic(T, scene_small, win_az):
-    """The TMA-staged coherence kernel (10-sample range window, 16-byte
-    aligned rows) against the generic kernel (the slave placed 8 bytes off a
+@pytest.mark.parametrize("win_rg,win_az", [(10, 3), (10, 6), (24, 6), (24, 3)])
+def test_coherence_tma_equals_generic(T, scene_small, win_rg, win_az):
+    """The TMA-staged coherence kernel (10- and 24-sample range windows,
+    16-byte aligned rows) against the generic kernel (the slave placed 8 bytes off a
     16-byte boundary takes it): the same vertical sums, the horizontal
     sliding sum restarted every 4 instead of every 8 outputs, so the two
     agree to FP32 rounding of the window sums."""
@@ -288,7 +288,7 @@ def test_coherence_tma_equals_generic(T, scene_small, win_az):
         job = T.CohJob(master=dm.data_ptr(), master_pitch=W * 4, slave=sl.data_ptr(),
                        slave_pitch=W * 8, coh=coh.data_ptr(), coh_pitch=W * 4, lines=L, pixels=W)
         torch.cuda.synchronize()
-        T.check(T.lib.tops_coherence(C.byref(job), 1, 10, win_az, None), "tops_coherence")
+        T.check(T.lib.tops_coherence(C.byref(job), 1, win_rg, win_az, None), "tops_coherence")
         torch.cuda.synchronize()
         out.append(coh.cpu().numpy())
     assert np.abs(out[0] - out[1]).max() < 2e-6
