@@ -69,10 +69,12 @@
 //
 // Precision modes: TOPS_PREC_SPLIT (default) forms each sample's deramp
 // phase in FP32 as rho(y) + G(y, x), rho the FP64 reference phase reduced
-// mod 2 pi once per slave line (double-single) and G the FP32 quadratic
-// about the burst's centre time.  TOPS_PREC_FP64 evaluates every sample's
-// deramp phase and its reduction in FP64.  Positions, LUT bins and Psi are
-// FP64 in both.
+// once per slave line and G the FP32 quadratic about the burst's centre
+// time, both in turns (cycles), so that the sum is reduced exactly by
+// t - rint(t) before the sine and cosine.  TOPS_PREC_FP64 evaluates every
+// sample's deramp phase and its reduction in FP64.  The reramp phase is
+// formed in turns in both modes.  Positions, LUT bins and Psi are FP64 in
+// both.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -201,10 +203,20 @@ __device__ __forceinline__ double deramp_phase(double ta, double kt, double tref
   return -kPi * kt * (e * e) - 2.0 * kPi * fdc * ta;
 }
 
-__device__ __forceinline__ float2 cmul_conj_phase(float2 a, float phi) {
-  // a * exp(-i phi)
+// Phases of the split arithmetic are carried in turns (cycles): a turn is
+// reduced to [-1/2, 1/2] by t - rint(t), exact for |t| < 2^22, and scaled
+// by 2 pi once for the sine and cosine.
+constexpr float kTwoPiF = 6.28318530717958647692f;
+__device__ __forceinline__ float turns_reduce(float t) { return t - rintf(t); }
+// An FP64 phase in radians as turns reduced to [-1/2, 1/2].
+__device__ __forceinline__ float to_turns(double phi) {
+  const double u = phi * kInvTwoPi;
+  return (float)(u - rint(u));
+}
+// a * exp(-i 2 pi t), t in turns
+__device__ __forceinline__ float2 cmul_conj_turns(float2 a, float t) {
   float s, c;
-  __sincosf(reduce_2pi_f(phi), &s, &c);
+  __sincosf(turns_reduce(t) * kTwoPiF, &s, &c);
   return make_float2(a.x * c + a.y * s, a.y * c - a.x * s);
 }
 
@@ -440,11 +452,11 @@ __device__ __forceinline__ float2 deramp_at(const RsShared &S, const ResampleJob
     } else {
       const DerampQuad refq = {S.ref_a0, S.ref_a1, S.ref_a2};
       const double ta = (double)(y - J.s_first_line) * J.dt;
-      rho = reduce_2pi(quad_eval(refq, ta));
+      rho = to_turns(quad_eval(refq, ta));
       tc = (float)(ta - S.tm);
     }
     const float G = fmaf(fmaf(g2c, tc, g1c), tc, g0c);
-    r = reduce_2pi_f(rho + G);
+    r = turns_reduce(rho + G) * kTwoPiF;
   } else {
     const double ta = ((unsigned)iy < (unsigned)RS_NSR) ? S.srow[iy].ta
                                                          : (double)(y - J.s_first_line) * J.dt;
@@ -466,7 +478,7 @@ __device__ __forceinline__ float2 deramp_staged(const RsShared &S, int x, int y,
   float r;
   if (kSplit) {
     const float G = fmaf(fmaf(g2c, sr.f.tc, g1c), sr.f.tc, g0c);
-    r = reduce_2pi_f(sr.f.rho + G);
+    r = turns_reduce(sr.f.rho + G) * kTwoPiF;
   } else {
     r = reduce_2pi(quad_eval(cq, sr.ta));
   }
@@ -561,7 +573,7 @@ __device__ __forceinline__ float2 pixel_keyed(const RsShared &S, const ResampleJ
   cr.ok = p0 >= J.sx0 + 5 && p0 <= J.sx1 - 7 && xb >= 0 && xb + 13 < RS_FW;
   if (cr.ok) {
     run_weights(cr, J);
-    return cmul_conj_phase(range_single(vrow, xb, cr), run_phase(R, cr));
+    return cmul_conj_turns(range_single(vrow, xb, cr), run_phase(R, cr));
   }
   if (p0 < J.sx0 || p0 > J.sx1) return make_float2(0.f, 0.f);
   if (p0 < J.sx0 + 5 || p0 > J.sx1 - 7) {
@@ -613,8 +625,8 @@ __device__ __forceinline__ void row_terms(const RsShared &S, const ResampleJob &
   }
   const double tc0 = (double)(L0 - J.s_first_line) * J.dt - S.tm;
   const double dt = J.dt;
-  R.rho = reduce_2pi(psi);
-  R.psif = (float)psi;
+  R.rho = to_turns(psi);
+  R.psif = (float)(psi * kInvTwoPi);
   R.R2 = (float)(m0 * tc0 * tc0 + 2.0 * tc0 * dt * m1 + dt * dt * m2);
   R.R1 = (float)(m0 * tc0 + dt * m1);
   R.R0 = (float)m0;
@@ -714,9 +726,9 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
     cq = refq;
     if (xin) cq = deramp_quad(J.kt[xa], J.tref[xa], J.fdc[xa]);
     const double d2 = cq.a2 - refq.a2, d1 = cq.a1 - refq.a1, d0 = cq.a0 - refq.a0;
-    g2c = (float)d2;
-    g1c = (float)(2.0 * d2 * tm + d1);
-    g0c = (float)((d2 * tm + d1) * tm + d0);
+    g2c = (float)(d2 * kInvTwoPi);   // in turns
+    g1c = (float)((2.0 * d2 * tm + d1) * kInvTwoPi);
+    g0c = (float)(((d2 * tm + d1) * tm + d0) * kInvTwoPi);
   }
   S.ring_gc[x] = make_float4(g2c, g1c, g0c, 0.f);
 
@@ -1002,7 +1014,7 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
       const double ta = (double)(y - J.s_first_line) * J.dt;
       RsSlaveRow sr;
       if (kSplit) {
-        sr.f.rho = reduce_2pi(quad_eval(refq, ta));
+        sr.f.rho = to_turns(quad_eval(refq, ta));
         sr.f.tc = (float)(ta - tm);
       } else {
         sr.ta = ta;
@@ -1172,8 +1184,8 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
           }
           float2 s0, s1;
           range_pair(cr0, cr1, V, odd, s0, s1);
-          const float2 o0 = cmul_conj_phase(s0, run_phase(R, cr0));
-          const float2 o1 = cmul_conj_phase(s1, run_phase(R, cr1));
+          const float2 o0 = cmul_conj_turns(s0, run_phase(R, cr0));
+          const float2 o1 = cmul_conj_turns(s1, run_phase(R, cr1));
           if (out16) {
             *reinterpret_cast<float4 *>(orow) = make_float4(o0.x, o0.y, o1.x, o1.y);
           } else {
@@ -1198,7 +1210,7 @@ __device__ __forceinline__ void resample_item(RsShared &S, const RsBatch &B, int
               const int e = atomicAdd(&S.gen_n[g], 1);
               S.gen[e] = (unsigned short)(k * 128 + dc + cc);
             } else if (cr.ok) {
-              orow[cc] = cmul_conj_phase(range_single(vrow, p0 - 5 - xw, cr), run_phase(R, cr));
+              orow[cc] = cmul_conj_turns(range_single(vrow, p0 - 5 - xw, cr), run_phase(R, cr));
             } else if (p0 < J.sx0 || p0 > J.sx1) {
               orow[cc] = make_float2(0.f, 0.f);
             } else {
