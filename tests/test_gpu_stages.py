@@ -263,8 +263,10 @@ def test_coherence_slave_equals_master(T, O, scene_small):
     assert np.all(gpu[~live] == 0)
 
 
-@pytest.mark.parametrize("win_rg,win_az", [(10, 3), (10, 6), (24, 6), (24, 3)])
-def test_coherence_tma_equals_generic(T, scene_small, win_rg, win_az):
+@pytest.mark.parametrize("win_rg,win_az,crop", [(10, 3, None), (10, 6, None), (24, 6, None),
+                                               (24, 3, None), (10, 3, (53, 40)),
+                                               (24, 6, (53, 40))])
+def test_coherence_tma_equals_generic(T, scene_small, win_rg, win_az, crop):
     """The TMA-staged coherence kernel (10- and 24-sample range windows,
     16-byte aligned rows) against the generic kernel (the slave placed 8 bytes off a
     16-byte boundary takes it): the same vertical sums, the horizontal
@@ -275,6 +277,9 @@ def test_coherence_tma_equals_generic(T, scene_small, win_rg, win_az):
     S = scene_small
     m = np.ascontiguousarray(S.burst(0, 1))
     s = np.ascontiguousarray(S.burst(1, 1)).astype(np.float32)
+    if crop:   # a partial strip and a segment shorter than a chunk group
+        m = np.ascontiguousarray(m[:crop[0], :crop[1]])
+        s = np.ascontiguousarray(s[:crop[0], :crop[1]])
     L, W = m.shape[:2]
     dm = torch.from_numpy(m.view(np.int32).reshape(L, W)).cuda()
     ds = torch.from_numpy(s).cuda()
